@@ -1,0 +1,363 @@
+"""Benchmark of the B200 PBF step: particle-steps/s on the 1M-particle dam.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--scene dam_1m] [--impl reference]
+
+One "step" is one full PBF time step (the stage order of the reference's
+Simulation/Source/main.cpp:71-124) over the whole particle set.  Prints ONE
+JSON line on rank 0.
+
+  value        particle-steps/s of K graph-replayed steps, state resident in HBM,
+               CUDA events on the library's stream, max over ranks
+  e2e          the same metric through the public C ABI with host buffers:
+               every step uploads x and v from pinned host memory, runs the
+               step and downloads x and v
+  roofline     the dominant kernel's algorithmic bytes per launch / its mean
+               duration (CUDA events around each kernel of K eagerly launched
+               steps on the library's stream), against the measured HBM copy
+               bandwidth
+  cpu_baseline the reference's own OpenMP build (oracle/_ref) on this host's
+               cores, a bounded sample of the same workload
+Multi-GPU: the path does not shard in this build (replicas only): every rank
+runs its own full scene on its own GPU; value sums the ranks' particle-steps
+over the slowest rank's time.
+`--impl reference` times the reference's CPU build instead (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+for _p in (ROOT, ROOT / "sph-cpp_b200"):
+    if str(_p) not in sys.path:
+        sys.path.insert(0, str(_p))
+
+METRIC = "particle-steps/s at 1M (plain vs learned warm-start, equal density error)"
+UNIT = "particle-steps/s"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--scene", default="dam_1m")
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--exact", action="store_true", help="exact_math=1 (bit-exact arithmetic)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU baseline sample")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(
+        os.environ.get("LOCAL_RANK", "0"))
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in (self.out or "").splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() in ("active", "1"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- algorithmic bytes
+def kernel_bytes(name: str, n: int, nbar: float, K: int, nbins: int) -> float:
+    """Compulsory DRAM bytes per launch of each kernel: each per-particle input
+    read once, each output written once, int32 neighbor-list entries read once;
+    gathered neighbour values counted as cache hits (they are re-reads of
+    arrays already streamed by the same launch)."""
+    L = 4.0 + 4.0 * nbar   # count + list
+    per = {
+        "ext_predict_hash": 16 + 16 + 16 + 16 + 4 + 4,           # x, v in; v, x*, key, rank out (+ histogram in L2)
+        "scan_reduce": 4.0 * nbins / n,
+        "scan_partials": 0.0,
+        "scan_apply": 8.0 * nbins / n,
+        "scatter": 4 + 4 + 4 + 8,                               # key, rank, orig in; pair out
+        "cell_sort": 8.0 + 4.0 * nbins / n,                     # pairs in place (read) + bin starts
+        "reorder": 8 + 4 + 3 * 16 + 3 * 16 + 4 + 4,             # pair, key, (x, x*, v) in and out, orig, key
+        "fill_neighbors": 16 + 4 * nbar + 4 + 8.0 * nbins / n,  # own x*, list + count out, bin starts
+        "density_lambda": 16 + L + 16 + 4 + 4,                  # x* in; list; (x*, lambda), rho, lambda out
+        "dp_update": 16 + L + 16 + (32.0 / K),                  # (x*, lambda) in; list; x* out; last: x in, v out
+        "viscosity": 16 + 16 + L + 16,
+        "vorticity": 16 + 16 + L + 16 + 16,
+        "apply_vorticity": 16 + 16 + 16 + L + 16,
+        "viscosity_final": 16 + 16 + L + 16 + 16 + 16 + 4 + 4,
+        "update_velocities": 16 + 16 + 16,
+        "color_field": 16 + 16 + L + 16,
+        "surface_tension": 16 + 16 + 16 + L + 16,
+    }
+    return per.get(name, 0.0) * n
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def ncu_traffic(kernel: str, scene: str) -> float | None:
+    """dram bytes per launch from a committed ncu summary, if one exists for this
+    kernel and workload (profiles/<kernel>_<scene>.txt, line 'dram_bytes_per_launch: X')."""
+    f = ROOT / "profiles" / f"{kernel}_{scene}.txt"
+    if not f.exists():
+        return None
+    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", f.read_text())
+    return float(m.group(1)) if m else None
+
+
+# ---------------------------------------------------------------- CPU reference
+def run_reference_cpu(scene, steps: int, warmup: int, budget_s: float | None) -> dict:
+    """The reference's own OpenMP build on all host cores (oracle/_ref);
+    the oracle restatement when the reference build is absent."""
+    from oracle.oracle import OracleSim, RefSim, host_cores, ref_available
+    p = scene.params()
+    x = scene.positions()
+    cores = host_cores()
+    if ref_available():
+        sim = RefSim(p, scene.n, threads=cores)
+        kind = "reference"
+    else:
+        os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+        sim = OracleSim(p, scene.n)
+        kind = "port"
+    sim.set_state(x)
+    for _ in range(max(warmup, 0)):
+        sim.step(1)
+    if budget_s is not None:
+        t0 = time.perf_counter()
+        sim.step(1)
+        one = time.perf_counter() - t0
+        steps = max(1, min(steps, int(budget_s / max(one, 1e-6))))
+    t0 = time.perf_counter()
+    sim.step(steps)
+    dt = time.perf_counter() - t0
+    sim.close()
+    return {"value": scene.n * steps / dt, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": f"{scene.name}: {scene.n} particles, {steps} timed full steps after {max(warmup, 0)} warm-up "
+                      f"step(s), std::chrono/perf_counter wall time, {dt:.2f} s",
+            "steps": steps, "seconds": dt}
+
+
+# ---------------------------------------------------------------- main
+def main():
+    args = parse_args()
+    rank, world, local = dist_env()
+    from pbf_b200 import make_scene
+    scene = make_scene(args.scene, exact_math=1 if args.exact else 0)
+    K, W = args.steps, args.warmup
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        r = run_reference_cpu(scene, K, W, None)
+        line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+                "steps": r["steps"], "warmup": W, "ms_per_step": 1e3 * r["seconds"] / r["steps"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded jittered dam-break lattice)",
+                "config": {"workload": scene.name, "particles": scene.n, "solve_steps": scene.solve_steps,
+                           "lambda_epsilon": scene.lambda_epsilon, "neighbor_cap": scene.neighbor_cap},
+                "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
+                                 "sample": r["sample"]},
+                "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+
+    from pbf_b200 import Particles
+    p = scene.params()
+    x0 = scene.positions()
+    g = Particles(p, scene.n)
+    g.upload(x0)
+    stream = torch.cuda.ExternalStream(g.stream_handle())
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize()
+        g.sync()
+
+    def max_over_ranks(v: float) -> float:
+        if pg is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up (also captures the one-step graph)
+    for _ in range(max(W, 3)):
+        g.step(1)
+    barrier()
+
+    # ---- device-resident timed region: K graph replays ----
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier()
+        e0.record(stream)
+        for _ in range(K):
+            g.step(1)
+        e1.record(stream)
+        e1.synchronize()
+        barrier()
+    t_dev = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    st = g.stats()
+    nbar = st["mean_neighbors"]
+
+    # ---- per-kernel times: K eager steps with CUDA events around each kernel ----
+    g.set_timing(True)
+    g.reset_timing()
+    g.step(K)
+    kt = g.kernel_times()
+    g.set_timing(False)
+    total_kernel_ms = sum(v["total_ms"] for v in kt.values())
+    dom = max(kt.items(), key=lambda kv: kv[1]["total_ms"])
+    dom_name, dom_t = dom[0], dom[1]
+    dom_avg_s = dom_t["total_ms"] / dom_t["launches"] / 1e3
+    nbins = int(g._lib.pbf_num_bins(g.ctx))
+    dom_bytes = kernel_bytes(dom_name, scene.n, nbar, scene.solve_steps, nbins)
+    peaks = measured_peaks()
+    achieved = dom_bytes / dom_avg_s / 1e9
+    step_bytes = sum(kernel_bytes(k, scene.n, nbar, scene.solve_steps, nbins) * v["launches"] for k, v in kt.items()) / K
+    kernels = {k: {"launches": v["launches"], "ms_per_launch": v["total_ms"] / v["launches"],
+                   "share": v["total_ms"] / total_kernel_ms,
+                   "gbs": kernel_bytes(k, scene.n, nbar, scene.solve_steps, nbins) / (v["total_ms"] / v["launches"] / 1e3) / 1e9}
+               for k, v in sorted(kt.items(), key=lambda kv: -kv[1]["total_ms"])}
+
+    # ---- end to end through the C ABI with pinned host buffers ----
+    xh = torch.empty((scene.n, 3), dtype=torch.float32, pin_memory=True).numpy()
+    vh = torch.empty((scene.n, 3), dtype=torch.float32, pin_memory=True).numpy()
+    xh[:] = x0
+    vh[:] = 0.0
+    import ctypes as C
+    lib = g._lib
+    px, pv = xh.ctypes.data_as(C.c_void_p), vh.ctypes.data_as(C.c_void_p)
+    for _ in range(2):
+        assert lib.pbf_upload(g.ctx, px, pv, scene.n) == 0
+        assert lib.pbf_step(g.ctx, 1) == 0
+        assert lib.pbf_download(g.ctx, px, pv, None, None) == 0
+    barrier()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(K):
+        lib.pbf_upload(g.ctx, px, pv, scene.n)
+        lib.pbf_step(g.ctx, 1)
+        lib.pbf_download(g.ctx, px, pv, None, None)
+    f1.record(stream)
+    f1.synchronize()
+    barrier()
+    t_e2e = max_over_ranks(f0.elapsed_time(f1) / 1e3)
+
+    ok = bool(np.isfinite(xh).all())
+    launches = g.launches_per_step() * K
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = run_reference_cpu(scene, 100, 1, args.cpu_seconds)
+        except Exception as e:  # reported, never fatal for the GPU line
+            cpu = {"error": str(e)}
+    if pg is not None:
+        pg.barrier()
+
+    if rank == 0:
+        value = scene.n * K * world / t_dev
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": max(W, 3),
+            "ms_per_step": 1e3 * t_dev / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded jittered dam-break lattice, zero initial velocity)",
+            "config": {"workload": scene.name, "particles": scene.n, "lattice": list(scene.lattice),
+                       "box": list(scene.box_max), "solve_steps": scene.solve_steps,
+                       "lambda_epsilon": scene.lambda_epsilon, "neighbor_cap": scene.neighbor_cap,
+                       "exact_math": scene.exact_math, "scorr": "off (reference has none)",
+                       "parallelism": f"replicas x{world}",
+                       "l2": "no flush: per-step working set (lists %.0f MB + state) > 126 MB L2" % (
+                           scene.n * (4 * nbar + 4) / 1e6)},
+            "e2e": {"value": scene.n * K * world / t_e2e, "unit": UNIT, "h2d_bytes_per_step": scene.n * 24,
+                    "d2h_bytes_per_step": scene.n * 24},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peaks["hbm_gbs"],
+                         "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                         "traffic": ncu_traffic(dom_name, scene.name),
+                         "algorithmic_bytes_per_launch": dom_bytes, "peak_source": peaks["source"],
+                         "step_gbs": step_bytes / (t_dev / K) / 1e9},
+            "kernels": kernels,
+            "physics": {"mean_neighbors": nbar, "cap_hits": st["cap_hits"],
+                        "mean_density_error": st["mean_density_error"], "error_flags": st["error_flags"],
+                        "finite": ok},
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    g.close()
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,232 @@
+/*
+ * pbf.h — C ABI of the B200 position-based-fluids (PBF) step.
+ *
+ * Drop-in for the per-stage call surface of the reference's
+ * sim::Particles<float,3> (Simulation/Source/particles.h:256-487), which the
+ * reference reaches through sim::algorithms (Common/sim_algorithms.h:38-260).
+ * A generic lambda-taking template cannot cross a C ABI, so the boundary keeps
+ * the *stage* surface: one exported function per Particles stage, plus a fused,
+ * CUDA-graph-captured whole step.  include/pbf_particles.hpp wraps this in a
+ * C++ class with the reference's method names.
+ *
+ * Conventions
+ *  - Every function returns 0 on success or a negative PBF_ERR_* code; the
+ *    message is available from pbf_last_error(ctx).  No C++ exception crosses
+ *    the ABI (the reference throws std::runtime_error, array.h:128-129; the
+ *    C++ facade turns a nonzero status back into std::runtime_error).
+ *  - Host arrays are the reference's Vec<float,3> layout: 12-byte AoS float[3]
+ *    (Common/vec.h:184-192), indexed by the reference's particle index.
+ *  - Work is stream-ordered on the context's own CUDA stream; functions that
+ *    return host data synchronise that stream.  One context per host thread;
+ *    a context is not re-entrant.
+ *  - Spans: the reference's IndexSpan arguments are kept for call-surface
+ *    fidelity.  A single rank always passes [0, N); any other span returns
+ *    PBF_ERR_SPAN.
+ *  - Device memory is owned by the context (allocated once in pbf_create,
+ *    sized by capacity); the caller keeps ownership of its host arrays.
+ */
+#ifndef PBF_B200_H
+#define PBF_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PBF_OK 0
+#define PBF_ERR_ARG -1        /* bad argument (null pointer, size) */
+#define PBF_ERR_CUDA -2       /* CUDA runtime error */
+#define PBF_ERR_CAPACITY -3   /* n > capacity (reference: array.h:128-129) */
+#define PBF_ERR_SPAN -4       /* span other than [0, N) */
+#define PBF_ERR_PARAMS -5     /* parameters outside what the reference grid supports */
+#define PBF_ERR_STATE -6      /* call out of order (e.g. no neighbor lists yet) */
+#define PBF_ERR_DEVICE -7     /* device-side check tripped (see pbf_stats_t.error_flags) */
+#define PBF_ERR_IO -8         /* INI file unreadable */
+
+/* Device-side error flag bits (pbf_stats_t.error_flags). */
+#define PBF_FLAG_KEY_RANGE 1u     /* a bin id fell outside the grid; clamped */
+#define PBF_FLAG_NONFINITE 2u     /* a non-finite position was hashed */
+
+/*
+ * Parameter block.  Field meaning follows the reference's public
+ * Parameters<float,3> fields (Common/parameters.h:550-573); pbf_params_derive
+ * fills the derived ones the way Parameters::derive_from_input does
+ * (parameters.h:123-148).
+ */
+typedef struct pbf_params {
+  float time_step;            /* dt                                   (parameters.h:564) */
+  float gravity;              /* g, applied to v.y                    (particles.h:268)  */
+  float gamma;                /* surface tension; 0 = stage is a no-op (particles.h:400-431) */
+  float visc_c;               /* XSPH coefficient                     (particles.h:445)  */
+  float lambda_epsilon;       /* constraint-force-mixing epsilon      (particles.h:340)  */
+  float vorticity_coef;       /* vorticity confinement epsilon        (particles.h:484)  */
+  float smoothing_radius;     /* h                                    (parameters.h:555) */
+  float neighbor_bin_spacing; /* s, grid cell edge and list radius    (neighbors.h:198)  */
+  float rest_density;         /* rho0                                 (parameters.h:557) */
+  float rest_mass;            /* m                                    (parameters.h:558) */
+  float max_speed;            /* 0.5*h*K/dt, velocity clamp scale     (parameters.h:145) */
+  float particle_rest_spacing;/* lattice spacing                      (parameters.h:553) */
+  float boundary_min[3];      /* wall clamp box                       (particles.h:525)  */
+  float boundary_max[3];
+  float mover_center[3];      /* mover sphere centre                  (particles.h:517)  */
+  float mover_radius;         /* 0.2 in the reference                 (particles.h:515)  */
+  int32_t solve_steps;        /* K Jacobi iterations                  (main.cpp:82)      */
+  int32_t neighbor_cap;       /* 60 in the reference (MAX_NEIGHBORS, neighbors.h:39); <= 64 */
+  /* Artificial-pressure term s_corr = -k (W(r)/W(dq))^n (Macklin & Mueller
+   * 2013).  Not in the reference (particles.h:348-358 has none): k = 0 keeps
+   * reference parity. */
+  float scorr_k;
+  float scorr_n;
+  float scorr_dq;             /* as a fraction of h */
+  /* 1: every kernel evaluates in the reference's operation order with
+   * IEEE-rounded add/mul/div/sqrt and no FMA (bit-identical to the reference's
+   * CPU build on the same inputs); 0: fast math in the physics gathers
+   * (reciprocals, FMA), results within the 1e-5 parity tolerance.  The
+   * neighbor search, predict and boundary clamp are always exact. */
+  int32_t exact_math;
+  int32_t reserved[3];
+} pbf_params;
+
+/* Physics statistics of the current state (a residual density pass over the
+ * current positions with the current neighbor lists; no state is modified). */
+typedef struct pbf_stats_t {
+  uint64_t n;
+  double mean_density_error;  /* mean_i max(rho_i/rho0 - 1, 0) (clamped constraint, particles.h:325) */
+  double max_density_error;   /* max_i  max(rho_i/rho0 - 1, 0) */
+  double kinetic_energy;      /* sum_i 0.5 m |v_i|^2 */
+  double center_of_mass[3];   /* mean_i x_i */
+  double mean_neighbors;      /* mean list length */
+  uint64_t cap_hits;          /* particles whose list is at the cap */
+  uint32_t error_flags;       /* PBF_FLAG_* bits raised since the last pbf_stats */
+  uint32_t pad;
+} pbf_stats_t;
+
+typedef struct pbf_ctx pbf_ctx;
+
+/* ---- parameters and scene construction (host only, no GPU needed) ---- */
+
+/* Reference defaults for the keys the INI may omit: mover radius 0.2,
+ * neighbor cap 60, rest mass 1, s_corr off; everything else -1 as the
+ * reference's read_INI leaves an absent key (parameters.h:96-118). */
+void pbf_params_init(pbf_params* p);
+
+/* Derive spacing-dependent fields as Parameters::derive_from_input does
+ * (parameters.h:123-148): h = 1.8*spacing if h <= 0, s = 1.2*h if s <= 0,
+ * m = 1, rho0 = m/spacing^3 (unless rest_density_override > 0),
+ * max_speed = 0.5*h*K/dt. */
+int pbf_params_derive(pbf_params* p, float rest_spacing, float rest_density_override);
+
+/* Read the reference's INI schema (parameters.h:92-119) into p and the
+ * initial-fluid box; derives as above.  fluid_min/fluid_max may be NULL. */
+int pbf_params_from_ini(const char* path, pbf_params* p, float fluid_min[3], float fluid_max[3]);
+
+/* Lattice counts per axis = floor(extent/spacing) (aabb.h:213-219). */
+int pbf_lattice_dims(const float fluid_min[3], const float fluid_max[3], float spacing,
+                     int64_t dims_out[3]);
+
+/* construct_fluid (particles.h:231-250): z outer, x inner,
+ * x = (idx*spacing + min) + spacing/2, then a seeded jitter, uniform in
+ * [-amp, +amp) per axis, from SplitMix64 over (seed, 3*index + axis).
+ * x_out holds dims[0]*dims[1]*dims[2] AoS float3 entries. */
+int pbf_build_lattice(const float fluid_min[3], const int64_t dims[3], float spacing,
+                      float jitter_amp, uint64_t seed, float* x_out);
+
+/* Density of the centre particle of an unjittered spacing-lattice of
+ * (2r+1)^3 particles, computed with the reference's Poly6 sum
+ * (particles.h:292-313) in its neighbor-list order: the "rest density from an
+ * interior lattice particle" convention.  Host computation. */
+int pbf_lattice_rest_density(const pbf_params* p, float spacing, float* rho0_out);
+
+/* Grid dimensions the reference builds for p (neighbors.h:69-71). */
+int pbf_grid_dims(const pbf_params* p, int64_t dims_out[3]);
+
+/* ---- context ---- */
+
+/* Allocates every device buffer for up to `capacity` particles on the current
+ * CUDA device and validates p against the reference grid (box min >= 0 and
+ * all hashed bins in range). */
+int pbf_create(const pbf_params* p, size_t capacity, pbf_ctx** out);
+void pbf_destroy(pbf_ctx* ctx);
+const char* pbf_last_error(const pbf_ctx* ctx);
+/* Message of the last pbf_create failure (no context exists then). */
+const char* pbf_create_error(void);
+
+/* Replace the parameters (same capacity; grid must not grow). */
+int pbf_set_params(pbf_ctx* ctx, const pbf_params* p);
+int pbf_get_params(const pbf_ctx* ctx, pbf_params* p);
+
+/* Host AoS float3 state in; x* = x (particles.h:184-199).  v may be NULL (zero). */
+int pbf_upload(pbf_ctx* ctx, const float* x_aos, const float* v_aos, size_t n);
+/* Download in the reference's particle order; any pointer may be NULL. */
+int pbf_download(pbf_ctx* ctx, float* x_aos, float* v_aos, float* rho, float* lambda);
+size_t pbf_count(const pbf_ctx* ctx);
+
+/* Per-array access in the reference's particle order (parity and tests). */
+#define PBF_ARRAY_POSITIONS 0
+#define PBF_ARRAY_POSITION_STARS 1
+#define PBF_ARRAY_VELOCITIES 2
+#define PBF_ARRAY_SCRATCH 3      /* Vec scratch: dp, vorticity or color field */
+#define PBF_ARRAY_DENSITIES 4    /* scalar */
+#define PBF_ARRAY_LAMBDAS 5      /* scalar */
+int pbf_get_array(pbf_ctx* ctx, int which, float* host_out);
+int pbf_set_array(pbf_ctx* ctx, int which, const float* host_in);
+
+/* ---- stages: one per sim::Particles method, same span semantics ---- */
+int pbf_apply_external_forces(pbf_ctx* ctx, size_t b, size_t e);      /* particles.h:263-270 */
+int pbf_predict_positions(pbf_ctx* ctx, size_t b, size_t e);          /* particles.h:275-287 */
+int pbf_find_neighbors(pbf_ctx* ctx, size_t bin_b, size_t bin_e,
+                       size_t fill_b, size_t fill_e);                  /* particles.h:256-258 */
+int pbf_compute_densities(pbf_ctx* ctx, size_t b, size_t e);          /* particles.h:292-313 */
+int pbf_compute_pressure_lambdas(pbf_ctx* ctx, size_t b, size_t e);   /* particles.h:318-342 */
+int pbf_compute_pressure_dps(pbf_ctx* ctx, size_t b, size_t e, int substep); /* 348-358 */
+int pbf_update_position_stars(pbf_ctx* ctx, size_t b, size_t e);      /* particles.h:363-370 */
+int pbf_update_velocities(pbf_ctx* ctx, size_t b, size_t e);          /* particles.h:375-385 */
+int pbf_apply_surface_tension(pbf_ctx* ctx, size_t color_b, size_t color_e,
+                              size_t st_b, size_t st_e);               /* particles.h:400-431 */
+int pbf_apply_viscosity(pbf_ctx* ctx, size_t b, size_t e);            /* particles.h:436-447 */
+int pbf_compute_vorticity(pbf_ctx* ctx, size_t b, size_t e);          /* particles.h:452-466 */
+int pbf_apply_vorticity(pbf_ctx* ctx, size_t b, size_t e);            /* particles.h:471-487 */
+int pbf_update_positions(pbf_ctx* ctx, size_t b, size_t e);           /* particles.h:390-394 */
+
+/* The whole step of Simulation/Source/main.cpp:71-124 (single rank), fused
+ * and captured once as a CUDA graph per nsteps, then replayed. */
+int pbf_step(pbf_ctx* ctx, int nsteps);
+
+/* Parity exports in the reference's index space (synchronous):
+ *  idx   [N][cap] neighbor indices, entries past count set to -1 (neighbors.h:41-44)
+ *  count [N]
+ *  sorted_ids [N]   particle ids in sorted-bin order (neighbors.h:130-132)
+ *  sorted_keys [N]  bin id of each sorted entry
+ *  bin_begin/bin_end [B]  lower/upper bound of every bin (neighbors.h:137-148)
+ * Any pointer may be NULL. */
+int pbf_get_neighbors(pbf_ctx* ctx, int32_t* idx, int32_t* count);
+int pbf_get_bins(pbf_ctx* ctx, uint32_t* sorted_keys, uint32_t* sorted_ids,
+                 uint32_t* bin_begin, uint32_t* bin_end);
+int64_t pbf_num_bins(const pbf_ctx* ctx);
+
+int pbf_stats(pbf_ctx* ctx, pbf_stats_t* out);
+
+/* Device synchronisation of the context stream. */
+int pbf_sync(pbf_ctx* ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that order their
+ * own work or CUDA events after the context's kernels. */
+int pbf_get_stream(pbf_ctx* ctx, void** stream_out);
+
+/* ---- instrumentation ---- */
+/* Per-kernel device time: with timing on, pbf_step records a CUDA event
+ * around every kernel of every step on the context stream (inside the graph).
+ * pbf_kernel_times returns, per kernel family, launches and total ms since
+ * the last reset.  names[i] points to static strings. */
+int pbf_set_timing(pbf_ctx* ctx, int on);
+int pbf_kernel_times(pbf_ctx* ctx, int max_kinds, const char** names, int64_t* launches,
+                     double* total_ms, int* n_kinds);
+int pbf_reset_timing(pbf_ctx* ctx);
+/* Number of kernel launches one pbf_step(ctx, 1) issues. */
+int pbf_launches_per_step(pbf_ctx* ctx, int64_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PBF_B200_H */

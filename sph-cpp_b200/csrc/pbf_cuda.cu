@@ -1,0 +1,1599 @@
+// libpbf_b200: the position-based-fluids step of AdamSimpson/SPH-CPP
+// (Simulation/Source/particles.h, neighbors.h; stage order main.cpp:71-124)
+// as hand-written sm_100a kernels behind the C ABI of include/pbf.h.
+//
+// Data layout in HBM (capacity C particles, all 16-byte aligned float4 SoA):
+//   home buffers, persistent between steps, in the order of the last cell sort
+//     posH  (x, -)     pstH (x*, -)     velH (v, rho)     scrH (scratch Vec, |.|)
+//     lamH  float      origH uint32 (reference particle index of each slot)
+//   working buffers in the current step's sorted order
+//     posS, pstS, velS, origS, velT, xl = (x*, lambda) or (x*, |omega|)
+//   grid:   cell_count[B], cell_start[B+1] (begin/end of every bin),
+//           key/rank per particle, pairs[C] = (reference index << 32 | slot)
+//   lists:  nbr[cap][C] int32 slot indices (column-major: one warp reads one
+//           128-byte line per list entry), cnt[C]
+//
+// One step (pbf_step) is one CUDA graph of:
+//   memset counts -> ext+predict+hash+histogram -> 3-pass scan -> scatter ->
+//   per-cell stable fix-up -> reorder -> fill lists ->
+//   K x [density+lambda, delta-p+x* update (+ velocity on the last)] ->
+//   viscosity -> vorticity -> vorticity apply -> viscosity + x = x*.
+// Particles are kept in cell order between steps, so neighbours of a warp's
+// particles sit in a few contiguous slot ranges (L1/L2 reuse); the reference
+// index of every slot (origH) maps results back for downloads and parity.
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cmath>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/pbf.h"
+#include "pbf_internal.h"
+#include "pbf_kernels.cuh"
+
+using pbf::Dev;
+
+namespace {
+
+constexpr int kBlock = 256;
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+inline int blocks_for(size_t n, int b = kBlock) { return (int)((n + b - 1) / b); }
+
+// ============================================================================
+// Kernels
+// ============================================================================
+
+// Upload: AoS float3 host layout -> float4 home buffers, identity order.
+__global__ void k_upload(int n, const float* __restrict__ x, const float* __restrict__ v,
+                         float4* posH, float4* pstH, float4* velH, float4* scrH, float* lamH,
+                         uint32_t* origH) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 p = make_float4(x[3 * i], x[3 * i + 1], x[3 * i + 2], 0.0f);
+  posH[i] = p;
+  pstH[i] = p;
+  velH[i] = v ? make_float4(v[3 * i], v[3 * i + 1], v[3 * i + 2], 0.0f) : make_float4(0.f, 0.f, 0.f, 0.f);
+  scrH[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  lamH[i] = 0.0f;
+  origH[i] = (uint32_t)i;
+}
+
+// Home slot order -> reference order, AoS float3.
+__global__ void k_unpermute_vec(int n, const float4* __restrict__ src, const uint32_t* __restrict__ orig,
+                                float* dst) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  const float4 v = src[b];
+  const uint32_t o = orig[b];
+  dst[3 * (size_t)o] = v.x;
+  dst[3 * (size_t)o + 1] = v.y;
+  dst[3 * (size_t)o + 2] = v.z;
+}
+
+// component 3 of a float4 array, or a float array, -> reference order
+__global__ void k_unpermute_w(int n, const float4* __restrict__ src4, const float* __restrict__ src1,
+                              const uint32_t* __restrict__ orig, float* dst) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  dst[orig[b]] = src4 ? src4[b].w : src1[b];
+}
+
+// reference order AoS float3 -> home slot order (w kept)
+__global__ void k_permute_vec_in(int n, const float* __restrict__ src, const uint32_t* __restrict__ orig,
+                                 float4* dst) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  const size_t o = orig[b];
+  float4 d = dst[b];
+  d.x = src[3 * o];
+  d.y = src[3 * o + 1];
+  d.z = src[3 * o + 2];
+  dst[b] = d;
+}
+
+__global__ void k_permute_w_in(int n, const float* __restrict__ src, const uint32_t* __restrict__ orig,
+                               float4* dst4, float* dst1) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  const float v = src[orig[b]];
+  if (dst4) dst4[b].w = v; else dst1[b] = v;
+}
+
+// apply_external_forces (particles.h:263-270)
+__global__ void k_external(Dev P, int n, float4* vel) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n) return;
+  vel[a].y = pbf::xadd(vel[a].y, P.gdt);
+}
+
+// predict_positions (particles.h:275-287): x* = BC(x + v*dt)
+__device__ __forceinline__ float3 predict(const Dev& P, float4 x, float4 v) {
+  float3 s;
+  s.x = pbf::xadd(x.x, pbf::xmul(v.x, P.dt));
+  s.y = pbf::xadd(x.y, pbf::xmul(v.y, P.dt));
+  s.z = pbf::xadd(x.z, pbf::xmul(v.z, P.dt));
+  return pbf::boundary(P, s);
+}
+
+__global__ void k_predict(Dev P, int n, const float4* __restrict__ pos, const float4* __restrict__ vel,
+                          float4* pst) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n) return;
+  const float3 s = predict(P, pos[a], vel[a]);
+  pst[a] = make_float4(s.x, s.y, s.z, 0.0f);
+}
+
+// calculate_bins (neighbors.h:120-125) + bin histogram with per-particle rank.
+__global__ void k_hash(Dev P, int n, const float4* __restrict__ pst, uint32_t* key, uint32_t* rank,
+                       uint32_t* cell_count, uint32_t* err) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n) return;
+  const float4 s = pst[a];
+  uint32_t k;
+  if (!pbf::bin_of(P, s.x, s.y, s.z, k)) atomicOr(err, PBF_FLAG_KEY_RANGE);
+  key[a] = k;
+  rank[a] = atomicAdd(&cell_count[k], 1u);
+}
+
+// Fused apply_external_forces + predict_positions + calculate_bins + histogram.
+__global__ void k_ext_predict_hash(Dev P, int n, const float4* __restrict__ pos, float4* vel,
+                                   float4* pst, uint32_t* key, uint32_t* rank, uint32_t* cell_count,
+                                   uint32_t* err) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n) return;
+  float4 v = vel[a];
+  v.y = pbf::xadd(v.y, P.gdt);
+  vel[a] = v;
+  const float3 s = predict(P, pos[a], v);
+  pst[a] = make_float4(s.x, s.y, s.z, 0.0f);
+  uint32_t k;
+  if (!pbf::bin_of(P, s.x, s.y, s.z, k)) atomicOr(err, PBF_FLAG_KEY_RANGE);
+  key[a] = k;
+  rank[a] = atomicAdd(&cell_count[k], 1u);
+}
+
+// ---- exclusive scan of cell_count[0..m-1] (+ total at [m]) -> cell_start ----
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* warp_sums,
+                                                         uint32_t& total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_sums[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = blockDim.x >> 5;
+    uint32_t w = lane < nw ? warp_sums[lane] : 0u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < nw) warp_sums[lane] = w;
+  }
+  __syncthreads();
+  const uint32_t warp_prefix = wid > 0 ? warp_sums[wid - 1] : 0u;
+  total = warp_sums[(blockDim.x >> 5) - 1];
+  return warp_prefix + x - v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const uint32_t* __restrict__ in, int m,
+                                                              uint32_t* partial) {
+  __shared__ uint32_t ws[32];
+  const size_t base = (size_t)blockIdx.x * kScanTile + (size_t)threadIdx.x * kScanItems;
+  uint32_t s = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i)
+    if (base + i < (size_t)m) s += in[base + i];
+  uint32_t total;
+  block_exclusive_scan(s, ws, total);
+  if (threadIdx.x == 0) partial[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_partials(uint32_t* partial, int np) {
+  __shared__ uint32_t ws[32];
+  __shared__ uint32_t carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < np; base += kScanThreads) {
+    const int i = base + threadIdx.x;
+    const uint32_t v = i < np ? partial[i] : 0u;
+    uint32_t total;
+    const uint32_t ex = block_exclusive_scan(v, ws, total);
+    const uint32_t c = carry;
+    if (i < np) partial[i] = ex + c;
+    __syncthreads();
+    if (threadIdx.x == 0) carry = c + total;
+    __syncthreads();
+  }
+}
+
+// out[0..m] (m+1 entries): exclusive prefix of in[0..m-1], out[m] = total.
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply(const uint32_t* __restrict__ in, int m,
+                                                             const uint32_t* __restrict__ partial,
+                                                             uint32_t* out) {
+  __shared__ uint32_t ws[32];
+  const size_t base = (size_t)blockIdx.x * kScanTile + (size_t)threadIdx.x * kScanItems;
+  uint32_t v[kScanItems];
+  uint32_t s = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    v[i] = base + i < (size_t)m ? in[base + i] : 0u;
+    s += v[i];
+  }
+  uint32_t total;
+  uint32_t run = block_exclusive_scan(s, ws, total) + partial[blockIdx.x];
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    if (base + i <= (size_t)m) out[base + i] = run;
+    run += v[i];
+  }
+}
+
+// Stable counting-sort scatter: slot = start(bin) + rank; the fix-up below
+// orders every bin by reference index, which makes the whole permutation equal
+// to the reference's stable sort_by_key (neighbors.h:130-132).
+__global__ void k_scatter(int n, const uint32_t* __restrict__ key, const uint32_t* __restrict__ rank,
+                          const uint32_t* __restrict__ cell_start, const uint32_t* __restrict__ orig,
+                          unsigned long long* pairs) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n) return;
+  const uint32_t slot = cell_start[key[a]] + rank[a];
+  pairs[slot] = ((unsigned long long)orig[a] << 32) | (unsigned long long)a;
+}
+
+__global__ void k_cell_sort(int nbins, const uint32_t* __restrict__ cell_start, unsigned long long* pairs) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nbins) return;
+  const uint32_t b0 = cell_start[c], b1 = cell_start[c + 1];
+  if (b1 - b0 < 2) return;
+  for (uint32_t i = b0 + 1; i < b1; ++i) {
+    const unsigned long long v = pairs[i];
+    uint32_t j = i;
+    while (j > b0 && pairs[j - 1] > v) {
+      pairs[j] = pairs[j - 1];
+      --j;
+    }
+    pairs[j] = v;
+  }
+}
+
+// Gather the state into sorted order.  full = also lambda and scratch (the
+// per-stage path, where every reference array must follow its particle).
+template <bool FULL>
+__global__ void k_reorder(int n, const unsigned long long* __restrict__ pairs, const uint32_t* __restrict__ key,
+                          const float4* __restrict__ posH, const float4* __restrict__ pstH,
+                          const float4* __restrict__ velH, const float4* __restrict__ scrH,
+                          const float* __restrict__ lamH, float4* posS, float4* pstS, float4* velS,
+                          float4* scrS, float* lamS, uint32_t* origS, uint32_t* keyH) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  const unsigned long long pr = pairs[b];
+  const uint32_t a = (uint32_t)(pr & 0xffffffffull);
+  origS[b] = (uint32_t)(pr >> 32);
+  keyH[b] = key[a];
+  posS[b] = posH[a];
+  pstS[b] = pstH[a];
+  velS[b] = velH[a];
+  if (FULL) {
+    scrS[b] = scrH[a];
+    lamS[b] = lamH[a];
+  }
+}
+
+// fill_neighbors (neighbors.h:197-230) over slots in sorted order: 27 bins in
+// the reference's order (x offset outer, z inner, float re-hash of
+// coord + i*s), candidates of a bin in ascending reference index, strict
+// d^2 < s^2, self skipped, first `cap` kept.
+__global__ void __launch_bounds__(kBlock) k_fill(Dev P, int n, size_t stride, const float4* __restrict__ pst,
+                                                 const uint32_t* __restrict__ cell_start, int32_t* nbr,
+                                                 int32_t* cnt, uint32_t* err) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  const float4 xp = pst[b];
+  int count = 0;
+  const int cap = P.cap;
+  for (int i = -1; i < 2 && count < cap; i++) {
+    const float cx = pbf::xadd(xp.x, pbf::xmul((float)i, P.s));
+    for (int j = -1; j < 2 && count < cap; j++) {
+      const float cy = pbf::xadd(xp.y, pbf::xmul((float)j, P.s));
+      for (int k = -1; k < 2 && count < cap; k++) {
+        const float cz = pbf::xadd(xp.z, pbf::xmul((float)k, P.s));
+        uint32_t nb;
+        if (!pbf::bin_of(P, cx, cy, cz, nb)) {
+          atomicOr(err, PBF_FLAG_KEY_RANGE);
+          continue;
+        }
+        const uint32_t q0 = cell_start[nb], q1 = cell_start[nb + 1];
+        for (uint32_t q = q0; q < q1; ++q) {
+          if (q == (uint32_t)b) continue;
+          const float4 xq = pst[q];
+          const float d2 = pbf::mag2<true>(pbf::xsub(xp.x, xq.x), pbf::xsub(xp.y, xq.y), pbf::xsub(xp.z, xq.z));
+          if (d2 < P.s2) {
+            nbr[(size_t)count * stride + b] = (int32_t)q;
+            if (++count >= cap) break;
+          }
+        }
+      }
+    }
+  }
+  cnt[b] = count;
+}
+
+// ---- density (particles.h:292-313) ----
+// Per-stage form: writes rho into vel.w and, when a neighbour coincides, the
+// nudged x* back (the reference writes position_stars_[p] in place).
+template <bool X>
+__global__ void __launch_bounds__(kBlock) k_density(Dev P, int n, size_t stride, const int32_t* __restrict__ nbr,
+                                                    const int32_t* __restrict__ cnt, float4* pst, float4* vel) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  float4 xp = pst[b];
+  const int c = cnt[b];
+  float rho = pbf::M<X>(P.m, P.W0);
+  bool nudged = false;
+  for (int k = 0; k < c; ++k) {
+    const int q = nbr[(size_t)k * stride + b];
+    const float4 xq = pst[q];
+    float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
+    float rm = pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz));
+    if ((double)rm < 0.00000001) {
+      const float4 v = vel[b];
+      xp.x = pbf::xsub(xp.x, pbf::xdiv(pbf::xmul(v.x, P.dt), 50.0f));
+      xp.y = pbf::xsub(xp.y, pbf::xdiv(pbf::xmul(v.y, P.dt), 50.0f));
+      xp.z = pbf::xsub(xp.z, pbf::xdiv(pbf::xmul(v.z, P.dt), 50.0f));
+      nudged = true;
+      rx = pbf::S<X>(xp.x, xq.x); ry = pbf::S<X>(xp.y, xq.y); rz = pbf::S<X>(xp.z, xq.z);
+      rm = pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz));
+    }
+    rho = pbf::A<X>(rho, pbf::M<X>(P.m, pbf::poly6<X>(P, rm)));
+  }
+  vel[b].w = rho;
+  if (nudged) pst[b] = xp;
+}
+
+// compute_pressure_lambdas (particles.h:318-342), per-stage form.
+template <bool X>
+__device__ __forceinline__ void lambda_terms(const Dev& P, float rx, float ry, float rz, float rm, float3& sg,
+                                             float& sumC) {
+  const float3 dw = pbf::del_spikey<X>(P, rx, ry, rz, rm);
+  const float gx = pbf::M<X>(P.neg_inv_rho0, dw.x), gy = pbf::M<X>(P.neg_inv_rho0, dw.y),
+              gz = pbf::M<X>(P.neg_inv_rho0, dw.z);
+  sg.x = pbf::S<X>(sg.x, gx);
+  sg.y = pbf::S<X>(sg.y, gy);
+  sg.z = pbf::S<X>(sg.z, gz);
+  sumC = pbf::A<X>(sumC, pbf::mag2<X>(gx, gy, gz));
+}
+
+template <bool X>
+__device__ __forceinline__ float lambda_of(const Dev& P, float rho, float3 sg, float sumC) {
+  const float constraint = pbf::S<X>(pbf::D<X>(rho, P.rho0), 1.0f);
+  const float Cp = constraint < 0.0f ? 0.0f : constraint;
+  sumC = pbf::A<X>(sumC, pbf::mag2<X>(sg.x, sg.y, sg.z));
+  return pbf::D<X>(-Cp, pbf::A<X>(sumC, P.lambda_eps));
+}
+
+template <bool X>
+__global__ void __launch_bounds__(kBlock) k_lambda(Dev P, int n, size_t stride, const int32_t* __restrict__ nbr,
+                                                   const int32_t* __restrict__ cnt, const float4* __restrict__ pst,
+                                                   const float4* __restrict__ vel, float* lam) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  const float4 xp = pst[b];
+  const int c = cnt[b];
+  float3 sg = make_float3(0.f, 0.f, 0.f);
+  float sumC = 0.0f;
+  for (int k = 0; k < c; ++k) {
+    const float4 xq = pst[nbr[(size_t)k * stride + b]];
+    const float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
+    lambda_terms<X>(P, rx, ry, rz, pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz)), sg, sumC);
+  }
+  lam[b] = lambda_of<X>(P, vel[b].w, sg, sumC);
+}
+
+// Fused density + lambda: one neighbour pass computes rho_p and the gradient
+// sums (lambda needs only its own density).  Writes xl = (x*, lambda) for the
+// delta-p gather, rho into vel.w and lambda into the home lambda array.  If a
+// neighbour coincides (particles.h:303-305) the nudged x* travels in xl and the
+// gradient sums are recomputed with it.
+template <bool X>
+__global__ void __launch_bounds__(kBlock) k_density_lambda(Dev P, int n, size_t stride,
+                                                           const int32_t* __restrict__ nbr,
+                                                           const int32_t* __restrict__ cnt,
+                                                           const float4* __restrict__ pst, float4* xl,
+                                                           float4* vel, float* lam) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  float4 xp = pst[b];
+  const int c = cnt[b];
+  float rho = pbf::M<X>(P.m, P.W0);
+  float3 sg = make_float3(0.f, 0.f, 0.f);
+  float sumC = 0.0f;
+  bool nudged = false;
+  for (int k = 0; k < c; ++k) {
+    const float4 xq = pst[nbr[(size_t)k * stride + b]];
+    float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
+    float rm = pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz));
+    if ((double)rm < 0.00000001) {
+      const float4 v = vel[b];
+      xp.x = pbf::xsub(xp.x, pbf::xdiv(pbf::xmul(v.x, P.dt), 50.0f));
+      xp.y = pbf::xsub(xp.y, pbf::xdiv(pbf::xmul(v.y, P.dt), 50.0f));
+      xp.z = pbf::xsub(xp.z, pbf::xdiv(pbf::xmul(v.z, P.dt), 50.0f));
+      nudged = true;
+      rx = pbf::S<X>(xp.x, xq.x); ry = pbf::S<X>(xp.y, xq.y); rz = pbf::S<X>(xp.z, xq.z);
+      rm = pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz));
+    }
+    rho = pbf::A<X>(rho, pbf::M<X>(P.m, pbf::poly6<X>(P, rm)));
+    lambda_terms<X>(P, rx, ry, rz, rm, sg, sumC);
+  }
+  if (nudged) {
+    sg = make_float3(0.f, 0.f, 0.f);
+    sumC = 0.0f;
+    for (int k = 0; k < c; ++k) {
+      const float4 xq = pst[nbr[(size_t)k * stride + b]];
+      const float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
+      lambda_terms<X>(P, rx, ry, rz, pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz)), sg, sumC);
+    }
+  }
+  const float l = lambda_of<X>(P, rho, sg, sumC);
+  xl[b] = make_float4(xp.x, xp.y, xp.z, l);
+  vel[b].w = rho;
+  lam[b] = l;
+}
+
+// compute_pressure_dps (particles.h:348-358) summand; s_corr optional.
+template <bool X, bool SCORR>
+__device__ __forceinline__ void dp_term(const Dev& P, float lp, float lq, float rx, float ry, float rz, float rm,
+                                        float3& dp) {
+  float l = pbf::A<X>(lp, lq);
+  if (SCORR) {
+    const float w = pbf::poly6<X>(P, rm);
+    l = l - P.scorr_k * powf(w * P.inv_wdq, P.scorr_n);
+  }
+  const float3 dw = pbf::del_spikey<X>(P, rx, ry, rz, rm);
+  dp.x = pbf::A<X>(dp.x, pbf::M<X>(l, dw.x));
+  dp.y = pbf::A<X>(dp.y, pbf::M<X>(l, dw.y));
+  dp.z = pbf::A<X>(dp.z, pbf::M<X>(l, dw.z));
+}
+
+// Per-stage delta-p -> scratch.
+template <bool X, bool SCORR>
+__global__ void __launch_bounds__(kBlock) k_dp(Dev P, int n, size_t stride, const int32_t* __restrict__ nbr,
+                                               const int32_t* __restrict__ cnt, const float4* __restrict__ pst,
+                                               const float* __restrict__ lam, float4* scr) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  const float4 xp = pst[b];
+  const float lp = lam[b];
+  const int c = cnt[b];
+  float3 dp = make_float3(0.f, 0.f, 0.f);
+  for (int k = 0; k < c; ++k) {
+    const int q = nbr[(size_t)k * stride + b];
+    const float4 xq = pst[q];
+    const float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
+    dp_term<X, SCORR>(P, lp, lam[q], rx, ry, rz, pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz)), dp);
+  }
+  scr[b] = make_float4(pbf::M<X>(P.inv_rho0, dp.x), pbf::M<X>(P.inv_rho0, dp.y), pbf::M<X>(P.inv_rho0, dp.z), 0.0f);
+}
+
+// update_position_stars (particles.h:363-370), per-stage.
+__global__ void k_update_xs(Dev P, int n, float4* pst, const float4* __restrict__ scr) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  const float4 x = pst[b], d = scr[b];
+  const float3 s = pbf::boundary(P, make_float3(pbf::xadd(x.x, d.x), pbf::xadd(x.y, d.y), pbf::xadd(x.z, d.z)));
+  pst[b] = make_float4(s.x, s.y, s.z, 0.0f);
+}
+
+// update_velocities (particles.h:375-385), always exact (per-particle).
+__device__ __forceinline__ float3 velocity_of(const Dev& P, float4 xs, float4 x) {
+  float3 v = make_float3(pbf::xdiv(pbf::xsub(xs.x, x.x), P.dt), pbf::xdiv(pbf::xsub(xs.y, x.y), P.dt),
+                         pbf::xdiv(pbf::xsub(xs.z, x.z), P.dt));
+  if ((double)pbf::mag2<true>(v.x, v.y, v.z) < P.vthr) v = make_float3(0.f, 0.f, 0.f);
+  return v;
+}
+
+__global__ void k_update_v(Dev P, int n, const float4* __restrict__ pst, const float4* __restrict__ pos,
+                           float4* vel) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  const float3 v = velocity_of(P, pst[b], pos[b]);
+  vel[b] = make_float4(v.x, v.y, v.z, vel[b].w);
+}
+
+// Fused delta-p + x* update (+ velocity update on the last iteration): reads
+// (x*, lambda) of neighbours from xl, writes the new x* (Jacobi: nobody reads
+// pst in this kernel).
+template <bool X, bool SCORR, bool LAST>
+__global__ void __launch_bounds__(kBlock) k_dp_update(Dev P, int n, size_t stride, const int32_t* __restrict__ nbr,
+                                                      const int32_t* __restrict__ cnt, const float4* __restrict__ xl,
+                                                      float4* pst, const float4* __restrict__ pos, float4* vel) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  const float4 xp = xl[b];
+  const int c = cnt[b];
+  float3 dp = make_float3(0.f, 0.f, 0.f);
+  for (int k = 0; k < c; ++k) {
+    const float4 xq = xl[nbr[(size_t)k * stride + b]];
+    const float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
+    dp_term<X, SCORR>(P, xp.w, xq.w, rx, ry, rz, pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz)), dp);
+  }
+  const float dx = pbf::M<X>(P.inv_rho0, dp.x), dy = pbf::M<X>(P.inv_rho0, dp.y), dz = pbf::M<X>(P.inv_rho0, dp.z);
+  const float3 s = pbf::boundary(P, make_float3(pbf::xadd(xp.x, dx), pbf::xadd(xp.y, dy), pbf::xadd(xp.z, dz)));
+  const float4 ns = make_float4(s.x, s.y, s.z, 0.0f);
+  pst[b] = ns;
+  if (LAST) {
+    const float3 v = velocity_of(P, ns, pos[b]);
+    vel[b] = make_float4(v.x, v.y, v.z, vel[b].w);
+  }
+}
+
+// apply_surface_tension (particles.h:400-431): colour-field pass ...
+template <bool X>
+__global__ void __launch_bounds__(kBlock) k_color(Dev P, int n, size_t stride, const int32_t* __restrict__ nbr,
+                                                  const int32_t* __restrict__ cnt, const float4* __restrict__ pst,
+                                                  const float4* __restrict__ vel, float4* scr) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  const float4 xp = pst[b];
+  const int c = cnt[b];
+  float3 col = make_float3(0.f, 0.f, 0.f);
+  for (int k = 0; k < c; ++k) {
+    const int q = nbr[(size_t)k * stride + b];
+    const float4 xq = pst[q];
+    const float rq = vel[q].w;
+    const float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
+    const float3 dw = pbf::del_spikey<X>(P, rx, ry, rz, pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz)));
+    col.x = pbf::A<X>(col.x, pbf::D<X>(dw.x, rq));
+    col.y = pbf::A<X>(col.y, pbf::D<X>(dw.y, rq));
+    col.z = pbf::A<X>(col.z, pbf::D<X>(dw.z, rq));
+  }
+  scr[b] = make_float4(pbf::M<X>(P.h, col.x), pbf::M<X>(P.h, col.y), pbf::M<X>(P.h, col.z), 0.0f);
+}
+
+// ... then the cohesion + curvature force pass (always exact: rare path).
+__global__ void __launch_bounds__(kBlock) k_surface(Dev P, int n, size_t stride, const int32_t* __restrict__ nbr,
+                                                    const int32_t* __restrict__ cnt, const float4* __restrict__ pst,
+                                                    const float4* __restrict__ scr, float4* vel) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  const float4 xp = pst[b], sp = scr[b];
+  const float rp = vel[b].w;
+  const int c = cnt[b];
+  const float ng = -P.gamma;
+  float3 f = make_float3(0.f, 0.f, 0.f);
+  for (int k = 0; k < c; ++k) {
+    const int q = nbr[(size_t)k * stride + b];
+    const float4 xq = pst[q], sq = scr[q];
+    const float rq = vel[q].w;
+    const float rx = pbf::xsub(xp.x, xq.x), ry = pbf::xsub(xp.y, xq.y), rz = pbf::xsub(xp.z, xq.z);
+    float rm = __fsqrt_rn(pbf::mag2<true>(rx, ry, rz));
+    if ((double)rm < P.h_eps) rm = (float)P.h_eps;
+    const float cs = pbf::xmul(ng, pbf::c_spline<true>(P, rm));
+    const float K = (float)__ddiv_rn(__dmul_rn(2.0, (double)P.rho0), (double)pbf::xadd(rp, rq));
+    f.x = pbf::xadd(f.x, pbf::xmul(K, pbf::xadd(pbf::xdiv(pbf::xmul(cs, rx), rm), pbf::xmul(ng, pbf::xsub(sp.x, sq.x)))));
+    f.y = pbf::xadd(f.y, pbf::xmul(K, pbf::xadd(pbf::xdiv(pbf::xmul(cs, ry), rm), pbf::xmul(ng, pbf::xsub(sp.y, sq.y)))));
+    f.z = pbf::xadd(f.z, pbf::xmul(K, pbf::xadd(pbf::xdiv(pbf::xmul(cs, rz), rm), pbf::xmul(ng, pbf::xsub(sp.z, sq.z)))));
+  }
+  float4 v = vel[b];
+  v.x = pbf::xadd(v.x, pbf::xmul(pbf::xdiv(f.x, rp), P.dt));
+  v.y = pbf::xadd(v.y, pbf::xmul(pbf::xdiv(f.y, rp), P.dt));
+  v.z = pbf::xadd(v.z, pbf::xmul(pbf::xdiv(f.z, rp), P.dt));
+  vel[b] = v;
+}
+
+// XSPH viscosity (particles.h:436-447), Jacobi: reads vin, writes vout.
+// FINAL also performs update_positions (particles.h:390-394) and writes the
+// step's results into the home buffers.
+template <bool X, bool FINAL>
+__global__ void __launch_bounds__(kBlock) k_viscosity(Dev P, int n, size_t stride, const int32_t* __restrict__ nbr,
+                                                      const int32_t* __restrict__ cnt, const float4* __restrict__ pst,
+                                                      const float4* __restrict__ vin, float4* vout, float4* posH,
+                                                      float4* pstH, const uint32_t* __restrict__ origS,
+                                                      uint32_t* origH) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  const float4 xp = pst[b], vp = vin[b];
+  const int c = cnt[b];
+  float3 dv = make_float3(0.f, 0.f, 0.f);
+  for (int k = 0; k < c; ++k) {
+    const int q = nbr[(size_t)k * stride + b];
+    const float4 xq = pst[q], vq = vin[q];
+    const float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
+    const float w = pbf::poly6<X>(P, pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz)));
+    if (X) {
+      dv.x = pbf::xadd(dv.x, pbf::xdiv(pbf::xmul(pbf::xsub(vq.x, vp.x), w), vq.w));
+      dv.y = pbf::xadd(dv.y, pbf::xdiv(pbf::xmul(pbf::xsub(vq.y, vp.y), w), vq.w));
+      dv.z = pbf::xadd(dv.z, pbf::xdiv(pbf::xmul(pbf::xsub(vq.z, vp.z), w), vq.w));
+    } else {
+      const float wr = __fdividef(w, vq.w);
+      dv.x = fmaf(vq.x - vp.x, wr, dv.x);
+      dv.y = fmaf(vq.y - vp.y, wr, dv.y);
+      dv.z = fmaf(vq.z - vp.z, wr, dv.z);
+    }
+  }
+  vout[b] = make_float4(pbf::A<X>(vp.x, pbf::M<X>(P.visc_c, dv.x)), pbf::A<X>(vp.y, pbf::M<X>(P.visc_c, dv.y)),
+                        pbf::A<X>(vp.z, pbf::M<X>(P.visc_c, dv.z)), vp.w);
+  if (FINAL) {
+    posH[b] = xp;
+    pstH[b] = xp;
+    origH[b] = origS[b];
+  }
+}
+
+// compute_vorticity (particles.h:452-466): omega into scratch (w = |omega|,
+// computed as magnitude() would) and (x*, |omega|) into xl for the apply pass.
+template <bool X>
+__global__ void __launch_bounds__(kBlock) k_vorticity(Dev P, int n, size_t stride, const int32_t* __restrict__ nbr,
+                                                      const int32_t* __restrict__ cnt, const float4* __restrict__ pst,
+                                                      const float4* __restrict__ vel, float4* scr, float4* xl) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  const float4 xp = pst[b], vp = vel[b];
+  const int c = cnt[b];
+  float3 w = make_float3(0.f, 0.f, 0.f);
+  for (int k = 0; k < c; ++k) {
+    const int q = nbr[(size_t)k * stride + b];
+    const float4 xq = pst[q], vq = vel[q];
+    const float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
+    const float3 d = pbf::del_spikey<X>(P, rx, ry, rz, pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz)));
+    const float ax = pbf::S<X>(vq.x, vp.x), ay = pbf::S<X>(vq.y, vp.y), az = pbf::S<X>(vq.z, vp.z);
+    // cross(v_diff, del) (vec.h:622-630)
+    w.x = pbf::A<X>(w.x, pbf::S<X>(pbf::M<X>(ay, d.z), pbf::M<X>(az, d.y)));
+    w.y = pbf::A<X>(w.y, pbf::S<X>(pbf::M<X>(az, d.x), pbf::M<X>(ax, d.z)));
+    w.z = pbf::A<X>(w.z, pbf::S<X>(pbf::M<X>(ax, d.y), pbf::M<X>(ay, d.x)));
+  }
+  const float wm = __fsqrt_rn(pbf::mag2<true>(w.x, w.y, w.z));
+  scr[b] = make_float4(w.x, w.y, w.z, wm);
+  if (xl) xl[b] = make_float4(xp.x, xp.y, xp.z, wm);
+}
+
+// apply_vorticity (particles.h:471-487).  PACKED reads (x*, |omega|) of
+// neighbours from xl (one 16-byte load); otherwise from pst and scratch.
+template <bool X, bool PACKED>
+__global__ void __launch_bounds__(kBlock) k_apply_vorticity(Dev P, int n, size_t stride,
+                                                            const int32_t* __restrict__ nbr,
+                                                            const int32_t* __restrict__ cnt,
+                                                            const float4* __restrict__ xl,
+                                                            const float4* __restrict__ pst,
+                                                            const float4* __restrict__ scr, float4* vel) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  const float4 xp = PACKED ? xl[b] : pst[b];
+  const int c = cnt[b];
+  float3 eta = make_float3(0.f, 0.f, 0.f);
+  for (int k = 0; k < c; ++k) {
+    const int q = nbr[(size_t)k * stride + b];
+    float4 xq;
+    float vm;
+    if (PACKED) {
+      xq = xl[q];
+      vm = xq.w;
+    } else {
+      xq = pst[q];
+      const float4 sq = scr[q];
+      vm = __fsqrt_rn(pbf::mag2<true>(sq.x, sq.y, sq.z));
+    }
+    const float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
+    const float3 d = pbf::del_spikey<X>(P, rx, ry, rz, pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz)));
+    eta.x = pbf::A<X>(eta.x, pbf::M<X>(vm, d.x));
+    eta.y = pbf::A<X>(eta.y, pbf::M<X>(vm, d.y));
+    eta.z = pbf::A<X>(eta.z, pbf::M<X>(vm, d.z));
+  }
+  const float den = pbf::A<X>(pbf::SQ<X>(pbf::mag2<X>(eta.x, eta.y, eta.z)), FLT_EPSILON);
+  const float Nx = pbf::D<X>(eta.x, den), Ny = pbf::D<X>(eta.y, den), Nz = pbf::D<X>(eta.z, den);
+  const float4 wp = scr[b];
+  const float cx = pbf::S<X>(pbf::M<X>(Ny, wp.z), pbf::M<X>(Nz, wp.y));
+  const float cy = pbf::S<X>(pbf::M<X>(Nz, wp.x), pbf::M<X>(Nx, wp.z));
+  const float cz = pbf::S<X>(pbf::M<X>(Nx, wp.y), pbf::M<X>(Ny, wp.x));
+  float4 v = vel[b];
+  v.x = pbf::A<X>(v.x, pbf::M<X>(pbf::M<X>(cx, P.vort_eps), P.dt));
+  v.y = pbf::A<X>(v.y, pbf::M<X>(pbf::M<X>(cy, P.vort_eps), P.dt));
+  v.z = pbf::A<X>(v.z, pbf::M<X>(pbf::M<X>(cz, P.vort_eps), P.dt));
+  vel[b] = v;
+}
+
+// Residual statistics (no state change): density over the current lists,
+// clamped error, kinetic energy, centre of mass, list lengths.
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__global__ void __launch_bounds__(kBlock) k_stats(Dev P, int n, size_t stride, const int32_t* __restrict__ nbr,
+                                                  const int32_t* __restrict__ cnt, const float4* __restrict__ pst,
+                                                  const float4* __restrict__ pos, const float4* __restrict__ vel,
+                                                  double* acc, unsigned long long* maxerr,
+                                                  unsigned long long* hits) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  double e = 0.0, ke = 0.0, cx = 0.0, cy = 0.0, cz = 0.0, nn = 0.0;
+  if (b < n) {
+    const float4 xp = pst[b];
+    const int c = cnt[b];
+    float d = pbf::xmul(P.m, P.W0);
+    for (int k = 0; k < c; ++k) {
+      const float4 xq = pst[nbr[(size_t)k * stride + b]];
+      const float rx = pbf::xsub(xp.x, xq.x), ry = pbf::xsub(xp.y, xq.y), rz = pbf::xsub(xp.z, xq.z);
+      d = pbf::xadd(d, pbf::xmul(P.m, pbf::poly6<true>(P, __fsqrt_rn(pbf::mag2<true>(rx, ry, rz)))));
+    }
+    e = (double)d / (double)P.rho0 - 1.0;
+    if (e < 0.0) e = 0.0;
+    atomicMax(maxerr, (unsigned long long)__double_as_longlong(e));
+    const float4 v = vel[b];
+    ke = 0.5 * (double)P.m * ((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z);
+    const float4 x = pos[b];
+    cx = x.x; cy = x.y; cz = x.z;
+    nn = c;
+    if (c >= P.cap) atomicAdd(hits, 1ull);
+  }
+  e = warp_sum(e); ke = warp_sum(ke); cx = warp_sum(cx); cy = warp_sum(cy); cz = warp_sum(cz); nn = warp_sum(nn);
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&acc[0], e); atomicAdd(&acc[1], ke); atomicAdd(&acc[2], cx);
+    atomicAdd(&acc[3], cy); atomicAdd(&acc[4], cz); atomicAdd(&acc[5], nn);
+  }
+}
+
+// Neighbour lists in reference index space, [N][cap], -1 past count.
+__global__ void k_export_neighbors(int n, size_t stride, int cap, const int32_t* __restrict__ nbr,
+                                   const int32_t* __restrict__ cnt, const uint32_t* __restrict__ orig,
+                                   int32_t* idx_out, int32_t* cnt_out) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  const size_t o = orig[b];
+  const int c = cnt[b];
+  if (cnt_out) cnt_out[o] = c;
+  if (idx_out)
+    for (int k = 0; k < cap; ++k)
+      idx_out[o * cap + k] = k < c ? (int32_t)orig[nbr[(size_t)k * stride + b]] : -1;
+}
+
+}  // namespace
+
+// ============================================================================
+// Context
+// ============================================================================
+struct pbf_ctx {
+  pbf_params params{};
+  Dev dev{};
+  size_t capacity = 0, n = 0;
+  int64_t dims[3] = {0, 0, 0};
+  int nbins = 0, nscan_parts = 0;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool lists_valid = false;
+
+  float4 *posH = nullptr, *pstH = nullptr, *velH = nullptr, *scrH = nullptr;
+  float4 *posS = nullptr, *pstS = nullptr, *velS = nullptr, *scrS = nullptr, *xl = nullptr, *velT = nullptr;
+  float *lamH = nullptr, *lamS = nullptr;
+  uint32_t *origH = nullptr, *origS = nullptr, *key = nullptr, *rank = nullptr, *keyH = nullptr;
+  uint32_t *cell_count = nullptr, *cell_start = nullptr, *scan_part = nullptr, *err = nullptr;
+  unsigned long long* pairs = nullptr;
+  int32_t *nbr = nullptr, *cnt = nullptr;
+  float* stage = nullptr;  // 6*C floats: two AoS float3 staging areas
+  int32_t* stage_i = nullptr;  // neighbor export staging (C*cap + C)
+  double* acc = nullptr;
+  unsigned long long *maxerr = nullptr, *hits = nullptr;
+
+  std::map<int, cudaGraphExec_t> graphs;
+  std::vector<void*> allocations;
+
+  bool timing = false;
+  struct Mark {
+    const char* name;
+    cudaEvent_t start, stop;
+  };
+  std::vector<Mark> marks;
+  size_t marks_used = 0;
+  std::map<std::string, std::pair<int64_t, double>> times;
+  std::vector<std::string> time_order;
+
+  std::string error;
+};
+
+namespace {
+
+thread_local std::string g_create_error;
+
+int fail(pbf_ctx* c, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (c) c->error = buf; else g_create_error = buf;
+  return code;
+}
+
+#define CK(call)                                                                             \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return fail(ctx, PBF_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));        \
+  } while (0)
+
+int check_launch(pbf_ctx* ctx, const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(ctx, PBF_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+  return PBF_OK;
+}
+
+// Build the device constant block from the public parameters (all derived
+// constants are evaluated on the host in the reference's types).
+int make_dev(pbf_ctx* ctx, const pbf_params& p, Dev& d, int64_t dims[3]) {
+  if (!(p.time_step > 0.0f) || !(p.smoothing_radius > 0.0f) || !(p.neighbor_bin_spacing > 0.0f) ||
+      !(p.rest_density > 0.0f) || !(p.rest_mass > 0.0f))
+    return fail(ctx, PBF_ERR_PARAMS, "time_step, smoothing_radius, neighbor_bin_spacing, rest_density and "
+                                     "rest_mass must be > 0");
+  if (p.solve_steps < 0) return fail(ctx, PBF_ERR_PARAMS, "solve_steps must be >= 0");
+  if (p.neighbor_cap < 1 || p.neighbor_cap > 64)
+    return fail(ctx, PBF_ERR_PARAMS, "neighbor_cap must be in [1, 64], got %d", p.neighbor_cap);
+  const float s = p.neighbor_bin_spacing;
+  for (int a = 0; a < 3; ++a) {
+    if (!(p.boundary_max[a] > p.boundary_min[a]))
+      return fail(ctx, PBF_ERR_PARAMS, "boundary max must exceed min on every axis");
+    // The reference's bin hash casts floor((x+s)/s) to size_t, defined only
+    // for x >= -s; every clamped position and its +-s re-hash must land in
+    // the grid (neighbors.h:69-71, 109-114, 172-185).
+    if (p.boundary_min[a] < 0.0f)
+      return fail(ctx, PBF_ERR_PARAMS, "boundary min must be >= 0 (reference bin hash, neighbors.h:109-114)");
+    dims[a] = pbf::grid_dim(p.boundary_max[a] - p.boundary_min[a], s);
+    const float lo = (p.boundary_min[a] - s);
+    const float hi = (p.boundary_max[a] + s);
+    if (pbf::axis_bin(lo, s) < 0 || pbf::axis_bin(hi, s) > dims[a] - 1)
+      return fail(ctx, PBF_ERR_PARAMS,
+                  "axis %d: the reference grid (ceil(extent/s)+2 = %lld bins) does not cover the boundary "
+                  "and its +-s neighbour bins; a box with min 0 and max not a multiple of s does",
+                  a, (long long)dims[a]);
+  }
+  const double nb = (double)dims[0] * (double)dims[1] * (double)dims[2];
+  if (nb >= 2147483647.0) return fail(ctx, PBF_ERR_PARAMS, "grid of %.0f bins exceeds 2^31", nb);
+  std::memset(&d, 0, sizeof(d));
+  const float h = p.smoothing_radius;
+  d.dt = p.time_step;
+  d.gdt = p.gravity * p.time_step;
+  d.h = h;
+  d.s = s;
+  d.s2 = s * s;
+  d.m = p.rest_mass;
+  d.rho0 = p.rest_density;
+  d.inv_rho0 = 1.0f / p.rest_density;
+  d.neg_inv_rho0 = -1.0f / p.rest_density;
+  d.poly6_norm = (float)(315.0 / (64.0 * M_PI * std::pow((double)h, 9.0)));
+  d.spikey_norm = (float)(-45.0 / (M_PI * std::pow((double)h, 6.0)));
+  d.cspline_norm = (float)(32.0 / (M_PI * std::pow((double)h, 9.0)));
+  {
+    const float a = h * h - 0.0f * 0.0f;
+    d.W0 = d.poly6_norm * a * a * a;
+  }
+  d.lambda_eps = p.lambda_epsilon;
+  d.visc_c = p.visc_c;
+  d.vort_eps = p.vorticity_coef;
+  d.gamma = p.gamma;
+  for (int a = 0; a < 3; ++a) {
+    d.bmin[a] = p.boundary_min[a];
+    d.bmax[a] = p.boundary_max[a];
+    d.mc[a] = p.mover_center[a];
+  }
+  d.mr = p.mover_radius;
+  d.mr2 = p.mover_radius * p.mover_radius;
+  d.scorr_k = p.scorr_k;
+  d.scorr_n = p.scorr_n;
+  if (p.scorr_k > 0.0f) {
+    const float r = p.scorr_dq * h;
+    float w = 0.0f;
+    if (!(r > h)) {
+      const float a = h * h - r * r;
+      w = d.poly6_norm * a * a * a;
+    }
+    if (!(w > 0.0f)) return fail(ctx, PBF_ERR_PARAMS, "scorr_dq must be in (0, 1)");
+    d.inv_wdq = 1.0f / w;
+  }
+  d.vthr = 0.000001 * (double)p.max_speed;
+  d.h_eps = (double)h * 0.000001;
+  d.dimx = (int)dims[0];
+  d.dimy = (int)dims[1];
+  d.dimz = (int)dims[2];
+  d.nbins = (int)(dims[0] * dims[1] * dims[2]);
+  d.cap = p.neighbor_cap;
+  return PBF_OK;
+}
+
+template <typename T>
+int dalloc(pbf_ctx* ctx, T** ptr, size_t count) {
+  void* p = nullptr;
+  const size_t bytes = count * sizeof(T) > 0 ? count * sizeof(T) : 16;
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess)
+    return fail(ctx, PBF_ERR_CUDA, "cudaMalloc(%zu bytes) failed: %s", bytes, cudaGetErrorString(e));
+  ctx->allocations.push_back(p);
+  *ptr = static_cast<T*>(p);
+  return PBF_OK;
+}
+
+void drop_graphs(pbf_ctx* ctx) {
+  for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
+  ctx->graphs.clear();
+}
+
+int check_span(pbf_ctx* ctx, size_t b, size_t e) {
+  if (b != 0 || e != ctx->n)
+    return fail(ctx, PBF_ERR_SPAN, "span [%zu, %zu) given; a single rank supports only [0, %zu)", b, e, ctx->n);
+  return PBF_OK;
+}
+
+int need_lists(pbf_ctx* ctx) {
+  if (!ctx->lists_valid) return fail(ctx, PBF_ERR_STATE, "no neighbor lists: call find_neighbors first");
+  return PBF_OK;
+}
+
+// ---- launch bookkeeping: per-kernel CUDA events when timing is on ----
+struct Launch {
+  pbf_ctx* ctx;
+  const char* name;
+  explicit Launch(pbf_ctx* c, const char* nm) : ctx(c), name(nm) {
+    if (!ctx->timing) return;
+    if (ctx->marks_used == ctx->marks.size()) {
+      pbf_ctx::Mark m{nm, nullptr, nullptr};
+      cudaEventCreate(&m.start);
+      cudaEventCreate(&m.stop);
+      ctx->marks.push_back(m);
+    }
+    ctx->marks[ctx->marks_used].name = nm;
+    cudaEventRecord(ctx->marks[ctx->marks_used].start, ctx->stream);
+  }
+  ~Launch() {
+    if (!ctx->timing) return;
+    cudaEventRecord(ctx->marks[ctx->marks_used].stop, ctx->stream);
+    ctx->marks_used++;
+  }
+};
+
+int harvest_times(pbf_ctx* ctx) {
+  if (!ctx->timing || ctx->marks_used == 0) return PBF_OK;
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (size_t i = 0; i < ctx->marks_used; ++i) {
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, ctx->marks[i].start, ctx->marks[i].stop));
+    auto it = ctx->times.find(ctx->marks[i].name);
+    if (it == ctx->times.end()) {
+      ctx->times[ctx->marks[i].name] = {1, (double)ms};
+      ctx->time_order.push_back(ctx->marks[i].name);
+    } else {
+      it->second.first += 1;
+      it->second.second += ms;
+    }
+  }
+  ctx->marks_used = 0;
+  return PBF_OK;
+}
+
+// ---- neighbor build ----
+// Hash + histogram must already have produced key/rank/cell_count.
+void launch_sort_to_pairs(pbf_ctx* ctx) {
+  const int n = (int)ctx->n;
+  const int m = ctx->nbins;  // scan m entries -> m+1 outputs
+  {
+    Launch L(ctx, "scan_reduce");
+    k_scan_reduce<<<ctx->nscan_parts, kScanThreads, 0, ctx->stream>>>(ctx->cell_count, m, ctx->scan_part);
+  }
+  {
+    Launch L(ctx, "scan_partials");
+    k_scan_partials<<<1, kScanThreads, 0, ctx->stream>>>(ctx->scan_part, ctx->nscan_parts);
+  }
+  {
+    Launch L(ctx, "scan_apply");
+    k_scan_apply<<<ctx->nscan_parts, kScanThreads, 0, ctx->stream>>>(ctx->cell_count, m, ctx->scan_part,
+                                                                     ctx->cell_start);
+  }
+  {
+    Launch L(ctx, "scatter");
+    k_scatter<<<blocks_for(n), kBlock, 0, ctx->stream>>>(n, ctx->key, ctx->rank, ctx->cell_start, ctx->origH,
+                                                         ctx->pairs);
+  }
+  {
+    Launch L(ctx, "cell_sort");
+    k_cell_sort<<<blocks_for(ctx->nbins), kBlock, 0, ctx->stream>>>(ctx->nbins, ctx->cell_start, ctx->pairs);
+  }
+}
+
+void launch_fill(pbf_ctx* ctx, const float4* pst) {
+  Launch L(ctx, "fill_neighbors");
+  k_fill<<<blocks_for(ctx->n), kBlock, 0, ctx->stream>>>(ctx->dev, (int)ctx->n, ctx->capacity, pst,
+                                                         ctx->cell_start, ctx->nbr, ctx->cnt, ctx->err);
+}
+
+// ---- the fused step (graph-capturable: fixed pointers, no host sync) ----
+template <bool X, bool SCORR>
+void launch_step_t(pbf_ctx* ctx) {
+  const int n = (int)ctx->n;
+  const size_t st = ctx->capacity;
+  const Dev& P = ctx->dev;
+  cudaStream_t s = ctx->stream;
+  const int g = blocks_for(n);
+  cudaMemsetAsync(ctx->cell_count, 0, sizeof(uint32_t) * (size_t)ctx->nbins, s);
+  {
+    Launch L(ctx, "ext_predict_hash");
+    k_ext_predict_hash<<<g, kBlock, 0, s>>>(P, n, ctx->posH, ctx->velH, ctx->pstH, ctx->key, ctx->rank,
+                                            ctx->cell_count, ctx->err);
+  }
+  launch_sort_to_pairs(ctx);
+  {
+    Launch L(ctx, "reorder");
+    k_reorder<false><<<g, kBlock, 0, s>>>(n, ctx->pairs, ctx->key, ctx->posH, ctx->pstH, ctx->velH, nullptr,
+                                          nullptr, ctx->posS, ctx->pstS, ctx->velS, nullptr, nullptr, ctx->origS,
+                                          ctx->keyH);
+  }
+  launch_fill(ctx, ctx->pstS);
+  const int K = ctx->params.solve_steps;
+  for (int it = 0; it < K; ++it) {
+    {
+      Launch L(ctx, "density_lambda");
+      k_density_lambda<X><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl, ctx->velS,
+                                               ctx->lamH);
+    }
+    Launch L(ctx, "dp_update");
+    if (it == K - 1)
+      k_dp_update<X, SCORR, true><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS,
+                                                       ctx->posS, ctx->velS);
+    else
+      k_dp_update<X, SCORR, false><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS,
+                                                        ctx->posS, ctx->velS);
+  }
+  if (K == 0) {
+    Launch L(ctx, "update_velocities");
+    k_update_v<<<g, kBlock, 0, s>>>(P, n, ctx->pstS, ctx->posS, ctx->velS);
+  }
+  if (ctx->params.gamma != 0.0f) {
+    {
+      Launch L(ctx, "color_field");
+      k_color<X><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->velS, ctx->scrH);
+    }
+    Launch L(ctx, "surface_tension");
+    k_surface<<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->scrH, ctx->velS);
+  }
+  {
+    Launch L(ctx, "viscosity");
+    k_viscosity<X, false><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->velS, ctx->velT,
+                                               nullptr, nullptr, nullptr, nullptr);
+  }
+  {
+    Launch L(ctx, "vorticity");
+    k_vorticity<X><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->velT, ctx->scrH, ctx->xl);
+  }
+  {
+    Launch L(ctx, "apply_vorticity");
+    k_apply_vorticity<X, true><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->xl, nullptr, ctx->scrH,
+                                                    ctx->velT);
+  }
+  {
+    Launch L(ctx, "viscosity_final");
+    k_viscosity<X, true><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->velT, ctx->velH,
+                                              ctx->posH, ctx->pstH, ctx->origS, ctx->origH);
+  }
+}
+
+void launch_step(pbf_ctx* ctx) {
+  const bool X = ctx->params.exact_math != 0, SC = ctx->params.scorr_k > 0.0f;
+  if (X) {
+    if (SC) launch_step_t<true, true>(ctx); else launch_step_t<true, false>(ctx);
+  } else {
+    if (SC) launch_step_t<false, true>(ctx); else launch_step_t<false, false>(ctx);
+  }
+}
+
+int launches_per_step(const pbf_ctx* ctx) {
+  // kernels only (the bin-count memset is not one): ext/predict/hash + 3 scan
+  // + scatter + cell sort + reorder + fill + 2K solve + (K==0: velocity)
+  // + 2 if gamma + 4 (visc, vort, apply, visc)
+  const int K = ctx->params.solve_steps;
+  return 1 + 3 + 1 + 1 + 1 + 1 + 2 * K + (K == 0 ? 1 : 0) + (ctx->params.gamma != 0.0f ? 2 : 0) + 4;
+}
+
+}  // namespace
+
+// ============================================================================
+// C ABI
+// ============================================================================
+extern "C" {
+
+const char* pbf_create_error(void) { return g_create_error.c_str(); }
+const char* pbf_last_error(const pbf_ctx* ctx) { return ctx ? ctx->error.c_str() : g_create_error.c_str(); }
+
+int pbf_create(const pbf_params* p, size_t capacity, pbf_ctx** out) {
+  pbf_ctx* ctx = nullptr;
+  if (!p || !out) return fail(nullptr, PBF_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (capacity == 0 || capacity >= (size_t)1 << 31)
+    return fail(nullptr, PBF_ERR_ARG, "capacity must be in [1, 2^31)");
+  ctx = new pbf_ctx();
+  ctx->params = *p;
+  int rc = make_dev(ctx, *p, ctx->dev, ctx->dims);
+  if (rc) {
+    g_create_error = ctx->error;
+    delete ctx;
+    return rc;
+  }
+  ctx->capacity = capacity;
+  ctx->nbins = ctx->dev.nbins;
+  ctx->nscan_parts = (int)(((size_t)ctx->nbins + 1 + kScanTile - 1) / kScanTile);
+  auto bail = [&](int code) {
+    g_create_error = ctx->error;
+    pbf_destroy(ctx);
+    return code;
+  };
+  if (cudaGetDevice(&ctx->device) != cudaSuccess) {
+    fail(ctx, PBF_ERR_CUDA, "no CUDA device");
+    return bail(PBF_ERR_CUDA);
+  }
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    fail(ctx, PBF_ERR_CUDA, "cudaStreamCreate failed");
+    return bail(PBF_ERR_CUDA);
+  }
+  const size_t C = capacity;
+  const size_t cap = (size_t)p->neighbor_cap;
+  if ((rc = dalloc(ctx, &ctx->posH, C)) || (rc = dalloc(ctx, &ctx->pstH, C)) || (rc = dalloc(ctx, &ctx->velH, C)) ||
+      (rc = dalloc(ctx, &ctx->scrH, C)) || (rc = dalloc(ctx, &ctx->posS, C)) || (rc = dalloc(ctx, &ctx->pstS, C)) ||
+      (rc = dalloc(ctx, &ctx->velS, C)) || (rc = dalloc(ctx, &ctx->scrS, C)) || (rc = dalloc(ctx, &ctx->xl, C)) ||
+      (rc = dalloc(ctx, &ctx->velT, C)) || (rc = dalloc(ctx, &ctx->lamH, C)) || (rc = dalloc(ctx, &ctx->lamS, C)) ||
+      (rc = dalloc(ctx, &ctx->origH, C)) || (rc = dalloc(ctx, &ctx->origS, C)) || (rc = dalloc(ctx, &ctx->key, C)) ||
+      (rc = dalloc(ctx, &ctx->rank, C)) || (rc = dalloc(ctx, &ctx->keyH, C)) ||
+      (rc = dalloc(ctx, &ctx->cell_count, (size_t)ctx->nbins)) ||
+      (rc = dalloc(ctx, &ctx->cell_start, (size_t)ctx->nbins + 1)) ||
+      (rc = dalloc(ctx, &ctx->scan_part, (size_t)ctx->nscan_parts)) || (rc = dalloc(ctx, &ctx->err, 1)) ||
+      (rc = dalloc(ctx, &ctx->pairs, C)) || (rc = dalloc(ctx, &ctx->nbr, C * cap)) ||
+      (rc = dalloc(ctx, &ctx->cnt, C)) || (rc = dalloc(ctx, &ctx->stage, 6 * C)) ||
+      (rc = dalloc(ctx, &ctx->stage_i, C * cap + C)) || (rc = dalloc(ctx, &ctx->acc, 8)) ||
+      (rc = dalloc(ctx, &ctx->maxerr, 1)) || (rc = dalloc(ctx, &ctx->hits, 1)))
+    return bail(rc);
+  if (cudaMemsetAsync(ctx->err, 0, sizeof(uint32_t), ctx->stream) != cudaSuccess ||
+      cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+    fail(ctx, PBF_ERR_CUDA, "initialisation failed");
+    return bail(PBF_ERR_CUDA);
+  }
+  *out = ctx;
+  return PBF_OK;
+}
+
+void pbf_destroy(pbf_ctx* ctx) {
+  if (!ctx) return;
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  drop_graphs(ctx);
+  for (auto& m : ctx->marks) {
+    cudaEventDestroy(m.start);
+    cudaEventDestroy(m.stop);
+  }
+  for (void* p : ctx->allocations) cudaFree(p);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+int pbf_set_params(pbf_ctx* ctx, const pbf_params* p) {
+  if (!ctx || !p) return PBF_ERR_ARG;
+  Dev d;
+  int64_t dims[3];
+  int rc = make_dev(ctx, *p, d, dims);
+  if (rc) return rc;
+  if (d.nbins > ctx->nbins || p->neighbor_cap > ctx->params.neighbor_cap)
+    return fail(ctx, PBF_ERR_PARAMS, "new parameters need a larger grid or neighbor cap than allocated");
+  if (d.nbins != ctx->nbins || p->neighbor_cap != ctx->params.neighbor_cap) ctx->lists_valid = false;
+  ctx->params = *p;
+  ctx->dev = d;
+  std::memcpy(ctx->dims, dims, sizeof(dims));
+  ctx->nbins = d.nbins;
+  ctx->nscan_parts = (int)(((size_t)ctx->nbins + 1 + kScanTile - 1) / kScanTile);
+  drop_graphs(ctx);
+  return PBF_OK;
+}
+
+int pbf_get_params(const pbf_ctx* ctx, pbf_params* p) {
+  if (!ctx || !p) return PBF_ERR_ARG;
+  *p = ctx->params;
+  return PBF_OK;
+}
+
+size_t pbf_count(const pbf_ctx* ctx) { return ctx ? ctx->n : 0; }
+int64_t pbf_num_bins(const pbf_ctx* ctx) { return ctx ? ctx->nbins : 0; }
+
+int pbf_upload(pbf_ctx* ctx, const float* x, const float* v, size_t n) {
+  if (!ctx || (!x && n)) return ctx ? fail(ctx, PBF_ERR_ARG, "null positions") : PBF_ERR_ARG;
+  if (n > ctx->capacity)
+    return fail(ctx, PBF_ERR_CAPACITY, "Not enough capacity: %zu particles > capacity %zu", n, ctx->capacity);
+  if (n != ctx->n) drop_graphs(ctx);
+  ctx->n = n;
+  ctx->lists_valid = false;
+  if (n == 0) return PBF_OK;
+  float* dx = ctx->stage;
+  float* dv = ctx->stage + 3 * ctx->capacity;
+  CK(cudaMemcpyAsync(dx, x, n * 3 * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  if (v) CK(cudaMemcpyAsync(dv, v, n * 3 * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  k_upload<<<blocks_for(n), kBlock, 0, ctx->stream>>>((int)n, dx, v ? dv : nullptr, ctx->posH, ctx->pstH,
+                                                      ctx->velH, ctx->scrH, ctx->lamH, ctx->origH);
+  return check_launch(ctx, "upload");
+}
+
+static int get_array_dev(pbf_ctx* ctx, int which, float* dst) {
+  const int n = (int)ctx->n, g = blocks_for(n);
+  switch (which) {
+    case PBF_ARRAY_POSITIONS: k_unpermute_vec<<<g, kBlock, 0, ctx->stream>>>(n, ctx->posH, ctx->origH, dst); break;
+    case PBF_ARRAY_POSITION_STARS: k_unpermute_vec<<<g, kBlock, 0, ctx->stream>>>(n, ctx->pstH, ctx->origH, dst); break;
+    case PBF_ARRAY_VELOCITIES: k_unpermute_vec<<<g, kBlock, 0, ctx->stream>>>(n, ctx->velH, ctx->origH, dst); break;
+    case PBF_ARRAY_SCRATCH: k_unpermute_vec<<<g, kBlock, 0, ctx->stream>>>(n, ctx->scrH, ctx->origH, dst); break;
+    case PBF_ARRAY_DENSITIES: k_unpermute_w<<<g, kBlock, 0, ctx->stream>>>(n, ctx->velH, nullptr, ctx->origH, dst); break;
+    case PBF_ARRAY_LAMBDAS: k_unpermute_w<<<g, kBlock, 0, ctx->stream>>>(n, nullptr, ctx->lamH, ctx->origH, dst); break;
+    default: return fail(ctx, PBF_ERR_ARG, "unknown array %d", which);
+  }
+  return check_launch(ctx, "unpermute");
+}
+
+int pbf_get_array(pbf_ctx* ctx, int which, float* host_out) {
+  if (!ctx || !host_out) return PBF_ERR_ARG;
+  if (ctx->n == 0) return PBF_OK;
+  const bool vec = which <= PBF_ARRAY_SCRATCH;
+  int rc = get_array_dev(ctx, which, ctx->stage);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(host_out, ctx->stage, ctx->n * (vec ? 3 : 1) * sizeof(float), cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PBF_OK;
+}
+
+int pbf_set_array(pbf_ctx* ctx, int which, const float* host_in) {
+  if (!ctx || !host_in) return PBF_ERR_ARG;
+  if (ctx->n == 0) return PBF_OK;
+  const int n = (int)ctx->n, g = blocks_for(n);
+  const bool vec = which <= PBF_ARRAY_SCRATCH;
+  CK(cudaMemcpyAsync(ctx->stage, host_in, ctx->n * (vec ? 3 : 1) * sizeof(float), cudaMemcpyHostToDevice,
+                     ctx->stream));
+  switch (which) {
+    case PBF_ARRAY_POSITIONS: k_permute_vec_in<<<g, kBlock, 0, ctx->stream>>>(n, ctx->stage, ctx->origH, ctx->posH); break;
+    case PBF_ARRAY_POSITION_STARS: k_permute_vec_in<<<g, kBlock, 0, ctx->stream>>>(n, ctx->stage, ctx->origH, ctx->pstH); break;
+    case PBF_ARRAY_VELOCITIES: k_permute_vec_in<<<g, kBlock, 0, ctx->stream>>>(n, ctx->stage, ctx->origH, ctx->velH); break;
+    case PBF_ARRAY_SCRATCH: k_permute_vec_in<<<g, kBlock, 0, ctx->stream>>>(n, ctx->stage, ctx->origH, ctx->scrH); break;
+    case PBF_ARRAY_DENSITIES: k_permute_w_in<<<g, kBlock, 0, ctx->stream>>>(n, ctx->stage, ctx->origH, ctx->velH, nullptr); break;
+    case PBF_ARRAY_LAMBDAS: k_permute_w_in<<<g, kBlock, 0, ctx->stream>>>(n, ctx->stage, ctx->origH, nullptr, ctx->lamH); break;
+    default: return fail(ctx, PBF_ERR_ARG, "unknown array %d", which);
+  }
+  int rc = check_launch(ctx, "set_array");
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PBF_OK;
+}
+
+int pbf_download(pbf_ctx* ctx, float* x, float* v, float* rho, float* lambda) {
+  if (!ctx) return PBF_ERR_ARG;
+  if (ctx->n == 0) return PBF_OK;
+  const size_t n = ctx->n;
+  float* sx = ctx->stage;
+  float* sv = ctx->stage + 3 * ctx->capacity;
+  int rc;
+  if (x) {
+    if ((rc = get_array_dev(ctx, PBF_ARRAY_POSITIONS, sx))) return rc;
+    CK(cudaMemcpyAsync(x, sx, n * 3 * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  if (v) {
+    if ((rc = get_array_dev(ctx, PBF_ARRAY_VELOCITIES, sv))) return rc;
+    CK(cudaMemcpyAsync(v, sv, n * 3 * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  if (rho || lambda) {
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (rho) {
+      if ((rc = get_array_dev(ctx, PBF_ARRAY_DENSITIES, sx))) return rc;
+      CK(cudaMemcpyAsync(rho, sx, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    if (lambda) {
+      if ((rc = get_array_dev(ctx, PBF_ARRAY_LAMBDAS, sv))) return rc;
+      CK(cudaMemcpyAsync(lambda, sv, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PBF_OK;
+}
+
+// ---- stages ----
+#define STAGE_PROLOGUE(b, e)              \
+  if (!ctx) return PBF_ERR_ARG;           \
+  {                                       \
+    int rc_ = check_span(ctx, b, e);      \
+    if (rc_) return rc_;                  \
+  }                                       \
+  if (ctx->n == 0) return PBF_OK;         \
+  const int n = (int)ctx->n;              \
+  const int g = blocks_for(ctx->n);       \
+  (void)g;                                \
+  const bool X = ctx->params.exact_math != 0; \
+  (void)X;
+
+int pbf_apply_external_forces(pbf_ctx* ctx, size_t b, size_t e) {
+  STAGE_PROLOGUE(b, e);
+  k_external<<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->velH);
+  return check_launch(ctx, "apply_external_forces");
+}
+
+int pbf_predict_positions(pbf_ctx* ctx, size_t b, size_t e) {
+  STAGE_PROLOGUE(b, e);
+  k_predict<<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->posH, ctx->velH, ctx->pstH);
+  return check_launch(ctx, "predict_positions");
+}
+
+int pbf_find_neighbors(pbf_ctx* ctx, size_t bin_b, size_t bin_e, size_t fill_b, size_t fill_e) {
+  if (!ctx) return PBF_ERR_ARG;
+  int rc = check_span(ctx, bin_b, bin_e);
+  if (rc) return rc;
+  if ((rc = check_span(ctx, fill_b, fill_e))) return rc;
+  if (ctx->n == 0) {
+    ctx->lists_valid = true;
+    return PBF_OK;
+  }
+  const int n = (int)ctx->n, g = blocks_for(ctx->n);
+  cudaStream_t s = ctx->stream;
+  CK(cudaMemsetAsync(ctx->cell_count, 0, sizeof(uint32_t) * (size_t)ctx->nbins, s));
+  k_hash<<<g, kBlock, 0, s>>>(ctx->dev, n, ctx->pstH, ctx->key, ctx->rank, ctx->cell_count, ctx->err);
+  launch_sort_to_pairs(ctx);
+  k_reorder<true><<<g, kBlock, 0, s>>>(n, ctx->pairs, ctx->key, ctx->posH, ctx->pstH, ctx->velH, ctx->scrH,
+                                       ctx->lamH, ctx->posS, ctx->pstS, ctx->velS, ctx->scrS, ctx->lamS, ctx->origS,
+                                       ctx->keyH);
+  const size_t f4 = sizeof(float4) * ctx->n;
+  CK(cudaMemcpyAsync(ctx->posH, ctx->posS, f4, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(ctx->pstH, ctx->pstS, f4, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(ctx->velH, ctx->velS, f4, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(ctx->scrH, ctx->scrS, f4, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(ctx->lamH, ctx->lamS, sizeof(float) * ctx->n, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(ctx->origH, ctx->origS, sizeof(uint32_t) * ctx->n, cudaMemcpyDeviceToDevice, s));
+  launch_fill(ctx, ctx->pstH);
+  rc = check_launch(ctx, "find_neighbors");
+  if (rc) return rc;
+  ctx->lists_valid = true;
+  return PBF_OK;
+}
+
+int pbf_compute_densities(pbf_ctx* ctx, size_t b, size_t e) {
+  STAGE_PROLOGUE(b, e);
+  if (int rc = need_lists(ctx)) return rc;
+  if (X) k_density<true><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH);
+  else k_density<false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH);
+  return check_launch(ctx, "compute_densities");
+}
+
+int pbf_compute_pressure_lambdas(pbf_ctx* ctx, size_t b, size_t e) {
+  STAGE_PROLOGUE(b, e);
+  if (int rc = need_lists(ctx)) return rc;
+  if (X) k_lambda<true><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->lamH);
+  else k_lambda<false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->lamH);
+  return check_launch(ctx, "compute_pressure_lambdas");
+}
+
+int pbf_compute_pressure_dps(pbf_ctx* ctx, size_t b, size_t e, int substep) {
+  (void)substep;  // unused by the reference too (particles.h:348)
+  STAGE_PROLOGUE(b, e);
+  if (int rc = need_lists(ctx)) return rc;
+  const bool SC = ctx->params.scorr_k > 0.0f;
+  const Dev& P = ctx->dev;
+  if (X && SC) k_dp<true, true><<<g, kBlock, 0, ctx->stream>>>(P, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->lamH, ctx->scrH);
+  else if (X) k_dp<true, false><<<g, kBlock, 0, ctx->stream>>>(P, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->lamH, ctx->scrH);
+  else if (SC) k_dp<false, true><<<g, kBlock, 0, ctx->stream>>>(P, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->lamH, ctx->scrH);
+  else k_dp<false, false><<<g, kBlock, 0, ctx->stream>>>(P, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->lamH, ctx->scrH);
+  return check_launch(ctx, "compute_pressure_dps");
+}
+
+int pbf_update_position_stars(pbf_ctx* ctx, size_t b, size_t e) {
+  STAGE_PROLOGUE(b, e);
+  k_update_xs<<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->pstH, ctx->scrH);
+  return check_launch(ctx, "update_position_stars");
+}
+
+int pbf_update_velocities(pbf_ctx* ctx, size_t b, size_t e) {
+  STAGE_PROLOGUE(b, e);
+  k_update_v<<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->pstH, ctx->posH, ctx->velH);
+  return check_launch(ctx, "update_velocities");
+}
+
+int pbf_apply_surface_tension(pbf_ctx* ctx, size_t cb, size_t ce, size_t sb, size_t se) {
+  if (!ctx) return PBF_ERR_ARG;
+  if (int rc = check_span(ctx, sb, se)) return rc;
+  STAGE_PROLOGUE(cb, ce);
+  if (int rc = need_lists(ctx)) return rc;
+  if (X) k_color<true><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->scrH);
+  else k_color<false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->scrH);
+  k_surface<<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->scrH, ctx->velH);
+  return check_launch(ctx, "apply_surface_tension");
+}
+
+int pbf_apply_viscosity(pbf_ctx* ctx, size_t b, size_t e) {
+  STAGE_PROLOGUE(b, e);
+  if (int rc = need_lists(ctx)) return rc;
+  if (X) k_viscosity<true, false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->velT, nullptr, nullptr, nullptr, nullptr);
+  else k_viscosity<false, false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->velT, nullptr, nullptr, nullptr, nullptr);
+  CK(cudaMemcpyAsync(ctx->velH, ctx->velT, sizeof(float4) * ctx->n, cudaMemcpyDeviceToDevice, ctx->stream));
+  return check_launch(ctx, "apply_viscosity");
+}
+
+int pbf_compute_vorticity(pbf_ctx* ctx, size_t b, size_t e) {
+  STAGE_PROLOGUE(b, e);
+  if (int rc = need_lists(ctx)) return rc;
+  if (X) k_vorticity<true><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->scrH, nullptr);
+  else k_vorticity<false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->scrH, nullptr);
+  return check_launch(ctx, "compute_vorticity");
+}
+
+int pbf_apply_vorticity(pbf_ctx* ctx, size_t b, size_t e) {
+  STAGE_PROLOGUE(b, e);
+  if (int rc = need_lists(ctx)) return rc;
+  if (X) k_apply_vorticity<true, false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, nullptr, ctx->pstH, ctx->scrH, ctx->velH);
+  else k_apply_vorticity<false, false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, nullptr, ctx->pstH, ctx->scrH, ctx->velH);
+  return check_launch(ctx, "apply_vorticity");
+}
+
+int pbf_update_positions(pbf_ctx* ctx, size_t b, size_t e) {
+  STAGE_PROLOGUE(b, e);
+  CK(cudaMemcpyAsync(ctx->posH, ctx->pstH, sizeof(float4) * ctx->n, cudaMemcpyDeviceToDevice, ctx->stream));
+  return PBF_OK;
+}
+
+int pbf_step(pbf_ctx* ctx, int nsteps) {
+  if (!ctx || nsteps < 0) return PBF_ERR_ARG;
+  if (ctx->n == 0 || nsteps == 0) return PBF_OK;
+  if (ctx->timing) {
+    for (int i = 0; i < nsteps; ++i) launch_step(ctx);
+    int rc = check_launch(ctx, "step");
+    if (rc) return rc;
+    ctx->lists_valid = true;
+    return harvest_times(ctx);
+  }
+  auto it = ctx->graphs.find(nsteps);
+  if (it == ctx->graphs.end()) {
+    cudaGraph_t graph = nullptr;
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    for (int i = 0; i < nsteps; ++i) launch_step(ctx);
+    cudaError_t le = cudaGetLastError();
+    cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
+    if (le != cudaSuccess || ce != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      return fail(ctx, PBF_ERR_CUDA, "graph capture failed: %s / %s", cudaGetErrorString(le),
+                  cudaGetErrorString(ce));
+    }
+    cudaGraphExec_t exec = nullptr;
+    cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) return fail(ctx, PBF_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ie));
+    it = ctx->graphs.emplace(nsteps, exec).first;
+  }
+  CK(cudaGraphLaunch(it->second, ctx->stream));
+  ctx->lists_valid = true;
+  return PBF_OK;
+}
+
+int pbf_sync(pbf_ctx* ctx) {
+  if (!ctx) return PBF_ERR_ARG;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PBF_OK;
+}
+
+int pbf_get_stream(pbf_ctx* ctx, void** stream_out) {
+  if (!ctx || !stream_out) return PBF_ERR_ARG;
+  *stream_out = (void*)ctx->stream;
+  return PBF_OK;
+}
+
+int pbf_get_neighbors(pbf_ctx* ctx, int32_t* idx, int32_t* count) {
+  if (!ctx) return PBF_ERR_ARG;
+  if (int rc = need_lists(ctx)) return rc;
+  if (ctx->n == 0) return PBF_OK;
+  const size_t n = ctx->n, cap = (size_t)ctx->params.neighbor_cap;
+  int32_t* di = ctx->stage_i;
+  int32_t* dc = ctx->stage_i + n * cap;
+  k_export_neighbors<<<blocks_for(n), kBlock, 0, ctx->stream>>>((int)n, ctx->capacity, (int)cap, ctx->nbr, ctx->cnt,
+                                                                 ctx->origH, di, dc);
+  if (int rc = check_launch(ctx, "export_neighbors")) return rc;
+  if (idx) CK(cudaMemcpyAsync(idx, di, n * cap * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  if (count) CK(cudaMemcpyAsync(count, dc, n * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PBF_OK;
+}
+
+int pbf_get_bins(pbf_ctx* ctx, uint32_t* sorted_keys, uint32_t* sorted_ids, uint32_t* bin_begin,
+                 uint32_t* bin_end) {
+  if (!ctx) return PBF_ERR_ARG;
+  if (int rc = need_lists(ctx)) return rc;
+  const size_t n = ctx->n, B = (size_t)ctx->nbins;
+  if (sorted_keys && n) CK(cudaMemcpyAsync(sorted_keys, ctx->keyH, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  if (sorted_ids && n) CK(cudaMemcpyAsync(sorted_ids, ctx->origH, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  if (bin_begin) CK(cudaMemcpyAsync(bin_begin, ctx->cell_start, B * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  if (bin_end) CK(cudaMemcpyAsync(bin_end, ctx->cell_start + 1, B * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PBF_OK;
+}
+
+int pbf_stats(pbf_ctx* ctx, pbf_stats_t* out) {
+  if (!ctx || !out) return PBF_ERR_ARG;
+  std::memset(out, 0, sizeof(*out));
+  out->n = ctx->n;
+  if (int rc = need_lists(ctx)) return rc;
+  cudaStream_t s = ctx->stream;
+  CK(cudaMemsetAsync(ctx->acc, 0, 8 * sizeof(double), s));
+  CK(cudaMemsetAsync(ctx->maxerr, 0, sizeof(unsigned long long), s));
+  CK(cudaMemsetAsync(ctx->hits, 0, sizeof(unsigned long long), s));
+  if (ctx->n) {
+    k_stats<<<blocks_for(ctx->n), kBlock, 0, s>>>(ctx->dev, (int)ctx->n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH,
+                                                  ctx->posH, ctx->velH, ctx->acc, ctx->maxerr, ctx->hits);
+    if (int rc = check_launch(ctx, "stats")) return rc;
+  }
+  double acc[8];
+  unsigned long long mx = 0, hits = 0;
+  uint32_t err = 0;
+  CK(cudaMemcpyAsync(acc, ctx->acc, sizeof(acc), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&mx, ctx->maxerr, sizeof(mx), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&hits, ctx->hits, sizeof(hits), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&err, ctx->err, sizeof(err), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemsetAsync(ctx->err, 0, sizeof(uint32_t), s));
+  CK(cudaStreamSynchronize(s));
+  const double n = ctx->n ? (double)ctx->n : 1.0;
+  double maxerr;
+  std::memcpy(&maxerr, &mx, sizeof(double));
+  out->mean_density_error = acc[0] / n;
+  out->max_density_error = maxerr;
+  out->kinetic_energy = acc[1];
+  out->center_of_mass[0] = acc[2] / n;
+  out->center_of_mass[1] = acc[3] / n;
+  out->center_of_mass[2] = acc[4] / n;
+  out->mean_neighbors = acc[5] / n;
+  out->cap_hits = hits;
+  out->error_flags = err;
+  return PBF_OK;
+}
+
+int pbf_set_timing(pbf_ctx* ctx, int on) {
+  if (!ctx) return PBF_ERR_ARG;
+  ctx->timing = on != 0;
+  return PBF_OK;
+}
+
+int pbf_reset_timing(pbf_ctx* ctx) {
+  if (!ctx) return PBF_ERR_ARG;
+  ctx->times.clear();
+  ctx->time_order.clear();
+  ctx->marks_used = 0;
+  return PBF_OK;
+}
+
+int pbf_kernel_times(pbf_ctx* ctx, int max_kinds, const char** names, int64_t* launches, double* total_ms,
+                     int* n_kinds) {
+  if (!ctx) return PBF_ERR_ARG;
+  if (int rc = harvest_times(ctx)) return rc;
+  int i = 0;
+  for (const auto& nm : ctx->time_order) {
+    if (i >= max_kinds) break;
+    const auto& t = ctx->times[nm];
+    // names point at the static string literals the launches were tagged with
+    for (const auto& m : ctx->marks)
+      if (nm == m.name) {
+        if (names) names[i] = m.name;
+        break;
+      }
+    if (launches) launches[i] = t.first;
+    if (total_ms) total_ms[i] = t.second;
+    ++i;
+  }
+  if (n_kinds) *n_kinds = i;
+  return PBF_OK;
+}
+
+int pbf_launches_per_step(pbf_ctx* ctx, int64_t* out) {
+  if (!ctx || !out) return PBF_ERR_ARG;
+  *out = launches_per_step(ctx);
+  return PBF_OK;
+}
+
+}  // extern "C"

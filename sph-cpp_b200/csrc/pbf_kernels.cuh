@@ -1,0 +1,141 @@
+// Device-side math of the PBF step for sm_100a.
+//
+// Two evaluation policies share every kernel:
+//   X = true  ("exact"): the reference's operation order with IEEE-rounded
+//             __fadd_rn/__fmul_rn/__fdiv_rn/__fsqrt_rn, never contracted to FMA,
+//             so results are bit-identical to the reference's gcc build
+//             (x86-64, no FMA) on the same inputs and neighbor lists.
+//   X = false ("fast"): FMA, reciprocal multiplies and rsqrt in the physics
+//             gathers; results within the 1e-5 parity tolerance.
+// The parts that decide neighbor sets (predict, boundary clamp, bin hash, the
+// distance test) are always exact, so neighbor lists are bit-identical in both.
+#pragma once
+#include <cfloat>
+#include <cstdint>
+
+namespace pbf {
+
+// Per-launch constant block (kernel argument, < 4 KB).
+struct Dev {
+  float dt, gdt;  // time step; g*dt rounded in float (particles.h:264-268)
+  float h, s, s2; // smoothing radius, bin spacing, s*s (neighbors.h:198)
+  float m, rho0, inv_rho0, neg_inv_rho0;  // (Real)1/rho0, (Real)-1/rho0 (particles.h:332,356)
+  float W0;       // Poly6(0) (particles.h:294)
+  float poly6_norm, spikey_norm, cspline_norm;  // kernels.h:62,160,218 (double -> float)
+  float lambda_eps, visc_c, vort_eps, gamma;
+  float bmin[3], bmax[3], mc[3];
+  float mr, mr2;  // mover radius and radius*radius in float (particles.h:515-519)
+  float scorr_k, scorr_n, inv_wdq;
+  double vthr;    // 0.000001 * max_speed, compared in double (particles.h:380)
+  double h_eps;   // smoothing_radius * 0.000001 in double (particles.h:420)
+  int dimx, dimy, dimz, nbins, cap;
+};
+
+// ---------------- exact scalar helpers ----------------
+__device__ __forceinline__ float xadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float xsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float xmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float xdiv(float a, float b) { return __fdiv_rn(a, b); }
+
+// Policy-selected ops.
+template <bool X> __device__ __forceinline__ float A(float a, float b) { return X ? __fadd_rn(a, b) : a + b; }
+template <bool X> __device__ __forceinline__ float S(float a, float b) { return X ? __fsub_rn(a, b) : a - b; }
+template <bool X> __device__ __forceinline__ float M(float a, float b) { return X ? __fmul_rn(a, b) : a * b; }
+template <bool X> __device__ __forceinline__ float D(float a, float b) { return X ? __fdiv_rn(a, b) : __fdividef(a, b); }
+template <bool X> __device__ __forceinline__ float SQ(float a) {
+  if (X) return __fsqrt_rn(a);
+  return a > 0.0f ? a * rsqrtf(a) : 0.0f;
+}
+
+// dot(r, r) from 0 in x, y, z order (vec.h:476-483, 490-494)
+template <bool X> __device__ __forceinline__ float mag2(float x, float y, float z) {
+  if (X) return __fadd_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)), __fmul_rn(z, z));
+  return fmaf(z, z, fmaf(y, y, x * x));
+}
+
+// Poly6 3D (kernels.h:64-70): norm*(h^2-r^2)^3, 0 for r > h.
+template <bool X> __device__ __forceinline__ float poly6(const Dev& P, float r) {
+  if (r > P.h) return 0.0f;
+  if (X) {
+    const float a = __fsub_rn(__fmul_rn(P.h, P.h), __fmul_rn(r, r));
+    return __fmul_rn(__fmul_rn(__fmul_rn(P.poly6_norm, a), a), a);
+  }
+  const float a = fmaf(-r, r, P.h * P.h);
+  return P.poly6_norm * a * a * a;
+}
+
+// Scalar factor f of Del_Spikey 3D (kernels.h:163-172) such that the gradient
+// is f*r in fast mode; exact mode evaluates component-wise as the reference:
+// ((norm*(h-r))*(h-r) * r_i) / (r + FLT_EPSILON).
+template <bool X> __device__ __forceinline__ float3 del_spikey(const Dev& P, float rx, float ry,
+                                                               float rz, float rm) {
+  if (rm > P.h) return make_float3(0.0f, 0.0f, 0.0f);
+  if (X) {
+    const float hr = __fsub_rn(P.h, rm);
+    const float s = __fmul_rn(__fmul_rn(P.spikey_norm, hr), hr);
+    const float den = __fadd_rn(rm, FLT_EPSILON);
+    return make_float3(__fdiv_rn(__fmul_rn(s, rx), den), __fdiv_rn(__fmul_rn(s, ry), den),
+                       __fdiv_rn(__fmul_rn(s, rz), den));
+  }
+  const float hr = P.h - rm;
+  const float f = P.spikey_norm * hr * hr * __fdividef(1.0f, rm + FLT_EPSILON);
+  return make_float3(f * rx, f * ry, f * rz);
+}
+
+// C_Spline 3D (kernels.h:220-228); the r <= h/2 branch is a double expression.
+template <bool X> __device__ __forceinline__ float c_spline(const Dev& P, float r) {
+  const float h = P.h;
+  if (r > h) return 0.0f;
+  if (r <= __fmul_rn(h, 0.5f)) {
+    const float hr = __fsub_rn(h, r);
+    const double t = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(2.0, (double)hr), (double)hr),
+                                                   (double)hr), (double)r), (double)r);
+    const double t2 = __dmul_rn(t, (double)r);
+    const float h6 = __fdiv_rn(__fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(h, h), h), h), h), h), 64.0f);
+    return (float)__dmul_rn((double)P.cspline_norm, __dsub_rn(t2, (double)h6));
+  }
+  const float hr = __fsub_rn(h, r);
+  float v = __fmul_rn(P.cspline_norm, hr);
+  v = __fmul_rn(v, hr);
+  v = __fmul_rn(v, hr);
+  v = __fmul_rn(v, r);
+  v = __fmul_rn(v, r);
+  return __fmul_rn(v, r);
+}
+
+// apply_boundary_conditions (particles.h:510-526), always exact.
+__device__ __forceinline__ float3 boundary(const Dev& P, float3 p) {
+  const float dx = xsub(p.x, P.mc[0]), dy = xsub(p.y, P.mc[1]), dz = xsub(p.z, P.mc[2]);
+  const float dr2 = mag2<true>(dx, dy, dz);
+  if (dr2 < P.mr2) {
+    const float dr = __fsqrt_rn(dr2);
+    const float a = xsub(P.mr, dr);
+    p.x = xadd(p.x, xdiv(xmul(a, dx), dr));
+    p.y = xadd(p.y, xdiv(xmul(a, dy), dr));
+    p.z = xadd(p.z, xdiv(xmul(a, dz), dr));
+  }
+  // clamp_in_place (utility_math.h:52-57)
+  p.x = p.x < P.bmin[0] ? P.bmin[0] : (p.x > P.bmax[0] ? P.bmax[0] : p.x);
+  p.y = p.y < P.bmin[1] ? P.bmin[1] : (p.y > P.bmax[1] ? P.bmax[1] : p.y);
+  p.z = p.z < P.bmin[2] ? P.bmin[2] : (p.z > P.bmax[2] ? P.bmax[2] : p.z);
+  return p;
+}
+
+// floor((c + s)/s) per axis (neighbors.h:109-114).  Returns false when the
+// coordinate is non-finite or lands outside the grid; ok grids (checked at
+// context creation) never do for clamped positions.
+__device__ __forceinline__ int dev_axis_bin(float c, float s) {
+  return (int)floorf(xdiv(xadd(c, s), s));
+}
+
+__device__ __forceinline__ bool bin_of(const Dev& P, float x, float y, float z, uint32_t& out) {
+  const int bx = dev_axis_bin(x, P.s), by = dev_axis_bin(y, P.s), bz = dev_axis_bin(z, P.s);
+  const bool ok = bx >= 0 && by >= 0 && bz >= 0 && bx < P.dimx && by < P.dimy && bz < P.dimz &&
+                  isfinite(x) && isfinite(y) && isfinite(z);
+  const int cx = min(max(bx, 0), P.dimx - 1), cy = min(max(by, 0), P.dimy - 1),
+            cz = min(max(bz, 0), P.dimz - 1);
+  out = (uint32_t)(P.dimx * P.dimy) * (uint32_t)cz + ((uint32_t)cy * (uint32_t)P.dimx + (uint32_t)cx);
+  return ok;
+}
+
+}  // namespace pbf

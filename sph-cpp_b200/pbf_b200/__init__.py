@@ -1,0 +1,232 @@
+"""Python host side of the B200 PBF step (libpbf_b200.so through its C ABI).
+
+`Particles` mirrors the reference's sim::Particles<float,3> call surface
+(Simulation/Source/particles.h:256-487): the same stage names, the same span
+arguments ([0, N) on a single rank) and the same error behaviour (a failing
+call raises RuntimeError, as the reference throws std::runtime_error).
+`scenes` builds the dam-break workloads.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from ._abi import PbfParams, PbfStats  # noqa: F401
+from .scenes import Scene, make_scene, SCENES  # noqa: F401
+
+__all__ = ["Particles", "PbfParams", "PbfStats", "Scene", "make_scene", "SCENES", "lib", "params_init"]
+
+
+def lib() -> C.CDLL:
+    return _abi.load()
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def params_init() -> PbfParams:
+    p = PbfParams()
+    lib().pbf_params_init(C.byref(p))
+    return p
+
+
+class Particles:
+    """A device-resident particle set plus its PBF solver (one pbf_ctx)."""
+
+    def __init__(self, params: PbfParams, capacity: int):
+        self._lib = lib()
+        self._ctx = C.c_void_p()
+        rc = self._lib.pbf_create(C.byref(params), int(capacity), C.byref(self._ctx))
+        if rc != 0:
+            raise RuntimeError(f"pbf_create failed ({rc}): {self._lib.pbf_create_error().decode()}")
+        self.capacity = int(capacity)
+
+    # -- lifetime --
+    def close(self) -> None:
+        if self._ctx:
+            self._lib.pbf_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int, what: str) -> None:
+        if rc != 0:
+            raise RuntimeError(f"{what} failed ({rc}): {self._lib.pbf_last_error(self._ctx).decode()}")
+
+    @property
+    def ctx(self) -> C.c_void_p:
+        return self._ctx
+
+    # -- state --
+    def local_count(self) -> int:
+        return int(self._lib.pbf_count(self._ctx))
+
+    def span(self) -> tuple[int, int]:
+        return 0, self.local_count()
+
+    def upload(self, x: np.ndarray, v: np.ndarray | None = None) -> None:
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, 3)
+        if v is not None:
+            v = np.ascontiguousarray(v, dtype=np.float32).reshape(-1, 3)
+            assert v.shape == x.shape
+        self._check(self._lib.pbf_upload(self._ctx, _ptr(x), _ptr(v), x.shape[0]), "upload")
+
+    def download(self) -> dict:
+        n = self.local_count()
+        x = np.empty((n, 3), np.float32)
+        v = np.empty((n, 3), np.float32)
+        rho = np.empty(n, np.float32)
+        lam = np.empty(n, np.float32)
+        self._check(self._lib.pbf_download(self._ctx, _ptr(x), _ptr(v), _ptr(rho), _ptr(lam)), "download")
+        return {"x": x, "v": v, "rho": rho, "lambda": lam}
+
+    def get_array(self, which: int) -> np.ndarray:
+        n = self.local_count()
+        out = np.empty((n, 3) if which <= _abi.ARRAY_SCRATCH else (n,), np.float32)
+        self._check(self._lib.pbf_get_array(self._ctx, which, _ptr(out)), "get_array")
+        return out
+
+    def set_array(self, which: int, values: np.ndarray) -> None:
+        a = np.ascontiguousarray(values, dtype=np.float32)
+        self._check(self._lib.pbf_set_array(self._ctx, which, _ptr(a)), "set_array")
+
+    def positions(self) -> np.ndarray:
+        return self.get_array(_abi.ARRAY_POSITIONS)
+
+    def position_stars(self) -> np.ndarray:
+        return self.get_array(_abi.ARRAY_POSITION_STARS)
+
+    def velocities(self) -> np.ndarray:
+        return self.get_array(_abi.ARRAY_VELOCITIES)
+
+    def densities(self) -> np.ndarray:
+        return self.get_array(_abi.ARRAY_DENSITIES)
+
+    def lambdas(self) -> np.ndarray:
+        return self.get_array(_abi.ARRAY_LAMBDAS)
+
+    def scratch(self) -> np.ndarray:
+        return self.get_array(_abi.ARRAY_SCRATCH)
+
+    # -- stages (particles.h:256-487) --
+    def apply_external_forces(self, span=None):
+        self._check(self._lib.pbf_apply_external_forces(self._ctx, *(span or self.span())), "apply_external_forces")
+
+    def predict_positions(self, span=None):
+        self._check(self._lib.pbf_predict_positions(self._ctx, *(span or self.span())), "predict_positions")
+
+    def find_neighbors(self, bin_span=None, fill_span=None):
+        b = bin_span or self.span()
+        f = fill_span or self.span()
+        self._check(self._lib.pbf_find_neighbors(self._ctx, b[0], b[1], f[0], f[1]), "find_neighbors")
+
+    def compute_densities(self, span=None):
+        self._check(self._lib.pbf_compute_densities(self._ctx, *(span or self.span())), "compute_densities")
+
+    def compute_pressure_lambdas(self, span=None):
+        self._check(self._lib.pbf_compute_pressure_lambdas(self._ctx, *(span or self.span())),
+                    "compute_pressure_lambdas")
+
+    def compute_pressure_dps(self, span=None, substep: int = 0):
+        s = span or self.span()
+        self._check(self._lib.pbf_compute_pressure_dps(self._ctx, s[0], s[1], substep), "compute_pressure_dps")
+
+    def update_position_stars(self, span=None):
+        self._check(self._lib.pbf_update_position_stars(self._ctx, *(span or self.span())), "update_position_stars")
+
+    def update_velocities(self, span=None):
+        self._check(self._lib.pbf_update_velocities(self._ctx, *(span or self.span())), "update_velocities")
+
+    def apply_surface_tension(self, color_span=None, st_span=None):
+        c = color_span or self.span()
+        s = st_span or self.span()
+        self._check(self._lib.pbf_apply_surface_tension(self._ctx, c[0], c[1], s[0], s[1]), "apply_surface_tension")
+
+    def apply_viscosity(self, span=None):
+        self._check(self._lib.pbf_apply_viscosity(self._ctx, *(span or self.span())), "apply_viscosity")
+
+    def compute_vorticity(self, span=None):
+        self._check(self._lib.pbf_compute_vorticity(self._ctx, *(span or self.span())), "compute_vorticity")
+
+    def apply_vorticity(self, span=None):
+        self._check(self._lib.pbf_apply_vorticity(self._ctx, *(span or self.span())), "apply_vorticity")
+
+    def update_positions(self, span=None):
+        self._check(self._lib.pbf_update_positions(self._ctx, *(span or self.span())), "update_positions")
+
+    # -- fused, graph-captured step (main.cpp:71-124) --
+    def step(self, nsteps: int = 1) -> None:
+        self._check(self._lib.pbf_step(self._ctx, int(nsteps)), "step")
+
+    def sync(self) -> None:
+        self._check(self._lib.pbf_sync(self._ctx), "sync")
+
+    def stream_handle(self) -> int:
+        """The cudaStream_t the context launches on (as an integer handle)."""
+        out = C.c_void_p()
+        self._check(self._lib.pbf_get_stream(self._ctx, C.byref(out)), "get_stream")
+        return int(out.value or 0)
+
+    def stats(self) -> dict:
+        st = PbfStats()
+        self._check(self._lib.pbf_stats(self._ctx, C.byref(st)), "stats")
+        return st.as_dict()
+
+    def neighbors(self, cap: int) -> tuple[np.ndarray, np.ndarray]:
+        n = self.local_count()
+        idx = np.empty((n, cap), np.int32)
+        cnt = np.empty(n, np.int32)
+        self._check(self._lib.pbf_get_neighbors(self._ctx, _ptr(idx), _ptr(cnt)), "get_neighbors")
+        return idx, cnt
+
+    def bins(self) -> dict:
+        n = self.local_count()
+        B = int(self._lib.pbf_num_bins(self._ctx))
+        keys = np.empty(n, np.uint32)
+        ids = np.empty(n, np.uint32)
+        begin = np.empty(B, np.uint32)
+        end = np.empty(B, np.uint32)
+        self._check(self._lib.pbf_get_bins(self._ctx, _ptr(keys), _ptr(ids), _ptr(begin), _ptr(end)), "get_bins")
+        return {"sorted_keys": keys, "sorted_ids": ids, "bin_begin": begin, "bin_end": end}
+
+    def params(self) -> PbfParams:
+        p = PbfParams()
+        self._check(self._lib.pbf_get_params(self._ctx, C.byref(p)), "get_params")
+        return p
+
+    def set_params(self, p: PbfParams) -> None:
+        self._check(self._lib.pbf_set_params(self._ctx, C.byref(p)), "set_params")
+
+    # -- instrumentation --
+    def set_timing(self, on: bool) -> None:
+        self._check(self._lib.pbf_set_timing(self._ctx, int(on)), "set_timing")
+
+    def reset_timing(self) -> None:
+        self._check(self._lib.pbf_reset_timing(self._ctx), "reset_timing")
+
+    def kernel_times(self) -> dict:
+        k = 64
+        names = (C.c_char_p * k)()
+        launches = (C.c_int64 * k)()
+        total = (C.c_double * k)()
+        nk = C.c_int()
+        self._check(self._lib.pbf_kernel_times(self._ctx, k, names, launches, total, C.byref(nk)), "kernel_times")
+        return {names[i].decode(): {"launches": int(launches[i]), "total_ms": float(total[i])} for i in range(nk.value)}
+
+    def launches_per_step(self) -> int:
+        out = C.c_int64()
+        self._check(self._lib.pbf_launches_per_step(self._ctx, C.byref(out)), "launches_per_step")
+        return int(out.value)

@@ -1,0 +1,165 @@
+"""ctypes declarations of the C ABI in include/pbf.h (libpbf_b200.so)."""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+PKG_ROOT = Path(__file__).resolve().parent.parent
+LIB_PATH = PKG_ROOT / "lib" / "libpbf_b200.so"
+
+PBF_OK = 0
+PBF_ERR_ARG = -1
+PBF_ERR_CUDA = -2
+PBF_ERR_CAPACITY = -3
+PBF_ERR_SPAN = -4
+PBF_ERR_PARAMS = -5
+PBF_ERR_STATE = -6
+PBF_ERR_DEVICE = -7
+PBF_ERR_IO = -8
+
+PBF_FLAG_KEY_RANGE = 1
+PBF_FLAG_NONFINITE = 2
+
+ARRAY_POSITIONS = 0
+ARRAY_POSITION_STARS = 1
+ARRAY_VELOCITIES = 2
+ARRAY_SCRATCH = 3
+ARRAY_DENSITIES = 4
+ARRAY_LAMBDAS = 5
+
+F3 = C.c_float * 3
+
+
+class PbfParams(C.Structure):
+    _fields_ = [
+        ("time_step", C.c_float),
+        ("gravity", C.c_float),
+        ("gamma", C.c_float),
+        ("visc_c", C.c_float),
+        ("lambda_epsilon", C.c_float),
+        ("vorticity_coef", C.c_float),
+        ("smoothing_radius", C.c_float),
+        ("neighbor_bin_spacing", C.c_float),
+        ("rest_density", C.c_float),
+        ("rest_mass", C.c_float),
+        ("max_speed", C.c_float),
+        ("particle_rest_spacing", C.c_float),
+        ("boundary_min", F3),
+        ("boundary_max", F3),
+        ("mover_center", F3),
+        ("mover_radius", C.c_float),
+        ("solve_steps", C.c_int32),
+        ("neighbor_cap", C.c_int32),
+        ("scorr_k", C.c_float),
+        ("scorr_n", C.c_float),
+        ("scorr_dq", C.c_float),
+        ("exact_math", C.c_int32),
+        ("reserved", C.c_int32 * 3),
+    ]
+
+    def as_dict(self) -> dict:
+        out = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            out[name] = list(v) if hasattr(v, "__len__") else v
+        return out
+
+
+class PbfStats(C.Structure):
+    _fields_ = [
+        ("n", C.c_uint64),
+        ("mean_density_error", C.c_double),
+        ("max_density_error", C.c_double),
+        ("kinetic_energy", C.c_double),
+        ("center_of_mass", C.c_double * 3),
+        ("mean_neighbors", C.c_double),
+        ("cap_hits", C.c_uint64),
+        ("error_flags", C.c_uint32),
+        ("pad", C.c_uint32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {
+            "n": int(self.n),
+            "mean_density_error": self.mean_density_error,
+            "max_density_error": self.max_density_error,
+            "kinetic_energy": self.kinetic_energy,
+            "center_of_mass": list(self.center_of_mass),
+            "mean_neighbors": self.mean_neighbors,
+            "cap_hits": int(self.cap_hits),
+            "error_flags": int(self.error_flags),
+        }
+
+
+_P = C.POINTER
+_vp = C.c_void_p
+_i = C.c_int
+_sz = C.c_size_t
+_fp = _P(C.c_float)
+
+# name -> (restype, argtypes); every symbol include/pbf.h declares.
+SIGNATURES = {
+    "pbf_params_init": (None, [_P(PbfParams)]),
+    "pbf_params_derive": (_i, [_P(PbfParams), C.c_float, C.c_float]),
+    "pbf_params_from_ini": (_i, [C.c_char_p, _P(PbfParams), _fp, _fp]),
+    "pbf_lattice_dims": (_i, [_fp, _fp, C.c_float, _P(C.c_int64)]),
+    "pbf_build_lattice": (_i, [_fp, _P(C.c_int64), C.c_float, C.c_float, C.c_uint64, _fp]),
+    "pbf_lattice_rest_density": (_i, [_P(PbfParams), C.c_float, _fp]),
+    "pbf_grid_dims": (_i, [_P(PbfParams), _P(C.c_int64)]),
+    "pbf_create": (_i, [_P(PbfParams), _sz, _P(_vp)]),
+    "pbf_destroy": (None, [_vp]),
+    "pbf_last_error": (C.c_char_p, [_vp]),
+    "pbf_create_error": (C.c_char_p, []),
+    "pbf_set_params": (_i, [_vp, _P(PbfParams)]),
+    "pbf_get_params": (_i, [_vp, _P(PbfParams)]),
+    "pbf_upload": (_i, [_vp, _vp, _vp, _sz]),
+    "pbf_download": (_i, [_vp, _vp, _vp, _vp, _vp]),
+    "pbf_count": (_sz, [_vp]),
+    "pbf_get_array": (_i, [_vp, _i, _vp]),
+    "pbf_set_array": (_i, [_vp, _i, _vp]),
+    "pbf_apply_external_forces": (_i, [_vp, _sz, _sz]),
+    "pbf_predict_positions": (_i, [_vp, _sz, _sz]),
+    "pbf_find_neighbors": (_i, [_vp, _sz, _sz, _sz, _sz]),
+    "pbf_compute_densities": (_i, [_vp, _sz, _sz]),
+    "pbf_compute_pressure_lambdas": (_i, [_vp, _sz, _sz]),
+    "pbf_compute_pressure_dps": (_i, [_vp, _sz, _sz, _i]),
+    "pbf_update_position_stars": (_i, [_vp, _sz, _sz]),
+    "pbf_update_velocities": (_i, [_vp, _sz, _sz]),
+    "pbf_apply_surface_tension": (_i, [_vp, _sz, _sz, _sz, _sz]),
+    "pbf_apply_viscosity": (_i, [_vp, _sz, _sz]),
+    "pbf_compute_vorticity": (_i, [_vp, _sz, _sz]),
+    "pbf_apply_vorticity": (_i, [_vp, _sz, _sz]),
+    "pbf_update_positions": (_i, [_vp, _sz, _sz]),
+    "pbf_step": (_i, [_vp, _i]),
+    "pbf_get_neighbors": (_i, [_vp, _vp, _vp]),
+    "pbf_get_bins": (_i, [_vp, _vp, _vp, _vp, _vp]),
+    "pbf_num_bins": (C.c_int64, [_vp]),
+    "pbf_stats": (_i, [_vp, _P(PbfStats)]),
+    "pbf_sync": (_i, [_vp]),
+    "pbf_get_stream": (_i, [_vp, _P(_vp)]),
+    "pbf_set_timing": (_i, [_vp, _i]),
+    "pbf_kernel_times": (_i, [_vp, _i, _P(C.c_char_p), _P(C.c_int64), _P(C.c_double), _P(C.c_int)]),
+    "pbf_reset_timing": (_i, [_vp]),
+    "pbf_launches_per_step": (_i, [_vp, _P(C.c_int64)]),
+}
+
+_lib = None
+
+
+def load(path: Path | None = None) -> C.CDLL:
+    """Load libpbf_b200.so; raises if it has not been built (there is no fallback)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise RuntimeError(
+            f"{p} is missing: build it with `python sph-cpp_b200/build.py` (the PBF step has no CPU fallback)")
+    lib = C.CDLL(str(p))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib

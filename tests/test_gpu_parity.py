@@ -1,0 +1,310 @@
+"""CUDA path (libpbf_b200 through its C ABI) against the oracle and the
+reference's golden vectors.
+
+Bars:
+  - neighbor search (bins, permutation, lists): bit-exact, always;
+  - exact_math = 1: every array bit-exact against the oracle (Jacobi XSPH),
+    stage by stage and over many fused steps;
+  - exact_math = 0 (the fast default): positions after one step within 1e-5
+    relative of the reference's own output; statistics after 100 steps
+    within 1%.
+"""
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle.oracle import (ARRAY_DENSITIES, ARRAY_LAMBDAS, ARRAY_POSITION_STARS, ARRAY_POSITIONS, ARRAY_SCRATCH,
+                           ARRAY_VELOCITIES, OracleSim, RefSim, ref_available)
+from pbf_b200 import Particles, _abi, make_scene
+
+pytestmark = pytest.mark.gpu
+GOLDEN = Path(__file__).resolve().parent / "golden"
+REL_TOL = 1e-5          # positions after one step, relative (to the coordinate scale of the box)
+STAT_TOL = 0.01         # 100-step statistics, relative
+ALL = (ARRAY_POSITIONS, ARRAY_POSITION_STARS, ARRAY_VELOCITIES, ARRAY_SCRATCH, ARRAY_DENSITIES, ARRAY_LAMBDAS)
+NAMES = {ARRAY_POSITIONS: "x", ARRAY_POSITION_STARS: "x*", ARRAY_VELOCITIES: "v", ARRAY_SCRATCH: "scratch",
+         ARRAY_DENSITIES: "rho", ARRAY_LAMBDAS: "lambda"}
+
+
+def pair(scene, visc_mode=0, exact=1):
+    sc = scene.with_(exact_math=exact)
+    p = sc.params()
+    g = Particles(p, sc.n)
+    o = OracleSim(p, sc.n, visc_mode=visc_mode)
+    x = sc.positions()
+    g.upload(x)
+    o.set_state(x)
+    return sc, p, g, o
+
+
+def assert_lists_equal(g, o, cap):
+    gi, gc = g.neighbors(cap)
+    oi, oc = o.neighbors()
+    assert np.array_equal(gc, oc), "neighbor counts differ"
+    assert np.array_equal(gi, oi), "neighbor lists differ"
+
+
+def assert_arrays(g, o, which=ALL, exact=True, rtol=0.0, atol=0.0):
+    for w in which:
+        a, b = g.get_array(w), o.get(w)
+        if exact:
+            bad = np.flatnonzero(a.ravel() != b.ravel())
+            assert bad.size == 0, f"{NAMES[w]}: {bad.size} values differ, first at {bad[:5]}"
+        else:
+            np.testing.assert_allclose(a, b, rtol=rtol, atol=atol, err_msg=NAMES[w])
+
+
+# ---------------------------------------------------------------- stage by stage
+@pytest.mark.parametrize("name", ["dam_2k", "dam_8k"])
+def test_every_stage_bit_exact_vs_oracle(name):
+    sc, p, g, o = pair(make_scene(name))
+    g.apply_external_forces(); o.stage(0)
+    assert_arrays(g, o)
+    g.predict_positions(); o.stage(1)
+    assert_arrays(g, o)
+    g.find_neighbors(); o.stage(2)
+    assert_lists_equal(g, o, p.neighbor_cap)
+    gb, ob = g.bins(), o.bins()
+    for k in ("sorted_keys", "sorted_ids", "bin_begin", "bin_end"):
+        assert np.array_equal(gb[k], ob[k]), k
+    for sub in range(p.solve_steps):
+        g.compute_densities(); o.stage(3, sub)
+        assert_arrays(g, o)
+        g.compute_pressure_lambdas(); o.stage(4, sub)
+        assert_arrays(g, o)
+        g.compute_pressure_dps(substep=sub); o.stage(5, sub)
+        assert_arrays(g, o)
+        g.update_position_stars(); o.stage(6, sub)
+        assert_arrays(g, o)
+    for stage, fn in ((7, g.update_velocities), (9, g.apply_viscosity), (10, g.compute_vorticity),
+                      (11, g.apply_vorticity), (9, g.apply_viscosity), (12, g.update_positions)):
+        fn()
+        o.stage(stage)
+        assert_arrays(g, o)
+
+
+def test_stages_fast_math_within_tolerance():
+    sc, p, g, o = pair(make_scene("dam_2k"), exact=0)
+    for i, fn in enumerate((g.apply_external_forces, g.predict_positions, g.find_neighbors)):
+        fn()
+        o.stage(i)
+    assert_lists_equal(g, o, p.neighbor_cap)
+    for sub in range(p.solve_steps):
+        g.compute_densities(); o.stage(3)
+        g.compute_pressure_lambdas(); o.stage(4)
+        g.compute_pressure_dps(); o.stage(5)
+        g.update_position_stars(); o.stage(6)
+    np.testing.assert_allclose(g.get_array(ARRAY_DENSITIES), o.get(ARRAY_DENSITIES), rtol=1e-5)
+    lam_g, lam_o = g.get_array(ARRAY_LAMBDAS), o.get(ARRAY_LAMBDAS)
+    np.testing.assert_allclose(lam_g, lam_o, rtol=1e-4, atol=1e-5 * np.abs(lam_o).max())
+    np.testing.assert_allclose(g.get_array(ARRAY_POSITION_STARS), o.get(ARRAY_POSITION_STARS), rtol=0,
+                               atol=REL_TOL * max(sc.box_max))
+
+
+# ---------------------------------------------------------------- fused, graph-captured step
+@pytest.mark.parametrize("steps", [1, 20])
+def test_fused_step_bit_exact_vs_oracle(steps):
+    sc, p, g, o = pair(make_scene("dam_8k"))
+    g.step(steps)
+    o.step(steps)
+    assert_arrays(g, o, which=(ARRAY_POSITIONS, ARRAY_VELOCITIES, ARRAY_DENSITIES, ARRAY_LAMBDAS, ARRAY_SCRATCH))
+    assert_lists_equal(g, o, p.neighbor_cap)
+
+
+def test_fused_step_replay_is_deterministic():
+    sc, p, g, _ = pair(make_scene("dam_2k"), exact=0)
+    g.step(5)
+    a = g.download()
+    g.upload(sc.positions())
+    g.step(5)
+    b = g.download()
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_fused_step_fast_vs_reference_golden():
+    """One fast step against the reference's own step-1 output (golden)."""
+    gd = np.load(GOLDEN / "dam_2k_step1.npz")
+    sc = make_scene("dam_2k")
+    p = sc.params()
+    assert np.float32(p.rest_density) == gd["rest_density"]
+    g = Particles(p, sc.n)
+    g.upload(gd["x0"])
+    g.step(1)
+    x = g.positions()
+    scale = max(sc.box_max)
+    np.testing.assert_allclose(x, gd["x1"], rtol=0, atol=REL_TOL * scale)
+    # the lists the step built are the reference's, bit for bit
+    idx, cnt = g.neighbors(60)
+    assert np.array_equal(cnt, gd["cnt"].astype(np.int32))
+    ref = gd["nbr"].astype(np.int32)
+    mask = np.arange(60)[None, :] < cnt[:, None]
+    assert np.array_equal(np.where(mask, idx, -1), np.where(mask, ref, -1))
+    b = g.bins()
+    for k in ("sorted_keys", "sorted_ids", "bin_begin", "bin_end"):
+        assert np.array_equal(b[k], gd[k]), k
+
+
+def test_fused_step_exact_positions_bitwise_vs_reference_golden():
+    """exact_math: x after step 1 is bit-identical to the reference's."""
+    gd = np.load(GOLDEN / "dam_2k_step1.npz")
+    sc = make_scene("dam_2k", exact_math=1)
+    g = Particles(sc.params(), sc.n)
+    g.upload(gd["x0"])
+    g.step(1)
+    assert np.array_equal(g.positions(), gd["x1"])
+    assert np.array_equal(g.densities(), gd["rho"])
+    assert np.array_equal(g.lambdas(), gd["lam"])
+
+
+def _stat_close(a: dict, b: dict, keys=("mean_density_error", "max_density_error", "kinetic_energy")):
+    for k in keys:
+        assert a[k] == pytest.approx(b[k], rel=STAT_TOL), (k, a[k], b[k])
+    for i in range(3):
+        assert a["center_of_mass"][i] == pytest.approx(b["center_of_mass"][i], rel=STAT_TOL)
+
+
+def test_golden_trajectory_statistics_fast():
+    gd = np.load(GOLDEN / "dam_2k_traj.npz")
+    sc = make_scene("dam_2k")
+    g = Particles(sc.params(), sc.n)
+    g.upload(sc.positions())
+    cols = list(gd["columns"])
+    for s in range(int(gd["steps"])):
+        g.step(1)
+    st = g.stats()
+    row = gd["stats"][-1]
+    ref = {"mean_density_error": row[cols.index("mean_err")], "max_density_error": row[cols.index("max_err")],
+           "kinetic_energy": row[cols.index("ke")],
+           "center_of_mass": [row[cols.index("cx")], row[cols.index("cy")], row[cols.index("cz")]]}
+    _stat_close(st, ref)
+
+
+def test_65k_100_steps_statistics_vs_oracle_and_reference():
+    sc = make_scene("dam_65k")
+    p = sc.params()
+    g = Particles(p, sc.n)
+    x = sc.positions()
+    g.upload(x)
+    g.step(sc.steps)
+    st = g.stats()
+    o = OracleSim(p, sc.n, visc_mode=0)
+    o.set_state(x)
+    o.step(sc.steps)
+    _stat_close(st, o.stats())
+    if ref_available():
+        r = RefSim(p, sc.n)
+        r.set_state(x)
+        r.step(sc.steps)
+        _stat_close(st, r.stats(p))
+
+
+# ---------------------------------------------------------------- variants
+def test_neighbor_cap_64_bit_exact():
+    sc, p, g, o = pair(make_scene("dam_8k", neighbor_cap=64))
+    g.step(3)
+    o.step(3)
+    assert_lists_equal(g, o, 64)
+    assert_arrays(g, o, which=(ARRAY_POSITIONS, ARRAY_VELOCITIES))
+
+
+def test_scorr_matches_oracle():
+    sc, p, g, o = pair(make_scene("dam_2k", scorr=(0.1, 4.0, 0.2)), exact=1)
+    g.step(2)
+    o.step(2)
+    np.testing.assert_allclose(g.positions(), o.get(ARRAY_POSITIONS), rtol=0, atol=REL_TOL * max(sc.box_max))
+
+
+def test_surface_tension_bit_exact():
+    sc, p, g, o = pair(make_scene("dam_2k", gamma=600.0))
+    g.step(3)
+    o.step(3)
+    assert_arrays(g, o, which=(ARRAY_POSITIONS, ARRAY_VELOCITIES, ARRAY_DENSITIES, ARRAY_SCRATCH))
+    sc, p, g, o = pair(make_scene("dam_2k", gamma=600.0))
+    for i in range(3):
+        [g.apply_external_forces, g.predict_positions, g.find_neighbors][i]()
+        o.stage(i)
+    g.compute_densities(); o.stage(3)
+    g.apply_surface_tension(); o.stage(8)
+    assert_arrays(g, o, which=(ARRAY_VELOCITIES, ARRAY_SCRATCH))
+
+
+def test_mover_sphere_push():
+    """apply_boundary_conditions (particles.h:514-522) with the mover inside the fluid."""
+    sc, p, g, o = pair(make_scene("dam_2k", mover_center=(4.0, 2.0, 2.0)))
+    g.step(2)
+    o.step(2)
+    assert_arrays(g, o, which=(ARRAY_POSITIONS, ARRAY_VELOCITIES))
+
+
+# ---------------------------------------------------------------- edge cases and errors
+def test_empty_and_single_particle():
+    sc = make_scene("dam_2k")
+    p = sc.params()
+    g = Particles(p, 16)
+    g.upload(np.zeros((0, 3), np.float32))
+    g.step(3)
+    assert g.local_count() == 0
+    assert g.stats()["n"] == 0
+    one = np.array([[3.0, 3.0, 3.0]], np.float32)
+    g.upload(one)
+    o = OracleSim(p, 16)
+    o.set_state(one)
+    g.step(2)
+    o.step(2)
+    assert np.array_equal(g.positions(), o.get(ARRAY_POSITIONS))
+    idx, cnt = g.neighbors(p.neighbor_cap)
+    assert cnt.tolist() == [0]
+
+
+def test_errors_are_reported_not_faulted():
+    sc = make_scene("dam_2k")
+    p = sc.params()
+    g = Particles(p, 100)
+    with pytest.raises(RuntimeError, match="capacity"):
+        g.upload(np.zeros((101, 3), np.float32))
+    g.upload(sc.positions()[:100])
+    with pytest.raises(RuntimeError, match="span"):
+        g.apply_external_forces((0, 50))
+    with pytest.raises(RuntimeError, match="neighbor lists"):
+        g.compute_densities()
+    g.find_neighbors()
+    g.compute_densities()
+    st = g.stats()
+    assert st["error_flags"] == 0
+
+
+def test_all_particles_in_one_cell():
+    """Degenerate input: every particle at the same wall corner (coincident
+    neighbours trigger the density nudge of particles.h:303-305)."""
+    sc = make_scene("dam_2k")
+    p = sc.params()
+    x = np.zeros((100, 3), np.float32)
+    v = np.tile(np.array([[0.5, -1.0, 0.25]], np.float32), (100, 1))
+    g = Particles(p, 100)
+    o = OracleSim(p, 100)
+    g.upload(x, v)
+    o.set_state(x, v)
+    for i, fn in enumerate((g.apply_external_forces, g.predict_positions, g.find_neighbors)):
+        fn()
+        o.stage(i)
+    assert_lists_equal(g, o, p.neighbor_cap)
+    gi, gc = g.neighbors(p.neighbor_cap)
+    assert gc.min() == 60
+
+
+def test_timing_api_counts_every_kernel():
+    sc = make_scene("dam_2k")
+    g = Particles(sc.params(), sc.n)
+    g.upload(sc.positions())
+    g.set_timing(True)
+    g.step(2)
+    t = g.kernel_times()
+    g.set_timing(False)
+    launches = sum(v["launches"] for v in t.values())
+    assert launches == 2 * g.launches_per_step()
+    assert t["density_lambda"]["launches"] == 2 * sc.solve_steps
+    assert all(v["total_ms"] > 0 for v in t.values())
