@@ -1444,7 +1444,11 @@ int pbf_update_positions(pbf_ctx* ctx, size_t b, size_t e) {
 
 int pbf_step(pbf_ctx* ctx, int nsteps) {
   if (!ctx || nsteps < 0) return PBF_ERR_ARG;
-  if (ctx->n == 0 || nsteps == 0) return PBF_OK;
+  if (nsteps == 0) return PBF_OK;
+  if (ctx->n == 0) {
+    ctx->lists_valid = true;  // an empty set has (empty) lists
+    return PBF_OK;
+  }
   if (ctx->timing) {
     for (int i = 0; i < nsteps; ++i) launch_step(ctx);
     int rc = check_launch(ctx, "step");
