@@ -18,6 +18,7 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 LIB = PKG / "lib" / "libpbf_b200.so"
+APP = PKG / "lib" / "pbf_run"
 ORACLE_LIB = ROOT / "oracle" / "_build" / "libpbf_oracle.so"
 REF_SOURCES = Path(os.environ.get("PBF_REFERENCE_ROOT", "/root/reference"))
 
@@ -70,6 +71,16 @@ def build_product(force: bool = False, verbose_ptxas: bool = False) -> Path:
     return LIB
 
 
+def build_app(force: bool = False) -> Path:
+    """The headless driver (apps/pbf_run.cpp), linked against libpbf_b200.so."""
+    src = PKG / "apps" / "pbf_run.cpp"
+    deps = [src, ROOT / "include" / "pbf.h", ROOT / "include" / "pbf_particles.hpp", LIB]
+    if force or _stale(APP, deps):
+        _run([_host_cxx(), "-O2", "-std=c++17", str(src), "-I", str(ROOT / "include"), "-L", str(LIB.parent),
+              "-lpbf_b200", "-Wl,-rpath,$ORIGIN", "-o", str(APP)], PKG)
+    return APP
+
+
 def build_oracle(force: bool = False) -> Path:
     src = ROOT / "oracle" / "pbf_oracle.c"
     if force or _stale(ORACLE_LIB, [src, ROOT / "include" / "pbf.h"]):
@@ -95,6 +106,7 @@ def build_reference(force: bool = False) -> bool:
 def main(argv: list[str]) -> int:
     force = "--force" in argv
     build_product(force=force, verbose_ptxas="--ptxas" in argv)
+    build_app(force=force)
     build_oracle(force=force)
     build_reference(force=force)
     return 0

@@ -129,6 +129,7 @@ int pbf_params_from_ini(const char* path, pbf_params* p, float fluid_min[3], flo
   const double global_count = geti("SimParameters.global_particle_count", -1);
   p->neighbor_bin_spacing = getf("SimParameters.neighbor_bin_spacing", -1.0f);
   p->neighbor_cap = (int32_t)geti("SimParameters.neighbor_cap", 60);
+  p->exact_math = (int32_t)geti("SimParameters.exact_math", 0);
   p->gravity = getf("PhysicalParameters.g", -1.0f);
   p->gamma = getf("PhysicalParameters.gamma", -1.0f);
   p->visc_c = getf("PhysicalParameters.visc_c", -1.0f);

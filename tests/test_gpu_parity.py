@@ -98,8 +98,10 @@ def test_stages_fast_math_within_tolerance():
         g.compute_pressure_dps(); o.stage(5)
         g.update_position_stars(); o.stage(6)
     np.testing.assert_allclose(g.get_array(ARRAY_DENSITIES), o.get(ARRAY_DENSITIES), rtol=1e-5)
+    # lambda = -C/(sum|grad C|^2 + eps) with C = rho/rho0 - 1: a 1e-5 relative
+    # density difference moves C by up to 1e-5, so lambda by 1e-5/eps.
     lam_g, lam_o = g.get_array(ARRAY_LAMBDAS), o.get(ARRAY_LAMBDAS)
-    np.testing.assert_allclose(lam_g, lam_o, rtol=1e-4, atol=1e-5 * np.abs(lam_o).max())
+    np.testing.assert_allclose(lam_g, lam_o, rtol=1e-4, atol=1e-5 / p.lambda_epsilon)
     np.testing.assert_allclose(g.get_array(ARRAY_POSITION_STARS), o.get(ARRAY_POSITION_STARS), rtol=0,
                                atol=REL_TOL * max(sc.box_max))
 
@@ -183,23 +185,68 @@ def test_golden_trajectory_statistics_fast():
     _stat_close(st, ref)
 
 
-def test_65k_100_steps_statistics_vs_oracle_and_reference():
+def test_65k_100_steps_exact_bitwise_vs_oracle():
+    """exact_math over the full 100-step 65k run: every position and velocity
+    bit-identical to the oracle (Jacobi XSPH), hence identical statistics."""
+    sc, p, g, o = pair(make_scene("dam_65k"))
+    g.step(sc.steps)
+    o.step(sc.steps)
+    assert_arrays(g, o, which=(ARRAY_POSITIONS, ARRAY_VELOCITIES, ARRAY_DENSITIES))
+    a, b = g.stats(), o.stats()
+    for k in ("mean_density_error", "max_density_error", "kinetic_energy"):
+        assert a[k] == pytest.approx(b[k], rel=1e-12), k
+
+
+# Statistics after 100 steps of the 65k dam, fast math against the oracle.
+# The reference disagrees with ITSELF beyond 1% on the density-error
+# statistics: its in-place XSPH (particles.h:436-447) makes every OpenMP run
+# different.  Measured on the 65k dam after 100 steps, reference at 2 and 8
+# threads and the oracle (Jacobi):
+#   eps = 600: mean err 0.427-0.459 (7.5%), max err 3.58-4.37 (22%),
+#              KE 3.49e7-3.56e7 (2%), centre of mass 0.1%
+#   eps = 1:   mean err 0.00781-0.00799 (2.2%), p90 2%, max 0.102-0.120 (17%),
+#              KE 0.04%, centre of mass 0.01%
+# KE and centre of mass are held to 1% (2% for KE at eps = 600); the
+# density-error statistics to the reference's own spread above.
+STAT_BARS = {
+    600.0: {"mean_density_error": 0.08, "max_density_error": 0.25, "kinetic_energy": 0.02, "com": 0.01},
+    1.0: {"mean_density_error": 0.03, "max_density_error": 0.20, "kinetic_energy": 0.01, "com": 0.01},
+}
+
+
+@pytest.mark.parametrize("eps", [600.0, 1.0])
+def test_65k_100_steps_fast_statistics(eps):
+    sc, p, g, o = pair(make_scene("dam_65k", lambda_epsilon=eps), exact=0)
+    g.step(sc.steps)
+    o.step(sc.steps)
+    a, b = g.stats(), o.stats()
+    bars = STAT_BARS[eps]
+    for k in ("mean_density_error", "max_density_error", "kinetic_energy"):
+        assert a[k] == pytest.approx(b[k], rel=bars[k]), (k, a[k], b[k])
+    for i in range(3):
+        assert a["center_of_mass"][i] == pytest.approx(b["center_of_mass"][i], rel=bars["com"])
+    assert a["error_flags"] == 0
+
+
+def test_65k_100_steps_fast_vs_reference_build():
+    """The same run against the reference's own OpenMP build (when present)."""
+    if not ref_available():
+        pytest.skip("reference build not present")
     sc = make_scene("dam_65k")
     p = sc.params()
     g = Particles(p, sc.n)
     x = sc.positions()
     g.upload(x)
     g.step(sc.steps)
-    st = g.stats()
-    o = OracleSim(p, sc.n, visc_mode=0)
-    o.set_state(x)
-    o.step(sc.steps)
-    _stat_close(st, o.stats())
-    if ref_available():
-        r = RefSim(p, sc.n)
-        r.set_state(x)
-        r.step(sc.steps)
-        _stat_close(st, r.stats(p))
+    r = RefSim(p, sc.n)
+    r.set_state(x)
+    r.step(sc.steps)
+    a, b = g.stats(), r.stats(p)
+    bars = STAT_BARS[600.0]
+    for k in ("mean_density_error", "max_density_error", "kinetic_energy"):
+        assert a[k] == pytest.approx(b[k], rel=bars[k]), (k, a[k], b[k])
+    for i in range(3):
+        assert a["center_of_mass"][i] == pytest.approx(b["center_of_mass"][i], rel=bars["com"])
 
 
 # ---------------------------------------------------------------- variants
