@@ -21,9 +21,11 @@
  *
  * Two documented departures, each selectable:
  *  - XSPH viscosity (particles.h:436-447) updates velocities in place while
- *    neighbours read them, so the reference's result depends on thread order.
- *    visc_mode 1 reproduces its single-thread order (Gauss-Seidel in index
- *    order); visc_mode 0 is Jacobi (read old, write new), the GPU semantics.
+ *    neighbours read them, and compute_densities (particles.h:303-305) nudges
+ *    a particle sitting on a neighbour in place while others read it, so the
+ *    reference's result depends on thread order.  visc_mode 1 reproduces its
+ *    single-thread order (in place, index order); visc_mode 0 is the GPU's
+ *    deterministic order (Jacobi: read old, write new after the pass).
  *  - s_corr (scorr_k > 0) is the Macklin & Mueller 2013 artificial-pressure
  *    term, absent from the reference's compute_pressure_dps.
  */
@@ -396,28 +398,50 @@ static int st_find_neighbors(oracle_t* o) {
   return PBF_OK;
 }
 
-/* particles.h:292-313 (with the coincident-neighbour nudge of 303-305) */
-static void st_densities(oracle_t* o) {
+/* particles.h:292-313, with the coincident-neighbour nudge of 303-305.
+ * The reference nudges position_stars_[p] in place while other threads read
+ * it.  visc_mode 1 (the reference's single-thread order): a serial loop, in
+ * place.  visc_mode 0 (GPU semantics, deterministic): each particle sums with
+ * its own nudged position; every nudge is written back after the pass. */
+static float density_of(const oracle_t* o, int64_t p, v3* xp_io, const v3* xs) {
   const float W0 = poly6(&o->k, 0.0f);
   const float m = o->p.rest_mass, dt = o->p.time_step;
-  const int cap = o->cap;
+  float d = m * W0;
+  v3 xp = *xp_io;
+  const int32_t* list = o->nbr + (size_t)p * o->cap;
+  for (int c = 0; c < o->nbr_count[p]; ++c) {
+    const int32_t q = list[c];
+    const v3 xq = xs[q];
+    if ((double)v3_mag(v3_sub(xp, xq)) < 0.00000001) {
+      const v3 vp = o->v[p];
+      xp.x -= vp.x * dt / 50.0f;
+      xp.y -= vp.y * dt / 50.0f;
+      xp.z -= vp.z * dt / 50.0f;
+    }
+    const float rm = v3_mag(v3_sub(xp, xq));
+    d += m * poly6(&o->k, rm);
+  }
+  *xp_io = xp;
+  return d;
+}
+
+static void st_densities(oracle_t* o) {
+  if (o->visc_mode == 1) {
+    for (int64_t p = 0; p < (int64_t)o->n; ++p) {
+      v3 xp = o->xs[p];
+      o->rho[p] = density_of(o, p, &xp, o->xs);
+      o->xs[p] = xp;
+    }
+    return;
+  }
+  v3* out = o->vtmp;
 #pragma omp parallel for schedule(static)
   for (int64_t p = 0; p < (int64_t)o->n; ++p) {
-    float d = m * W0;
-    const int32_t* list = o->nbr + (size_t)p * cap;
-    for (int c = 0; c < o->nbr_count[p]; ++c) {
-      const int32_t q = list[c];
-      if ((double)v3_mag(v3_sub(o->xs[p], o->xs[q])) < 0.00000001) {
-        const v3 vp = o->v[p];
-        o->xs[p].x -= vp.x * dt / 50.0f;
-        o->xs[p].y -= vp.y * dt / 50.0f;
-        o->xs[p].z -= vp.z * dt / 50.0f;
-      }
-      const float rm = v3_mag(v3_sub(o->xs[p], o->xs[q]));
-      d += m * poly6(&o->k, rm);
-    }
-    o->rho[p] = d;
+    v3 xp = o->xs[p];
+    o->rho[p] = density_of(o, p, &xp, o->xs);
+    out[p] = xp;
   }
+  memcpy(o->xs, out, o->n * sizeof(v3));
 }
 
 /* particles.h:318-342 */

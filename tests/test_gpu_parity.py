@@ -197,56 +197,65 @@ def test_65k_100_steps_exact_bitwise_vs_oracle():
         assert a[k] == pytest.approx(b[k], rel=1e-12), k
 
 
-# Statistics after 100 steps of the 65k dam, fast math against the oracle.
-# The reference disagrees with ITSELF beyond 1% on the density-error
-# statistics: its in-place XSPH (particles.h:436-447) makes every OpenMP run
-# different.  Measured on the 65k dam after 100 steps, reference at 2 and 8
-# threads and the oracle (Jacobi):
-#   eps = 600: mean err 0.427-0.459 (7.5%), max err 3.58-4.37 (22%),
-#              KE 3.49e7-3.56e7 (2%), centre of mass 0.1%
-#   eps = 1:   mean err 0.00781-0.00799 (2.2%), p90 2%, max 0.102-0.120 (17%),
-#              KE 0.04%, centre of mass 0.01%
-# KE and centre of mass are held to 1% (2% for KE at eps = 600); the
-# density-error statistics to the reference's own spread above.
+# Statistics of the 65k dam over steps 81-100 (the mean of the 20 per-step
+# values), fast math against the oracle and the reference.  The reference
+# disagrees with ITSELF from run to run (its in-place XSPH and nudge races,
+# particles.h:303-305, 436-447): single-step snapshots after 100 steps spread
+# 7.5% (mean density error) and 22% (max) between its OpenMP runs at
+# eps = 600.  Averaged over steps 81-100 the spread between the reference at 2
+# and 8 threads, the oracle, and the oracle started 1 ulp off is:
+#   eps = 600: mean err 0.69%, max err 0.55%, KE 1.01%, centre of mass 0.16%
+#   eps = 1:   mean err 0.74%, max err 5.5%,  KE 0.06%, centre of mass 0.02%
+# and one more reference run at eps = 600 gave an averaged max error of 3.683
+# against 3.741-3.763 for the others (2.2%): at this eps the max is set by
+# particles piled exactly into wall corners.
+# The bars: 1% wherever the spread is below 1%, else about twice the spread.
 STAT_BARS = {
-    600.0: {"mean_density_error": 0.08, "max_density_error": 0.25, "kinetic_energy": 0.02, "com": 0.01},
-    1.0: {"mean_density_error": 0.03, "max_density_error": 0.20, "kinetic_energy": 0.01, "com": 0.01},
+    600.0: {"mean_density_error": 0.01, "max_density_error": 0.05, "kinetic_energy": 0.015, "com": 0.01},
+    1.0: {"mean_density_error": 0.01, "max_density_error": 0.06, "kinetic_energy": 0.01, "com": 0.01},
 }
+STAT_KEYS = ("mean_density_error", "max_density_error", "kinetic_energy")
+
+
+def averaged_stats(sim, stats, steps=100, window=20):
+    sim.step(steps - window)
+    acc = []
+    for _ in range(window):
+        sim.step(1)
+        st = stats()
+        acc.append([st[k] for k in STAT_KEYS] + list(st["center_of_mass"]))
+    m = np.mean(acc, axis=0)
+    return dict(zip(STAT_KEYS, m[:3])) | {"center_of_mass": list(m[3:])}
+
+
+def check_bars(a, b, bars):
+    for k in STAT_KEYS:
+        assert a[k] == pytest.approx(b[k], rel=bars[k]), (k, a[k], b[k])
+    for i in range(3):
+        assert a["center_of_mass"][i] == pytest.approx(b["center_of_mass"][i], rel=bars["com"])
 
 
 @pytest.mark.parametrize("eps", [600.0, 1.0])
 def test_65k_100_steps_fast_statistics(eps):
     sc, p, g, o = pair(make_scene("dam_65k", lambda_epsilon=eps), exact=0)
-    g.step(sc.steps)
-    o.step(sc.steps)
-    a, b = g.stats(), o.stats()
-    bars = STAT_BARS[eps]
-    for k in ("mean_density_error", "max_density_error", "kinetic_energy"):
-        assert a[k] == pytest.approx(b[k], rel=bars[k]), (k, a[k], b[k])
-    for i in range(3):
-        assert a["center_of_mass"][i] == pytest.approx(b["center_of_mass"][i], rel=bars["com"])
-    assert a["error_flags"] == 0
+    a = averaged_stats(g, g.stats)
+    b = averaged_stats(o, o.stats)
+    check_bars(a, b, STAT_BARS[eps])
+    assert g.stats()["error_flags"] == 0
 
 
 def test_65k_100_steps_fast_vs_reference_build():
-    """The same run against the reference's own OpenMP build (when present)."""
+    """The same averaged statistics against the reference's own OpenMP build."""
     if not ref_available():
         pytest.skip("reference build not present")
     sc = make_scene("dam_65k")
     p = sc.params()
-    g = Particles(p, sc.n)
     x = sc.positions()
+    g = Particles(p, sc.n)
     g.upload(x)
-    g.step(sc.steps)
     r = RefSim(p, sc.n)
     r.set_state(x)
-    r.step(sc.steps)
-    a, b = g.stats(), r.stats(p)
-    bars = STAT_BARS[600.0]
-    for k in ("mean_density_error", "max_density_error", "kinetic_energy"):
-        assert a[k] == pytest.approx(b[k], rel=bars[k]), (k, a[k], b[k])
-    for i in range(3):
-        assert a["center_of_mass"][i] == pytest.approx(b["center_of_mass"][i], rel=bars["com"])
+    check_bars(averaged_stats(g, g.stats), averaged_stats(r, lambda: r.stats(p)), STAT_BARS[600.0])
 
 
 # ---------------------------------------------------------------- variants
@@ -341,6 +350,46 @@ def test_all_particles_in_one_cell():
     assert_lists_equal(g, o, p.neighbor_cap)
     gi, gc = g.neighbors(p.neighbor_cap)
     assert gc.min() == 60
+
+
+def _coincident_scene():
+    sc = make_scene("dam_2k")
+    x = sc.positions()
+    x[1::97] = x[0::97][: x[1::97].shape[0]]  # every 97th particle sits exactly on its predecessor
+    v = np.zeros_like(x)
+    v[:, 1] = -0.5
+    v[::5, 0] = 0.25
+    return sc, x, v
+
+
+def test_coincident_particles_nudge_fused_bit_exact():
+    """compute_densities' nudge of a particle sitting on a neighbour
+    (particles.h:303-305), deterministic order, through the fused step."""
+    sc, x, v = _coincident_scene()
+    p = sc.with_(exact_math=1).params()
+    g = Particles(p, sc.n)
+    o = OracleSim(p, sc.n)
+    g.upload(x, v)
+    o.set_state(x, v)
+    g.step(3)
+    o.step(3)
+    assert_arrays(g, o, which=(ARRAY_POSITIONS, ARRAY_VELOCITIES, ARRAY_DENSITIES, ARRAY_LAMBDAS))
+
+
+def test_coincident_particles_nudge_stages_bit_exact():
+    sc, x, v = _coincident_scene()
+    p = sc.with_(exact_math=1).params()
+    g = Particles(p, sc.n)
+    o = OracleSim(p, sc.n)
+    g.upload(x, v)
+    o.set_state(x, v)
+    for i, fn in enumerate((g.apply_external_forces, g.predict_positions, g.find_neighbors)):
+        fn()
+        o.stage(i)
+    g.compute_densities(); o.stage(3)
+    assert_arrays(g, o, which=(ARRAY_POSITION_STARS, ARRAY_DENSITIES))
+    g.compute_pressure_lambdas(); o.stage(4)
+    assert_arrays(g, o, which=(ARRAY_LAMBDAS,))
 
 
 def test_timing_api_counts_every_kernel():
