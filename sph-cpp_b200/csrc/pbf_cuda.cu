@@ -333,11 +333,15 @@ __global__ void __launch_bounds__(kBlock) k_fill(Dev P, int n, size_t stride, co
 }
 
 // ---- density (particles.h:292-313) ----
-// Per-stage form: writes rho into vel.w and, when a neighbour coincides, the
-// nudged x* back (the reference writes position_stars_[p] in place).
+// Per-stage form: writes rho into vel.w.  A particle sitting on a neighbour is
+// nudged (particles.h:303-305); the reference writes position_stars_[p] in
+// place while other threads read it.  Here each particle sums with its own
+// nudged position and every position goes to pst_out, copied back after the
+// pass (deterministic: neighbours see nudges from the next stage on).
 template <bool X>
 __global__ void __launch_bounds__(kBlock) k_density(Dev P, int n, size_t stride, const int32_t* __restrict__ nbr,
-                                                    const int32_t* __restrict__ cnt, float4* pst, float4* vel) {
+                                                    const int32_t* __restrict__ cnt, const float4* __restrict__ pst,
+                                                    float4* vel, float4* pst_out) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= n) return;
   float4 xp = pst[b];
@@ -361,7 +365,8 @@ __global__ void __launch_bounds__(kBlock) k_density(Dev P, int n, size_t stride,
     rho = pbf::A<X>(rho, pbf::M<X>(P.m, pbf::poly6<X>(P, rm)));
   }
   vel[b].w = rho;
-  if (nudged) pst[b] = xp;
+  pst_out[b] = xp;
+  (void)nudged;
 }
 
 // compute_pressure_lambdas (particles.h:318-342), per-stage form.
@@ -405,15 +410,17 @@ __global__ void __launch_bounds__(kBlock) k_lambda(Dev P, int n, size_t stride, 
 
 // Fused density + lambda: one neighbour pass computes rho_p and the gradient
 // sums (lambda needs only its own density).  Writes xl = (x*, lambda) for the
-// delta-p gather, rho into vel.w and lambda into the home lambda array.  If a
-// neighbour coincides (particles.h:303-305) the nudged x* travels in xl and the
-// gradient sums are recomputed with it.
+// delta-p gather, rho into vel.w and lambda into the home lambda array.  When
+// a particle sits on a neighbour it is nudged (particles.h:303-305) and the
+// launch raises *nudge: k_lambda_fixup then recomputes every lambda from the
+// nudged positions, which is what a separate lambda stage after the density
+// stage sees.
 template <bool X>
 __global__ void __launch_bounds__(kBlock) k_density_lambda(Dev P, int n, size_t stride,
                                                            const int32_t* __restrict__ nbr,
                                                            const int32_t* __restrict__ cnt,
                                                            const float4* __restrict__ pst, float4* xl,
-                                                           float4* vel, float* lam) {
+                                                           float4* vel, float* lam, uint32_t* nudge) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= n) return;
   float4 xp = pst[b];
@@ -438,19 +445,34 @@ __global__ void __launch_bounds__(kBlock) k_density_lambda(Dev P, int n, size_t 
     rho = pbf::A<X>(rho, pbf::M<X>(P.m, pbf::poly6<X>(P, rm)));
     lambda_terms<X>(P, rx, ry, rz, rm, sg, sumC);
   }
-  if (nudged) {
-    sg = make_float3(0.f, 0.f, 0.f);
-    sumC = 0.0f;
-    for (int k = 0; k < c; ++k) {
-      const float4 xq = pst[nbr[(size_t)k * stride + b]];
-      const float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
-      lambda_terms<X>(P, rx, ry, rz, pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz)), sg, sumC);
-    }
-  }
+  if (nudged) *nudge = 1u;
   const float l = lambda_of<X>(P, rho, sg, sumC);
   xl[b] = make_float4(xp.x, xp.y, xp.z, l);
   vel[b].w = rho;
   lam[b] = l;
+}
+
+// Lambda recomputed from the (nudged) positions in xl, only when the
+// preceding density_lambda launch nudged a particle; otherwise every block
+// returns at once.
+template <bool X>
+__global__ void __launch_bounds__(kBlock) k_lambda_fixup(Dev P, int n, size_t stride, const int32_t* __restrict__ nbr,
+                                                         const int32_t* __restrict__ cnt,
+                                                         const float4* __restrict__ xl, const float4* __restrict__ vel,
+                                                         float* lam, const uint32_t* __restrict__ nudge) {
+  if (*nudge == 0u) return;
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  const float4 xp = xl[b];
+  const int c = cnt[b];
+  float3 sg = make_float3(0.f, 0.f, 0.f);
+  float sumC = 0.0f;
+  for (int k = 0; k < c; ++k) {
+    const float4 xq = xl[nbr[(size_t)k * stride + b]];
+    const float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
+    lambda_terms<X>(P, rx, ry, rz, pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz)), sg, sumC);
+  }
+  lam[b] = lambda_of<X>(P, vel[b].w, sg, sumC);
 }
 
 // compute_pressure_dps (particles.h:348-358) summand; s_corr optional.
@@ -519,16 +541,28 @@ __global__ void k_update_v(Dev P, int n, const float4* __restrict__ pst, const f
 template <bool X, bool SCORR, bool LAST>
 __global__ void __launch_bounds__(kBlock) k_dp_update(Dev P, int n, size_t stride, const int32_t* __restrict__ nbr,
                                                       const int32_t* __restrict__ cnt, const float4* __restrict__ xl,
-                                                      float4* pst, const float4* __restrict__ pos, float4* vel) {
+                                                      float4* pst, const float4* __restrict__ pos, float4* vel,
+                                                      const float* __restrict__ lam,
+                                                      const uint32_t* __restrict__ nudge) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= n) return;
   const float4 xp = xl[b];
   const int c = cnt[b];
   float3 dp = make_float3(0.f, 0.f, 0.f);
-  for (int k = 0; k < c; ++k) {
-    const float4 xq = xl[nbr[(size_t)k * stride + b]];
-    const float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
-    dp_term<X, SCORR>(P, xp.w, xq.w, rx, ry, rz, pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz)), dp);
+  if (*nudge == 0u) {
+    for (int k = 0; k < c; ++k) {
+      const float4 xq = xl[nbr[(size_t)k * stride + b]];
+      const float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
+      dp_term<X, SCORR>(P, xp.w, xq.w, rx, ry, rz, pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz)), dp);
+    }
+  } else {  // lambdas were recomputed by k_lambda_fixup
+    const float lp = lam[b];
+    for (int k = 0; k < c; ++k) {
+      const int q = nbr[(size_t)k * stride + b];
+      const float4 xq = xl[q];
+      const float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
+      dp_term<X, SCORR>(P, lp, lam[q], rx, ry, rz, pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz)), dp);
+    }
   }
   const float dx = pbf::M<X>(P.inv_rho0, dp.x), dy = pbf::M<X>(P.inv_rho0, dp.y), dz = pbf::M<X>(P.inv_rho0, dp.z);
   const float3 s = pbf::boundary(P, make_float3(pbf::xadd(xp.x, dx), pbf::xadd(xp.y, dy), pbf::xadd(xp.z, dz)));
@@ -779,7 +813,7 @@ struct pbf_ctx {
   float4 *posS = nullptr, *pstS = nullptr, *velS = nullptr, *scrS = nullptr, *xl = nullptr, *velT = nullptr;
   float *lamH = nullptr, *lamS = nullptr;
   uint32_t *origH = nullptr, *origS = nullptr, *key = nullptr, *rank = nullptr, *keyH = nullptr;
-  uint32_t *cell_count = nullptr, *cell_start = nullptr, *scan_part = nullptr, *err = nullptr;
+  uint32_t *cell_count = nullptr, *cell_start = nullptr, *scan_part = nullptr, *err = nullptr, *nudge = nullptr;
   unsigned long long* pairs = nullptr;
   int32_t *nbr = nullptr, *cnt = nullptr;
   float* stage = nullptr;  // 6*C floats: two AoS float3 staging areas
@@ -1039,18 +1073,24 @@ void launch_step_t(pbf_ctx* ctx) {
   launch_fill(ctx, ctx->pstS);
   const int K = ctx->params.solve_steps;
   for (int it = 0; it < K; ++it) {
+    cudaMemsetAsync(ctx->nudge, 0, sizeof(uint32_t), s);
     {
       Launch L(ctx, "density_lambda");
       k_density_lambda<X><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl, ctx->velS,
-                                               ctx->lamH);
+                                               ctx->lamH, ctx->nudge);
+    }
+    {
+      Launch L(ctx, "lambda_fixup");
+      k_lambda_fixup<X><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->velS, ctx->lamH,
+                                             ctx->nudge);
     }
     Launch L(ctx, "dp_update");
     if (it == K - 1)
       k_dp_update<X, SCORR, true><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS,
-                                                       ctx->posS, ctx->velS);
+                                                       ctx->posS, ctx->velS, ctx->lamH, ctx->nudge);
     else
       k_dp_update<X, SCORR, false><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS,
-                                                        ctx->posS, ctx->velS);
+                                                        ctx->posS, ctx->velS, ctx->lamH, ctx->nudge);
   }
   if (K == 0) {
     Launch L(ctx, "update_velocities");
@@ -1095,11 +1135,12 @@ void launch_step(pbf_ctx* ctx) {
 }
 
 int launches_per_step(const pbf_ctx* ctx) {
-  // kernels only (the bin-count memset is not one): ext/predict/hash + 3 scan
-  // + scatter + cell sort + reorder + fill + 2K solve + (K==0: velocity)
+  // kernels only (the memsets are not): ext/predict/hash + 3 scan + scatter
+  // + cell sort + reorder + fill + 3K solve (density/lambda, lambda fix-up,
+  // delta-p) + (K==0: velocity)
   // + 2 if gamma + 4 (visc, vort, apply, visc)
   const int K = ctx->params.solve_steps;
-  return 1 + 3 + 1 + 1 + 1 + 1 + 2 * K + (K == 0 ? 1 : 0) + (ctx->params.gamma != 0.0f ? 2 : 0) + 4;
+  return 1 + 3 + 1 + 1 + 1 + 1 + 3 * K + (K == 0 ? 1 : 0) + (ctx->params.gamma != 0.0f ? 2 : 0) + 4;
 }
 
 }  // namespace
@@ -1153,6 +1194,7 @@ int pbf_create(const pbf_params* p, size_t capacity, pbf_ctx** out) {
       (rc = dalloc(ctx, &ctx->cell_count, (size_t)ctx->nbins)) ||
       (rc = dalloc(ctx, &ctx->cell_start, (size_t)ctx->nbins + 1)) ||
       (rc = dalloc(ctx, &ctx->scan_part, (size_t)ctx->nscan_parts)) || (rc = dalloc(ctx, &ctx->err, 1)) ||
+      (rc = dalloc(ctx, &ctx->nudge, 1)) ||
       (rc = dalloc(ctx, &ctx->pairs, C)) || (rc = dalloc(ctx, &ctx->nbr, C * cap)) ||
       (rc = dalloc(ctx, &ctx->cnt, C)) || (rc = dalloc(ctx, &ctx->stage, 6 * C)) ||
       (rc = dalloc(ctx, &ctx->stage_i, C * cap + C)) || (rc = dalloc(ctx, &ctx->acc, 8)) ||
@@ -1362,8 +1404,9 @@ int pbf_find_neighbors(pbf_ctx* ctx, size_t bin_b, size_t bin_e, size_t fill_b, 
 int pbf_compute_densities(pbf_ctx* ctx, size_t b, size_t e) {
   STAGE_PROLOGUE(b, e);
   if (int rc = need_lists(ctx)) return rc;
-  if (X) k_density<true><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH);
-  else k_density<false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH);
+  if (X) k_density<true><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->pstS);
+  else k_density<false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->pstS);
+  CK(cudaMemcpyAsync(ctx->pstH, ctx->pstS, sizeof(float4) * ctx->n, cudaMemcpyDeviceToDevice, ctx->stream));
   return check_launch(ctx, "compute_densities");
 }
 
@@ -1601,3 +1644,4 @@ int pbf_launches_per_step(pbf_ctx* ctx, int64_t* out) {
 }
 
 }  // extern "C"
+
