@@ -226,6 +226,31 @@ int pbf_reset_timing(pbf_ctx* ctx);
 /* Number of kernel launches one pbf_step(ctx, 1) issues. */
 int pbf_launches_per_step(pbf_ctx* ctx, int64_t* out);
 
+/* ---- neighbor search that allocates nothing ----
+ * No counterpart in the reference.  For callers that may not allocate device
+ * memory: hosts that own every device allocation (their own pool or a fixed
+ * budget) and callers that cannot afford the device-wide synchronisation of
+ * cudaMalloc/cudaFree.  Builds the reference's neighbor lists (the same lists
+ * as pbf_find_neighbors + pbf_get_neighbors) for a caller-owned device point
+ * set, using only a file-scope device array of PBF_NOALLOC_SCRATCH_BYTES that
+ * every GPU loading the library holds until the process exits.
+ *   d_x    device, n x 3 floats (AoS), the positions to bin
+ *   d_nbr  device, n x neighbor_cap int32: reference indices, -1 past the count
+ *   d_cnt  device, n int32 counts
+ *   stream a cudaStream_t (NULL: the legacy default stream); the work is
+ *          enqueued there and the call returns without synchronising.
+ * Limits: n <= PBF_NOALLOC_MAX_PARTICLES and a grid of at most
+ * PBF_NOALLOC_MAX_BINS bins; larger inputs return PBF_ERR_CAPACITY with the
+ * message in pbf_last_error(NULL).  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress); make that first call before
+ * any stream capture.  Every call reuses the same array: calls that overlap
+ * on the GPU (other streams, other host threads) race — serialise them. */
+#define PBF_NOALLOC_MAX_PARTICLES 65536
+#define PBF_NOALLOC_MAX_BINS 262144
+#define PBF_NOALLOC_SCRATCH_BYTES 4719616
+int pbf_find_neighbors_noalloc(const pbf_params* p, const float* d_x, size_t n, int32_t* d_nbr,
+                               int32_t* d_cnt, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

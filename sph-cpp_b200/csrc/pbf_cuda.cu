@@ -30,6 +30,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1645,3 +1646,163 @@ int pbf_launches_per_step(pbf_ctx* ctx, int64_t* out) {
 
 }  // extern "C"
 
+// ============================================================================
+// Neighbor search that allocates nothing
+// ============================================================================
+// For callers that may not allocate device memory themselves: hosts that own
+// every device allocation through their own pool or a fixed budget, and
+// callers that cannot afford the device-wide synchronisation cudaMalloc and
+// cudaFree imply.  All working memory lives in the file-scope array below
+// (PBF_NOALLOC_SCRATCH_BYTES, held on every GPU that loads the library until
+// the process exits); the caller passes only its inputs and outputs.
+namespace {
+
+constexpr size_t kAlign = 256;
+constexpr size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
+constexpr size_t kNaN = PBF_NOALLOC_MAX_PARTICLES;
+constexpr size_t kNaB = PBF_NOALLOC_MAX_BINS;
+constexpr size_t kNaParts = (kNaB + 1 + kScanTile - 1) / kScanTile;
+// layout of the scratch array (byte offsets)
+constexpr size_t kOffCount = 0;
+constexpr size_t kOffStart = align_up(kOffCount + 4 * kNaB);
+constexpr size_t kOffParts = align_up(kOffStart + 4 * (kNaB + 1));
+constexpr size_t kOffKey = align_up(kOffParts + 4 * kNaParts);
+constexpr size_t kOffRank = align_up(kOffKey + 4 * kNaN);
+constexpr size_t kOffIdent = align_up(kOffRank + 4 * kNaN);
+constexpr size_t kOffPairs = align_up(kOffIdent + 4 * kNaN);
+constexpr size_t kOffSortedX = align_up(kOffPairs + 8 * kNaN);
+constexpr size_t kOffSortedId = align_up(kOffSortedX + 16 * kNaN);
+constexpr size_t kOffErr = align_up(kOffSortedId + 4 * kNaN);
+constexpr size_t kNoallocBytes = align_up(kOffErr + 4);
+static_assert(kNoallocBytes == PBF_NOALLOC_SCRATCH_BYTES, "PBF_NOALLOC_SCRATCH_BYTES in pbf.h is stale");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
+
+// Device address of g_noalloc_scratch per device, looked up once per device
+// (host code must not use the symbol itself as an address).
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[128] = {nullptr};
+
+// calculate_bins over caller AoS positions (neighbors.h:120-125) + histogram.
+__global__ void k_noalloc_hash(Dev P, int n, const float* __restrict__ x, uint32_t* key, uint32_t* rank,
+                               uint32_t* ident, uint32_t* cell_count, uint32_t* err) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n) return;
+  uint32_t k;
+  if (!pbf::bin_of(P, x[3 * (size_t)a], x[3 * (size_t)a + 1], x[3 * (size_t)a + 2], k))
+    atomicOr(err, PBF_FLAG_KEY_RANGE);
+  key[a] = k;
+  ident[a] = (uint32_t)a;
+  rank[a] = atomicAdd(&cell_count[k], 1u);
+}
+
+__global__ void k_noalloc_gather(int n, const unsigned long long* __restrict__ pairs, const float* __restrict__ x,
+                                 float4* sorted_x, uint32_t* sorted_id) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  const unsigned long long pr = pairs[b];
+  const size_t a = (size_t)(pr & 0xffffffffull);
+  sorted_x[b] = make_float4(x[3 * a], x[3 * a + 1], x[3 * a + 2], 0.0f);
+  sorted_id[b] = (uint32_t)(pr >> 32);
+}
+
+// Variant of k_fill that writes the lists straight into the caller's output
+// in reference index space: out[id][k], -1 past the count.
+__global__ void __launch_bounds__(kBlock) k_noalloc_fill(Dev P, int n, const float4* __restrict__ pst,
+                                                         const uint32_t* __restrict__ sorted_id,
+                                                         const uint32_t* __restrict__ cell_start, int32_t* out,
+                                                         int32_t* out_cnt, uint32_t* err) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  const float4 xp = pst[b];
+  const int cap = P.cap;
+  int32_t* row = out + (size_t)sorted_id[b] * cap;
+  int count = 0;
+  for (int i = -1; i < 2 && count < cap; i++) {
+    const float cx = pbf::xadd(xp.x, pbf::xmul((float)i, P.s));
+    for (int j = -1; j < 2 && count < cap; j++) {
+      const float cy = pbf::xadd(xp.y, pbf::xmul((float)j, P.s));
+      for (int k = -1; k < 2 && count < cap; k++) {
+        const float cz = pbf::xadd(xp.z, pbf::xmul((float)k, P.s));
+        uint32_t nb;
+        if (!pbf::bin_of(P, cx, cy, cz, nb)) {
+          atomicOr(err, PBF_FLAG_KEY_RANGE);
+          continue;
+        }
+        const uint32_t q0 = cell_start[nb], q1 = cell_start[nb + 1];
+        for (uint32_t q = q0; q < q1; ++q) {
+          if (q == (uint32_t)b) continue;
+          const float4 xq = pst[q];
+          const float d2 = pbf::mag2<true>(pbf::xsub(xp.x, xq.x), pbf::xsub(xp.y, xq.y), pbf::xsub(xp.z, xq.z));
+          if (d2 < P.s2) {
+            row[count] = (int32_t)sorted_id[q];
+            if (++count >= cap) break;
+          }
+        }
+      }
+    }
+  }
+  for (int k = count; k < cap; ++k) row[k] = -1;
+  out_cnt[sorted_id[b]] = count;
+}
+
+}  // namespace
+
+extern "C" int pbf_find_neighbors_noalloc(const pbf_params* p, const float* d_x, size_t n, int32_t* d_nbr,
+                                          int32_t* d_cnt, void* stream_handle) {
+  if (!p || (n && (!d_x || !d_nbr || !d_cnt))) return fail(nullptr, PBF_ERR_ARG, "null argument");
+  if (n > PBF_NOALLOC_MAX_PARTICLES)
+    return fail(nullptr, PBF_ERR_CAPACITY, "pbf_find_neighbors_noalloc: %zu particles exceed the maximum of %d",
+                n, PBF_NOALLOC_MAX_PARTICLES);
+  Dev d;
+  int64_t dims[3];
+  if (int rc = make_dev(nullptr, *p, d, dims)) return rc;
+  if (d.nbins > PBF_NOALLOC_MAX_BINS)
+    return fail(nullptr, PBF_ERR_CAPACITY, "pbf_find_neighbors_noalloc: grid of %d bins exceeds the maximum of %d",
+                d.nbins, PBF_NOALLOC_MAX_BINS);
+  if (n == 0) return PBF_OK;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= 128)
+    return fail(nullptr, PBF_ERR_CUDA, "cudaGetDevice failed: %s", cudaGetErrorString(e));
+  unsigned char* base;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+      void* ptr = nullptr;
+      e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+      if (e != cudaSuccess || !ptr)
+        return fail(nullptr, PBF_ERR_CUDA, "cudaGetSymbolAddress(scratch) failed: %s", cudaGetErrorString(e));
+      g_noalloc_addr[dev] = ptr;
+    }
+    base = static_cast<unsigned char*>(g_noalloc_addr[dev]);
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream_handle);
+  auto* cell_count = reinterpret_cast<uint32_t*>(base + kOffCount);
+  auto* cell_start = reinterpret_cast<uint32_t*>(base + kOffStart);
+  auto* parts = reinterpret_cast<uint32_t*>(base + kOffParts);
+  auto* key = reinterpret_cast<uint32_t*>(base + kOffKey);
+  auto* rank = reinterpret_cast<uint32_t*>(base + kOffRank);
+  auto* ident = reinterpret_cast<uint32_t*>(base + kOffIdent);
+  auto* pairs = reinterpret_cast<unsigned long long*>(base + kOffPairs);
+  auto* sorted_x = reinterpret_cast<float4*>(base + kOffSortedX);
+  auto* sorted_id = reinterpret_cast<uint32_t*>(base + kOffSortedId);
+  auto* err = reinterpret_cast<uint32_t*>(base + kOffErr);
+  // The array keeps the previous call's contents: clear what must start at zero.
+  e = cudaMemsetAsync(cell_count, 0, 4 * (size_t)d.nbins, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, 4, s);
+  if (e != cudaSuccess) return fail(nullptr, PBF_ERR_CUDA, "cudaMemsetAsync failed: %s", cudaGetErrorString(e));
+  const int nn = (int)n, g = blocks_for(n);
+  const int nparts = (int)(((size_t)d.nbins + 1 + kScanTile - 1) / kScanTile);
+  k_noalloc_hash<<<g, kBlock, 0, s>>>(d, nn, d_x, key, rank, ident, cell_count, err);
+  k_scan_reduce<<<nparts, kScanThreads, 0, s>>>(cell_count, d.nbins, parts);
+  k_scan_partials<<<1, kScanThreads, 0, s>>>(parts, nparts);
+  k_scan_apply<<<nparts, kScanThreads, 0, s>>>(cell_count, d.nbins, parts, cell_start);
+  k_scatter<<<g, kBlock, 0, s>>>(nn, key, rank, cell_start, ident, pairs);
+  k_cell_sort<<<blocks_for(d.nbins), kBlock, 0, s>>>(d.nbins, cell_start, pairs);
+  k_noalloc_gather<<<g, kBlock, 0, s>>>(nn, pairs, d_x, sorted_x, sorted_id);
+  k_noalloc_fill<<<g, kBlock, 0, s>>>(d, nn, sorted_x, sorted_id, cell_start, d_nbr, d_cnt, err);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(nullptr, PBF_ERR_CUDA, "noalloc neighbor search launch: %s", cudaGetErrorString(e));
+  return PBF_OK;
+}

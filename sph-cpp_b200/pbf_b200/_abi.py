@@ -27,6 +27,9 @@ ARRAY_SCRATCH = 3
 ARRAY_DENSITIES = 4
 ARRAY_LAMBDAS = 5
 
+NOALLOC_MAX_PARTICLES = 65536
+NOALLOC_MAX_BINS = 262144
+
 F3 = C.c_float * 3
 
 
@@ -141,6 +144,7 @@ SIGNATURES = {
     "pbf_kernel_times": (_i, [_vp, _i, _P(C.c_char_p), _P(C.c_int64), _P(C.c_double), _P(C.c_int)]),
     "pbf_reset_timing": (_i, [_vp]),
     "pbf_launches_per_step": (_i, [_vp, _P(C.c_int64)]),
+    "pbf_find_neighbors_noalloc": (_i, [_P(PbfParams), _vp, _sz, _vp, _vp, _vp]),
 }
 
 _lib = None
