@@ -37,8 +37,10 @@
 #include "../../include/pbf.h"
 #include "pbf_internal.h"
 #include "pbf_kernels.cuh"
+#include "pbf_fast.cuh"
 
 using pbf::Dev;
+using pbf::Fast;
 
 namespace {
 
@@ -255,6 +257,8 @@ __global__ void k_scatter(int n, const uint32_t* __restrict__ key, const uint32_
   pairs[slot] = ((unsigned long long)orig[a] << 32) | (unsigned long long)a;
 }
 
+// Per-bin insertion sort of the scattered pairs into ascending reference
+// index (the no-allocation neighbor search uses this form).
 __global__ void k_cell_sort(int nbins, const uint32_t* __restrict__ cell_start, unsigned long long* pairs) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nbins) return;
@@ -269,6 +273,22 @@ __global__ void k_cell_sort(int nbins, const uint32_t* __restrict__ cell_start, 
     }
     pairs[j] = v;
   }
+}
+
+// Stable order inside every bin: the scatter above placed a bin's pairs in
+// atomic (arbitrary) order; each pair's final position is the bin start plus
+// the number of the bin's pairs with a smaller reference index (pairs are
+// unique, so this is a permutation of the bin's slots).
+__global__ void k_rank_in_bin(int n, const unsigned long long* __restrict__ pairs, const uint32_t* __restrict__ key,
+                              const uint32_t* __restrict__ cell_start, unsigned long long* sorted) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const unsigned long long pr = pairs[j];
+  const uint32_t c = key[(uint32_t)(pr & 0xffffffffull)];
+  const uint32_t b0 = cell_start[c], b1 = cell_start[c + 1];
+  uint32_t rank = 0;
+  for (uint32_t i = b0; i < b1; ++i) rank += pairs[i] < pr;
+  sorted[b0 + rank] = pr;
 }
 
 // Gather the state into sorted order.  full = also lambda and scratch (the
@@ -294,42 +314,75 @@ __global__ void k_reorder(int n, const unsigned long long* __restrict__ pairs, c
   }
 }
 
-// fill_neighbors (neighbors.h:197-230) over slots in sorted order: 27 bins in
-// the reference's order (x offset outer, z inner, float re-hash of
+// fill_neighbors (neighbors.h:197-230) over slots in sorted order: the 27
+// bins in the reference's order (x offset outer, z inner, float re-hash of
 // coord + i*s), candidates of a bin in ascending reference index, strict
-// d^2 < s^2, self skipped, first `cap` kept.
-__global__ void __launch_bounds__(kBlock) k_fill(Dev P, int n, size_t stride, const float4* __restrict__ pst,
-                                                 const uint32_t* __restrict__ cell_start, int32_t* nbr,
-                                                 int32_t* cnt, uint32_t* err) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+// d^2 < s^2, self skipped, the first `cap` kept.  Lists are row-major
+// ([slot][cap]): each thread fills its own contiguous run.  A neighbour bin whose every point is provably
+// farther than s from the particle is skipped: the per-axis distance from the
+// particle to the bin's face, less a margin of many ulps of the coordinate
+// (P.skip_eps), squared and summed, exceeds s^2.  Only bins equal to the
+// integer offset of the particle's own bin are skipped, so the reference's
+// float re-hash still decides which bins are visited.
+constexpr int kFillBlock = 128;
+
+__global__ void __launch_bounds__(kFillBlock) k_fill2(Dev P, int n, size_t stride, const float4* __restrict__ pst,
+                                                      const uint32_t* __restrict__ cell_start, int32_t* nbr,
+                                                      int32_t* cnt, uint32_t* err) {
+  const int b = blockIdx.x * kFillBlock + threadIdx.x;
   if (b >= n) return;
   const float4 xp = pst[b];
-  int count = 0;
   const int cap = P.cap;
-  for (int i = -1; i < 2 && count < cap; i++) {
-    const float cx = pbf::xadd(xp.x, pbf::xmul((float)i, P.s));
-    for (int j = -1; j < 2 && count < cap; j++) {
-      const float cy = pbf::xadd(xp.y, pbf::xmul((float)j, P.s));
-      for (int k = -1; k < 2 && count < cap; k++) {
-        const float cz = pbf::xadd(xp.z, pbf::xmul((float)k, P.s));
-        uint32_t nb;
-        if (!pbf::bin_of(P, cx, cy, cz, nb)) {
+  const float s = P.s;
+  int32_t* row = nbr + (size_t)b * stride;
+  // calculate_neighbor_indices (neighbors.h:172-185): the bin of coord + i*s
+  // per axis for i = -1, 0, 1, in the reference's float operations.  The 27
+  // bins combine these per-axis values, so 9 float hashes cover all of them.
+  int bx[3], by[3], bz[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const float o = pbf::xmul((float)(i - 1), s);
+    bx[i] = pbf::dev_axis_bin(pbf::xadd(xp.x, o), s);
+    by[i] = pbf::dev_axis_bin(pbf::xadd(xp.y, o), s);
+    bz[i] = pbf::dev_axis_bin(pbf::xadd(xp.z, o), s);
+  }
+  // Per-axis distance from the particle to its own bin's faces, less the margin.
+  const float lo[3] = {fmaxf(xp.x - ((float)bx[1] * s - s) - P.skip_eps, 0.f),
+                       fmaxf(xp.y - ((float)by[1] * s - s) - P.skip_eps, 0.f),
+                       fmaxf(xp.z - ((float)bz[1] * s - s) - P.skip_eps, 0.f)};
+  const float hi[3] = {fmaxf(((float)(bx[1] + 1) * s - s) - xp.x - P.skip_eps, 0.f),
+                       fmaxf(((float)(by[1] + 1) * s - s) - xp.y - P.skip_eps, 0.f),
+                       fmaxf(((float)(bz[1] + 1) * s - s) - xp.z - P.skip_eps, 0.f)};
+  const bool finite = isfinite(xp.x) && isfinite(xp.y) && isfinite(xp.z);
+  int count = 0;
+
+  for (int i = 0; i < 3; i++) {
+    const float ex = i == 0 ? lo[0] : (i == 2 ? hi[0] : 0.f);
+    for (int j = 0; j < 3; j++) {
+      const float ey = j == 0 ? lo[1] : (j == 2 ? hi[1] : 0.f);
+      for (int k = 0; k < 3; k++) {
+        const float ez = k == 0 ? lo[2] : (k == 2 ? hi[2] : 0.f);
+        const int cx = bx[i], cy = by[j], cz = bz[k];
+        if (!finite || cx < 0 || cy < 0 || cz < 0 || cx >= P.dimx || cy >= P.dimy || cz >= P.dimz) {
           atomicOr(err, PBF_FLAG_KEY_RANGE);
           continue;
         }
-        const uint32_t q0 = cell_start[nb], q1 = cell_start[nb + 1];
-        for (uint32_t q = q0; q < q1; ++q) {
-          if (q == (uint32_t)b) continue;
+        // a bin at the integer offset whose every point is farther than s: skip
+        if (cx == bx[1] + i - 1 && cy == by[1] + j - 1 && cz == bz[1] + k - 1 &&
+            ex * ex + ey * ey + ez * ez > P.s2)
+          continue;
+        const uint32_t nb = (uint32_t)(P.dimx * P.dimy) * (uint32_t)cz + ((uint32_t)cy * (uint32_t)P.dimx + (uint32_t)cx);
+        const uint32_t q1 = cell_start[nb + 1];
+        for (uint32_t q = cell_start[nb]; q < q1; ++q) {
           const float4 xq = pst[q];
           const float d2 = pbf::mag2<true>(pbf::xsub(xp.x, xq.x), pbf::xsub(xp.y, xq.y), pbf::xsub(xp.z, xq.z));
-          if (d2 < P.s2) {
-            nbr[(size_t)count * stride + b] = (int32_t)q;
-            if (++count >= cap) break;
-          }
+          if (d2 < P.s2 && q != (uint32_t)b && count < cap) row[count++] = (int32_t)q;
         }
+        if (count >= cap) goto done;
       }
     }
   }
+done:
   cnt[b] = count;
 }
 
@@ -350,7 +403,7 @@ __global__ void __launch_bounds__(kBlock) k_density(Dev P, int n, size_t stride,
   float rho = pbf::M<X>(P.m, P.W0);
   bool nudged = false;
   for (int k = 0; k < c; ++k) {
-    const int q = nbr[(size_t)k * stride + b];
+    const int q = nbr[(size_t)b * stride + k];
     const float4 xq = pst[q];
     float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
     float rm = pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz));
@@ -402,7 +455,7 @@ __global__ void __launch_bounds__(kBlock) k_lambda(Dev P, int n, size_t stride, 
   float3 sg = make_float3(0.f, 0.f, 0.f);
   float sumC = 0.0f;
   for (int k = 0; k < c; ++k) {
-    const float4 xq = pst[nbr[(size_t)k * stride + b]];
+    const float4 xq = pst[nbr[(size_t)b * stride + k]];
     const float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
     lambda_terms<X>(P, rx, ry, rz, pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz)), sg, sumC);
   }
@@ -417,13 +470,9 @@ __global__ void __launch_bounds__(kBlock) k_lambda(Dev P, int n, size_t stride, 
 // nudged positions, which is what a separate lambda stage after the density
 // stage sees.
 template <bool X>
-__global__ void __launch_bounds__(kBlock) k_density_lambda(Dev P, int n, size_t stride,
-                                                           const int32_t* __restrict__ nbr,
-                                                           const int32_t* __restrict__ cnt,
-                                                           const float4* __restrict__ pst, float4* xl,
-                                                           float4* vel, float* lam, uint32_t* nudge) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= n) return;
+__device__ __forceinline__ void density_lambda_one(const Dev& P, int b, size_t stride, const int32_t* __restrict__ nbr,
+                                                   const int32_t* __restrict__ cnt, const float4* __restrict__ pst,
+                                                   float4* xl, float4* vel, float* lam, uint32_t* nudge) {
   float4 xp = pst[b];
   const int c = cnt[b];
   float rho = pbf::M<X>(P.m, P.W0);
@@ -431,7 +480,7 @@ __global__ void __launch_bounds__(kBlock) k_density_lambda(Dev P, int n, size_t 
   float sumC = 0.0f;
   bool nudged = false;
   for (int k = 0; k < c; ++k) {
-    const float4 xq = pst[nbr[(size_t)k * stride + b]];
+    const float4 xq = pst[nbr[(size_t)b * stride + k]];
     float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
     float rm = pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz));
     if ((double)rm < 0.00000001) {
@@ -453,6 +502,64 @@ __global__ void __launch_bounds__(kBlock) k_density_lambda(Dev P, int n, size_t 
   lam[b] = l;
 }
 
+template <bool X>
+__global__ void __launch_bounds__(kBlock) k_density_lambda(Dev P, int n, size_t stride,
+                                                           const int32_t* __restrict__ nbr,
+                                                           const int32_t* __restrict__ cnt,
+                                                           const float4* __restrict__ pst, float4* xl,
+                                                           float4* vel, float* lam, uint32_t* nudge) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  density_lambda_one<X>(P, b, stride, nbr, cnt, pst, xl, vel, lam, nudge);
+}
+
+// Fast density + lambda (see pbf_fast.cuh), kGL lanes per particle.  A
+// particle nudged off a neighbour (particles.h:303-305) is seen at its nudged
+// position by the others from the delta-p pass on — the order in which the
+// reference's parallel builds see it when every neighbour reads before the
+// write; the exact path instead recomputes lambda (k_lambda_fixup).
+__global__ void __launch_bounds__(kBlock) kf_density_lambda(Dev P, Fast F, int n, size_t stride,
+                                                            const int32_t* __restrict__ nbr,
+                                                            const int32_t* __restrict__ cnt,
+                                                            const float4* __restrict__ pst, float4* xl, float4* vel,
+                                                            float* lam, uint32_t* nudge) {
+  const pbf::Group G = pbf::group_of(n);
+  const int b = G.b;
+  const float4 xp = pst[b];
+  const int c = G.live ? cnt[b] : 0;
+  float sw = 0.f, sgx = 0.f, sgy = 0.f, sgz = 0.f, sc = 0.f;
+  int close = 0;
+  pbf::gwalk1(nbr + (size_t)b * stride, c, G.lane, pst, [&](int, float4 xq) {
+    const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
+    const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+    close |= d2 < 4e-16f;
+    sw += pbf::poly_cube(F, d2);
+    const float t = F.lam_grad * pbf::spikey_over_r(F, d2);
+    sgx = fmaf(-t, dx, sgx);
+    sgy = fmaf(-t, dy, sgy);
+    sgz = fmaf(-t, dz, sgz);
+    sc = fmaf(t * t, d2, sc);
+  });
+  sw = pbf::gsum(sw);
+  sgx = pbf::gsum(sgx);
+  sgy = pbf::gsum(sgy);
+  sgz = pbf::gsum(sgz);
+  sc = pbf::gsum(sc);
+  close = pbf::gor(close);
+  if (!G.live || G.lane != 0) return;
+  if (close) {  // a neighbour (almost) on top: the reference-ordered path decides the nudge
+    density_lambda_one<false>(P, b, stride, nbr, cnt, pst, xl, vel, lam, nudge);
+    return;
+  }
+  const float rho = fmaf(F.m_poly, sw, F.m_w0);
+  const float C = fmaxf(fmaf(rho, F.inv_rho0, -1.0f), 0.0f);
+  sc = fmaf(sgz, sgz, fmaf(sgy, sgy, fmaf(sgx, sgx, sc)));
+  const float l = -C / (sc + F.lambda_eps);
+  xl[b] = make_float4(xp.x, xp.y, xp.z, l);
+  vel[b].w = rho;
+  lam[b] = l;
+}
+
 // Lambda recomputed from the (nudged) positions in xl, only when the
 // preceding density_lambda launch nudged a particle; otherwise every block
 // returns at once.
@@ -469,7 +576,7 @@ __global__ void __launch_bounds__(kBlock) k_lambda_fixup(Dev P, int n, size_t st
   float3 sg = make_float3(0.f, 0.f, 0.f);
   float sumC = 0.0f;
   for (int k = 0; k < c; ++k) {
-    const float4 xq = xl[nbr[(size_t)k * stride + b]];
+    const float4 xq = xl[nbr[(size_t)b * stride + k]];
     const float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
     lambda_terms<X>(P, rx, ry, rz, pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz)), sg, sumC);
   }
@@ -503,7 +610,7 @@ __global__ void __launch_bounds__(kBlock) k_dp(Dev P, int n, size_t stride, cons
   const int c = cnt[b];
   float3 dp = make_float3(0.f, 0.f, 0.f);
   for (int k = 0; k < c; ++k) {
-    const int q = nbr[(size_t)k * stride + b];
+    const int q = nbr[(size_t)b * stride + k];
     const float4 xq = pst[q];
     const float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
     dp_term<X, SCORR>(P, lp, lam[q], rx, ry, rz, pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz)), dp);
@@ -552,14 +659,14 @@ __global__ void __launch_bounds__(kBlock) k_dp_update(Dev P, int n, size_t strid
   float3 dp = make_float3(0.f, 0.f, 0.f);
   if (*nudge == 0u) {
     for (int k = 0; k < c; ++k) {
-      const float4 xq = xl[nbr[(size_t)k * stride + b]];
+      const float4 xq = xl[nbr[(size_t)b * stride + k]];
       const float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
       dp_term<X, SCORR>(P, xp.w, xq.w, rx, ry, rz, pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz)), dp);
     }
   } else {  // lambdas were recomputed by k_lambda_fixup
     const float lp = lam[b];
     for (int k = 0; k < c; ++k) {
-      const int q = nbr[(size_t)k * stride + b];
+      const int q = nbr[(size_t)b * stride + k];
       const float4 xq = xl[q];
       const float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
       dp_term<X, SCORR>(P, lp, lam[q], rx, ry, rz, pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz)), dp);
@@ -586,7 +693,7 @@ __global__ void __launch_bounds__(kBlock) k_color(Dev P, int n, size_t stride, c
   const int c = cnt[b];
   float3 col = make_float3(0.f, 0.f, 0.f);
   for (int k = 0; k < c; ++k) {
-    const int q = nbr[(size_t)k * stride + b];
+    const int q = nbr[(size_t)b * stride + k];
     const float4 xq = pst[q];
     const float rq = vel[q].w;
     const float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
@@ -610,7 +717,7 @@ __global__ void __launch_bounds__(kBlock) k_surface(Dev P, int n, size_t stride,
   const float ng = -P.gamma;
   float3 f = make_float3(0.f, 0.f, 0.f);
   for (int k = 0; k < c; ++k) {
-    const int q = nbr[(size_t)k * stride + b];
+    const int q = nbr[(size_t)b * stride + k];
     const float4 xq = pst[q], sq = scr[q];
     const float rq = vel[q].w;
     const float rx = pbf::xsub(xp.x, xq.x), ry = pbf::xsub(xp.y, xq.y), rz = pbf::xsub(xp.z, xq.z);
@@ -644,7 +751,7 @@ __global__ void __launch_bounds__(kBlock) k_viscosity(Dev P, int n, size_t strid
   const int c = cnt[b];
   float3 dv = make_float3(0.f, 0.f, 0.f);
   for (int k = 0; k < c; ++k) {
-    const int q = nbr[(size_t)k * stride + b];
+    const int q = nbr[(size_t)b * stride + k];
     const float4 xq = pst[q], vq = vin[q];
     const float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
     const float w = pbf::poly6<X>(P, pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz)));
@@ -680,7 +787,7 @@ __global__ void __launch_bounds__(kBlock) k_vorticity(Dev P, int n, size_t strid
   const int c = cnt[b];
   float3 w = make_float3(0.f, 0.f, 0.f);
   for (int k = 0; k < c; ++k) {
-    const int q = nbr[(size_t)k * stride + b];
+    const int q = nbr[(size_t)b * stride + k];
     const float4 xq = pst[q], vq = vel[q];
     const float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
     const float3 d = pbf::del_spikey<X>(P, rx, ry, rz, pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz)));
@@ -710,7 +817,7 @@ __global__ void __launch_bounds__(kBlock) k_apply_vorticity(Dev P, int n, size_t
   const int c = cnt[b];
   float3 eta = make_float3(0.f, 0.f, 0.f);
   for (int k = 0; k < c; ++k) {
-    const int q = nbr[(size_t)k * stride + b];
+    const int q = nbr[(size_t)b * stride + k];
     float4 xq;
     float vm;
     if (PACKED) {
@@ -740,6 +847,136 @@ __global__ void __launch_bounds__(kBlock) k_apply_vorticity(Dev P, int n, size_t
   vel[b] = v;
 }
 
+// ---- fast gathers (exact_math = 0), kGL lanes per particle, see pbf_fast.cuh ----
+template <bool SCORR, bool LAST>
+__global__ void __launch_bounds__(kBlock) kf_dp_update(Dev P, Fast F, int n, size_t stride,
+                                                       const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
+                                                       const float4* __restrict__ xl, float4* pst,
+                                                       const float4* __restrict__ pos, float4* vel,
+                                                       const float* __restrict__ lam,
+                                                       const uint32_t* __restrict__ nudge) {
+  const pbf::Group G = pbf::group_of(n);
+  const int b = G.b;
+  const float4 xp = xl[b];
+  const int c = G.live ? cnt[b] : 0;
+  float ax = 0.f, ay = 0.f, az = 0.f;
+  const float lp = xp.w;
+  pbf::gwalk1(nbr + (size_t)b * stride, c, G.lane, xl, [&](int, float4 xq) {
+    const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
+    const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+    float l = lp + xq.w;
+    if (SCORR) l -= P.scorr_k * __powf(F.visc_poly * pbf::poly_cube(F, d2) * P.inv_wdq, P.scorr_n);
+    const float t = l * pbf::spikey_over_r(F, d2);
+    ax = fmaf(t, dx, ax);
+    ay = fmaf(t, dy, ay);
+    az = fmaf(t, dz, az);
+  });
+  ax = pbf::gsum(ax);
+  ay = pbf::gsum(ay);
+  az = pbf::gsum(az);
+  if (!G.live || G.lane != 0) return;
+  const float3 s = pbf::boundary(P, make_float3(pbf::xadd(xp.x, F.dp_scale * ax), pbf::xadd(xp.y, F.dp_scale * ay),
+                                                pbf::xadd(xp.z, F.dp_scale * az)));
+  const float4 ns = make_float4(s.x, s.y, s.z, 0.0f);
+  pst[b] = ns;
+  if (LAST) {
+    const float3 v = velocity_of(P, ns, pos[b]);
+    vel[b] = make_float4(v.x, v.y, v.z, vel[b].w);
+  }
+}
+
+template <bool FINAL>
+__global__ void __launch_bounds__(kBlock) kf_viscosity(Dev P, Fast F, int n, size_t stride,
+                                                       const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
+                                                       const float4* __restrict__ pst, const float4* __restrict__ vin,
+                                                       float4* vout, float4* posH, float4* pstH,
+                                                       const uint32_t* __restrict__ origS, uint32_t* origH) {
+  const pbf::Group G = pbf::group_of(n);
+  const int b = G.b;
+  const float4 xp = pst[b], vp = vin[b];
+  const int c = G.live ? cnt[b] : 0;
+  float ax = 0.f, ay = 0.f, az = 0.f;
+  pbf::gwalk2(nbr + (size_t)b * stride, c, G.lane, pst, vin, [&](int, float4 xq, float4 vq) {
+    const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
+    const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+    const float wr = __fdividef(pbf::poly_cube(F, d2), vq.w);
+    ax = fmaf(vq.x - vp.x, wr, ax);
+    ay = fmaf(vq.y - vp.y, wr, ay);
+    az = fmaf(vq.z - vp.z, wr, az);
+  });
+  ax = pbf::gsum(ax);
+  ay = pbf::gsum(ay);
+  az = pbf::gsum(az);
+  if (!G.live || G.lane != 0) return;
+  const float k = F.visc_c * F.visc_poly;
+  vout[b] = make_float4(fmaf(k, ax, vp.x), fmaf(k, ay, vp.y), fmaf(k, az, vp.z), vp.w);
+  if (FINAL) {
+    posH[b] = xp;
+    pstH[b] = xp;
+    origH[b] = origS[b];
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) kf_vorticity(Dev P, Fast F, int n, size_t stride,
+                                                       const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
+                                                       const float4* __restrict__ pst, const float4* __restrict__ vel,
+                                                       float4* scr, float4* xl) {
+  const pbf::Group G = pbf::group_of(n);
+  const int b = G.b;
+  const float4 xp = pst[b], vp = vel[b];
+  const int c = G.live ? cnt[b] : 0;
+  float wx = 0.f, wy = 0.f, wz = 0.f;
+  pbf::gwalk2(nbr + (size_t)b * stride, c, G.lane, pst, vel, [&](int, float4 xq, float4 vq) {
+    const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
+    const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+    const float t = pbf::spikey_over_r(F, d2);
+    const float ux = vq.x - vp.x, uy = vq.y - vp.y, uz = vq.z - vp.z;
+    // cross(v_q - v_p, del W), del W = spikey * t * r
+    wx = fmaf(t, fmaf(uy, dz, -uz * dy), wx);
+    wy = fmaf(t, fmaf(uz, dx, -ux * dz), wy);
+    wz = fmaf(t, fmaf(ux, dy, -uy * dx), wz);
+  });
+  wx = pbf::gsum(wx) * F.spikey;
+  wy = pbf::gsum(wy) * F.spikey;
+  wz = pbf::gsum(wz) * F.spikey;
+  if (!G.live || G.lane != 0) return;
+  const float wm = sqrtf(fmaf(wz, wz, fmaf(wy, wy, wx * wx)));
+  scr[b] = make_float4(wx, wy, wz, wm);
+  xl[b] = make_float4(xp.x, xp.y, xp.z, wm);
+}
+
+__global__ void __launch_bounds__(kBlock) kf_apply_vorticity(Dev P, Fast F, int n, size_t stride,
+                                                             const int32_t* __restrict__ nbr,
+                                                             const int32_t* __restrict__ cnt,
+                                                             const float4* __restrict__ xl,
+                                                             const float4* __restrict__ scr, float4* vel) {
+  const pbf::Group G = pbf::group_of(n);
+  const int b = G.b;
+  const float4 xp = xl[b];
+  const int c = G.live ? cnt[b] : 0;
+  float ex = 0.f, ey = 0.f, ez = 0.f;
+  pbf::gwalk1(nbr + (size_t)b * stride, c, G.lane, xl, [&](int, float4 xq) {
+    const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
+    const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+    const float t = xq.w * pbf::spikey_over_r(F, d2);
+    ex = fmaf(t, dx, ex);
+    ey = fmaf(t, dy, ey);
+    ez = fmaf(t, dz, ez);
+  });
+  ex = pbf::gsum(ex) * F.spikey;
+  ey = pbf::gsum(ey) * F.spikey;
+  ez = pbf::gsum(ez) * F.spikey;
+  if (!G.live || G.lane != 0) return;
+  const float inv = __fdividef(1.0f, sqrtf(fmaf(ez, ez, fmaf(ey, ey, ex * ex))) + FLT_EPSILON);
+  const float Nx = ex * inv, Ny = ey * inv, Nz = ez * inv;
+  const float4 wp = scr[b];
+  float4 v = vel[b];
+  v.x = fmaf(fmaf(Ny, wp.z, -Nz * wp.y), F.vort_dt, v.x);
+  v.y = fmaf(fmaf(Nz, wp.x, -Nx * wp.z), F.vort_dt, v.y);
+  v.z = fmaf(fmaf(Nx, wp.y, -Ny * wp.x), F.vort_dt, v.z);
+  vel[b] = v;
+}
+
 // Residual statistics (no state change): density over the current lists,
 // clamped error, kinetic energy, centre of mass, list lengths.
 __device__ __forceinline__ double warp_sum(double v) {
@@ -760,7 +997,7 @@ __global__ void __launch_bounds__(kBlock) k_stats(Dev P, int n, size_t stride, c
     const int c = cnt[b];
     float d = pbf::xmul(P.m, P.W0);
     for (int k = 0; k < c; ++k) {
-      const float4 xq = pst[nbr[(size_t)k * stride + b]];
+      const float4 xq = pst[nbr[(size_t)b * stride + k]];
       const float rx = pbf::xsub(xp.x, xq.x), ry = pbf::xsub(xp.y, xq.y), rz = pbf::xsub(xp.z, xq.z);
       d = pbf::xadd(d, pbf::xmul(P.m, pbf::poly6<true>(P, __fsqrt_rn(pbf::mag2<true>(rx, ry, rz)))));
     }
@@ -792,7 +1029,7 @@ __global__ void k_export_neighbors(int n, size_t stride, int cap, const int32_t*
   if (cnt_out) cnt_out[o] = c;
   if (idx_out)
     for (int k = 0; k < cap; ++k)
-      idx_out[o * cap + k] = k < c ? (int32_t)orig[nbr[(size_t)k * stride + b]] : -1;
+      idx_out[o * cap + k] = k < c ? (int32_t)orig[nbr[(size_t)b * stride + k]] : -1;
 }
 
 }  // namespace
@@ -803,9 +1040,11 @@ __global__ void k_export_neighbors(int n, size_t stride, int cap, const int32_t*
 struct pbf_ctx {
   pbf_params params{};
   Dev dev{};
+  Fast fast{};
   size_t capacity = 0, n = 0;
   int64_t dims[3] = {0, 0, 0};
   int nbins = 0, nscan_parts = 0;
+  size_t lstride = 0;  // list row stride: neighbor_cap rounded up to 8 (whole 32-byte sectors)
   int device = 0;
   cudaStream_t stream = nullptr;
   bool lists_valid = false;
@@ -815,7 +1054,7 @@ struct pbf_ctx {
   float *lamH = nullptr, *lamS = nullptr;
   uint32_t *origH = nullptr, *origS = nullptr, *key = nullptr, *rank = nullptr, *keyH = nullptr;
   uint32_t *cell_count = nullptr, *cell_start = nullptr, *scan_part = nullptr, *err = nullptr, *nudge = nullptr;
-  unsigned long long* pairs = nullptr;
+  unsigned long long *pairs = nullptr, *pairs_sorted = nullptr;
   int32_t *nbr = nullptr, *cnt = nullptr;
   float* stage = nullptr;  // 6*C floats: two AoS float3 staging areas
   int32_t* stage_i = nullptr;  // neighbor export staging (C*cap + C)
@@ -938,6 +1177,12 @@ int make_dev(pbf_ctx* ctx, const pbf_params& p, Dev& d, int64_t dims[3]) {
   }
   d.vthr = 0.000001 * (double)p.max_speed;
   d.h_eps = (double)h * 0.000001;
+  {
+    // margin of the bin-skip test in k_fill2: 64 ulps of the largest hashed coordinate
+    float mx = 0.0f;
+    for (int a = 0; a < 3; ++a) mx = std::fmax(mx, std::fabs(p.boundary_max[a]) + 2.0f * s);
+    d.skip_eps = 64.0f * std::ldexp(1.0f, std::ilogb(mx) - 23);
+  }
   d.dimx = (int)dims[0];
   d.dimy = (int)dims[1];
   d.dimz = (int)dims[2];
@@ -1039,22 +1284,23 @@ void launch_sort_to_pairs(pbf_ctx* ctx) {
                                                          ctx->pairs);
   }
   {
-    Launch L(ctx, "cell_sort");
-    k_cell_sort<<<blocks_for(ctx->nbins), kBlock, 0, ctx->stream>>>(ctx->nbins, ctx->cell_start, ctx->pairs);
+    Launch L(ctx, "rank_in_bin");
+    k_rank_in_bin<<<blocks_for(n), kBlock, 0, ctx->stream>>>(n, ctx->pairs, ctx->key, ctx->cell_start,
+                                                             ctx->pairs_sorted);
   }
 }
 
 void launch_fill(pbf_ctx* ctx, const float4* pst) {
   Launch L(ctx, "fill_neighbors");
-  k_fill<<<blocks_for(ctx->n), kBlock, 0, ctx->stream>>>(ctx->dev, (int)ctx->n, ctx->capacity, pst,
-                                                         ctx->cell_start, ctx->nbr, ctx->cnt, ctx->err);
+  k_fill2<<<blocks_for(ctx->n, kFillBlock), kFillBlock, 0, ctx->stream>>>(ctx->dev, (int)ctx->n, ctx->lstride, pst,
+                                                                         ctx->cell_start, ctx->nbr, ctx->cnt, ctx->err);
 }
 
 // ---- the fused step (graph-capturable: fixed pointers, no host sync) ----
 template <bool X, bool SCORR>
 void launch_step_t(pbf_ctx* ctx) {
   const int n = (int)ctx->n;
-  const size_t st = ctx->capacity;
+  const size_t st = ctx->lstride;
   const Dev& P = ctx->dev;
   cudaStream_t s = ctx->stream;
   const int g = blocks_for(n);
@@ -1067,31 +1313,47 @@ void launch_step_t(pbf_ctx* ctx) {
   launch_sort_to_pairs(ctx);
   {
     Launch L(ctx, "reorder");
-    k_reorder<false><<<g, kBlock, 0, s>>>(n, ctx->pairs, ctx->key, ctx->posH, ctx->pstH, ctx->velH, nullptr,
+    k_reorder<false><<<g, kBlock, 0, s>>>(n, ctx->pairs_sorted, ctx->key, ctx->posH, ctx->pstH, ctx->velH, nullptr,
                                           nullptr, ctx->posS, ctx->pstS, ctx->velS, nullptr, nullptr, ctx->origS,
                                           ctx->keyH);
   }
   launch_fill(ctx, ctx->pstS);
   const int K = ctx->params.solve_steps;
+  const Fast& F = ctx->fast;
+  const int gg = blocks_for((size_t)n * pbf::kGL);  // kGL lanes per particle
   for (int it = 0; it < K; ++it) {
-    cudaMemsetAsync(ctx->nudge, 0, sizeof(uint32_t), s);
+    if (X) cudaMemsetAsync(ctx->nudge, 0, sizeof(uint32_t), s);
     {
       Launch L(ctx, "density_lambda");
-      k_density_lambda<X><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl, ctx->velS,
+      if (X)
+        k_density_lambda<X><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl, ctx->velS,
+                                                 ctx->lamH, ctx->nudge);
+      else
+        kf_density_lambda<<<gg, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl, ctx->velS,
                                                ctx->lamH, ctx->nudge);
     }
-    {
+    if (X) {
       Launch L(ctx, "lambda_fixup");
       k_lambda_fixup<X><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->velS, ctx->lamH,
                                              ctx->nudge);
     }
     Launch L(ctx, "dp_update");
-    if (it == K - 1)
-      k_dp_update<X, SCORR, true><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS,
+    const bool last = it == K - 1;
+    if (X) {
+      if (last)
+        k_dp_update<X, SCORR, true><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS,
+                                                         ctx->posS, ctx->velS, ctx->lamH, ctx->nudge);
+      else
+        k_dp_update<X, SCORR, false><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS,
+                                                          ctx->posS, ctx->velS, ctx->lamH, ctx->nudge);
+    } else {
+      if (last)
+        kf_dp_update<SCORR, true><<<gg, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS,
                                                        ctx->posS, ctx->velS, ctx->lamH, ctx->nudge);
-    else
-      k_dp_update<X, SCORR, false><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS,
+      else
+        kf_dp_update<SCORR, false><<<gg, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS,
                                                         ctx->posS, ctx->velS, ctx->lamH, ctx->nudge);
+    }
   }
   if (K == 0) {
     Launch L(ctx, "update_velocities");
@@ -1105,24 +1367,41 @@ void launch_step_t(pbf_ctx* ctx) {
     Launch L(ctx, "surface_tension");
     k_surface<<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->scrH, ctx->velS);
   }
-  {
-    Launch L(ctx, "viscosity");
-    k_viscosity<X, false><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->velS, ctx->velT,
-                                               nullptr, nullptr, nullptr, nullptr);
-  }
-  {
-    Launch L(ctx, "vorticity");
-    k_vorticity<X><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->velT, ctx->scrH, ctx->xl);
-  }
-  {
-    Launch L(ctx, "apply_vorticity");
-    k_apply_vorticity<X, true><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->xl, nullptr, ctx->scrH,
-                                                    ctx->velT);
-  }
-  {
+  if (X) {
+    {
+      Launch L(ctx, "viscosity");
+      k_viscosity<X, false><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->velS, ctx->velT,
+                                                 nullptr, nullptr, nullptr, nullptr);
+    }
+    {
+      Launch L(ctx, "vorticity");
+      k_vorticity<X><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->velT, ctx->scrH, ctx->xl);
+    }
+    {
+      Launch L(ctx, "apply_vorticity");
+      k_apply_vorticity<X, true><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->xl, nullptr, ctx->scrH,
+                                                      ctx->velT);
+    }
     Launch L(ctx, "viscosity_final");
     k_viscosity<X, true><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->velT, ctx->velH,
                                               ctx->posH, ctx->pstH, ctx->origS, ctx->origH);
+  } else {
+    {
+      Launch L(ctx, "viscosity");
+      kf_viscosity<false><<<gg, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->velS, ctx->velT,
+                                               nullptr, nullptr, nullptr, nullptr);
+    }
+    {
+      Launch L(ctx, "vorticity");
+      kf_vorticity<<<gg, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->velT, ctx->scrH, ctx->xl);
+    }
+    {
+      Launch L(ctx, "apply_vorticity");
+      kf_apply_vorticity<<<gg, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->scrH, ctx->velT);
+    }
+    Launch L(ctx, "viscosity_final");
+    kf_viscosity<true><<<gg, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->velT, ctx->velH,
+                                            ctx->posH, ctx->pstH, ctx->origS, ctx->origH);
   }
 }
 
@@ -1137,11 +1416,12 @@ void launch_step(pbf_ctx* ctx) {
 
 int launches_per_step(const pbf_ctx* ctx) {
   // kernels only (the memsets are not): ext/predict/hash + 3 scan + scatter
-  // + cell sort + reorder + fill + 3K solve (density/lambda, lambda fix-up,
-  // delta-p) + (K==0: velocity)
+  // + rank in bin + reorder + fill + K x (density/lambda, [exact: lambda
+  // fix-up], delta-p) + (K==0: velocity)
   // + 2 if gamma + 4 (visc, vort, apply, visc)
   const int K = ctx->params.solve_steps;
-  return 1 + 3 + 1 + 1 + 1 + 1 + 3 * K + (K == 0 ? 1 : 0) + (ctx->params.gamma != 0.0f ? 2 : 0) + 4;
+  const int per_iter = ctx->params.exact_math ? 3 : 2;
+  return 1 + 3 + 1 + 1 + 1 + 1 + per_iter * K + (K == 0 ? 1 : 0) + (ctx->params.gamma != 0.0f ? 2 : 0) + 4;
 }
 
 }  // namespace
@@ -1168,6 +1448,7 @@ int pbf_create(const pbf_params* p, size_t capacity, pbf_ctx** out) {
     delete ctx;
     return rc;
   }
+  ctx->fast = pbf::make_fast(ctx->dev);
   ctx->capacity = capacity;
   ctx->nbins = ctx->dev.nbins;
   ctx->nscan_parts = (int)(((size_t)ctx->nbins + 1 + kScanTile - 1) / kScanTile);
@@ -1185,7 +1466,8 @@ int pbf_create(const pbf_params* p, size_t capacity, pbf_ctx** out) {
     return bail(PBF_ERR_CUDA);
   }
   const size_t C = capacity;
-  const size_t cap = (size_t)p->neighbor_cap;
+  ctx->lstride = ((size_t)p->neighbor_cap + 7) / 8 * 8;
+  const size_t cap = ctx->lstride;
   if ((rc = dalloc(ctx, &ctx->posH, C)) || (rc = dalloc(ctx, &ctx->pstH, C)) || (rc = dalloc(ctx, &ctx->velH, C)) ||
       (rc = dalloc(ctx, &ctx->scrH, C)) || (rc = dalloc(ctx, &ctx->posS, C)) || (rc = dalloc(ctx, &ctx->pstS, C)) ||
       (rc = dalloc(ctx, &ctx->velS, C)) || (rc = dalloc(ctx, &ctx->scrS, C)) || (rc = dalloc(ctx, &ctx->xl, C)) ||
@@ -1196,7 +1478,7 @@ int pbf_create(const pbf_params* p, size_t capacity, pbf_ctx** out) {
       (rc = dalloc(ctx, &ctx->cell_start, (size_t)ctx->nbins + 1)) ||
       (rc = dalloc(ctx, &ctx->scan_part, (size_t)ctx->nscan_parts)) || (rc = dalloc(ctx, &ctx->err, 1)) ||
       (rc = dalloc(ctx, &ctx->nudge, 1)) ||
-      (rc = dalloc(ctx, &ctx->pairs, C)) || (rc = dalloc(ctx, &ctx->nbr, C * cap)) ||
+      (rc = dalloc(ctx, &ctx->pairs, C)) || (rc = dalloc(ctx, &ctx->pairs_sorted, C)) || (rc = dalloc(ctx, &ctx->nbr, C * cap)) ||
       (rc = dalloc(ctx, &ctx->cnt, C)) || (rc = dalloc(ctx, &ctx->stage, 6 * C)) ||
       (rc = dalloc(ctx, &ctx->stage_i, C * cap + C)) || (rc = dalloc(ctx, &ctx->acc, 8)) ||
       (rc = dalloc(ctx, &ctx->maxerr, 1)) || (rc = dalloc(ctx, &ctx->hits, 1)))
@@ -1234,6 +1516,8 @@ int pbf_set_params(pbf_ctx* ctx, const pbf_params* p) {
   if (d.nbins != ctx->nbins || p->neighbor_cap != ctx->params.neighbor_cap) ctx->lists_valid = false;
   ctx->params = *p;
   ctx->dev = d;
+  ctx->fast = pbf::make_fast(d);
+  ctx->lstride = ((size_t)p->neighbor_cap + 7) / 8 * 8;
   std::memcpy(ctx->dims, dims, sizeof(dims));
   ctx->nbins = d.nbins;
   ctx->nscan_parts = (int)(((size_t)ctx->nbins + 1 + kScanTile - 1) / kScanTile);
@@ -1385,7 +1669,7 @@ int pbf_find_neighbors(pbf_ctx* ctx, size_t bin_b, size_t bin_e, size_t fill_b, 
   CK(cudaMemsetAsync(ctx->cell_count, 0, sizeof(uint32_t) * (size_t)ctx->nbins, s));
   k_hash<<<g, kBlock, 0, s>>>(ctx->dev, n, ctx->pstH, ctx->key, ctx->rank, ctx->cell_count, ctx->err);
   launch_sort_to_pairs(ctx);
-  k_reorder<true><<<g, kBlock, 0, s>>>(n, ctx->pairs, ctx->key, ctx->posH, ctx->pstH, ctx->velH, ctx->scrH,
+  k_reorder<true><<<g, kBlock, 0, s>>>(n, ctx->pairs_sorted, ctx->key, ctx->posH, ctx->pstH, ctx->velH, ctx->scrH,
                                        ctx->lamH, ctx->posS, ctx->pstS, ctx->velS, ctx->scrS, ctx->lamS, ctx->origS,
                                        ctx->keyH);
   const size_t f4 = sizeof(float4) * ctx->n;
@@ -1405,8 +1689,8 @@ int pbf_find_neighbors(pbf_ctx* ctx, size_t bin_b, size_t bin_e, size_t fill_b, 
 int pbf_compute_densities(pbf_ctx* ctx, size_t b, size_t e) {
   STAGE_PROLOGUE(b, e);
   if (int rc = need_lists(ctx)) return rc;
-  if (X) k_density<true><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->pstS);
-  else k_density<false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->pstS);
+  if (X) k_density<true><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->pstS);
+  else k_density<false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->pstS);
   CK(cudaMemcpyAsync(ctx->pstH, ctx->pstS, sizeof(float4) * ctx->n, cudaMemcpyDeviceToDevice, ctx->stream));
   return check_launch(ctx, "compute_densities");
 }
@@ -1414,8 +1698,8 @@ int pbf_compute_densities(pbf_ctx* ctx, size_t b, size_t e) {
 int pbf_compute_pressure_lambdas(pbf_ctx* ctx, size_t b, size_t e) {
   STAGE_PROLOGUE(b, e);
   if (int rc = need_lists(ctx)) return rc;
-  if (X) k_lambda<true><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->lamH);
-  else k_lambda<false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->lamH);
+  if (X) k_lambda<true><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->lamH);
+  else k_lambda<false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->lamH);
   return check_launch(ctx, "compute_pressure_lambdas");
 }
 
@@ -1425,10 +1709,10 @@ int pbf_compute_pressure_dps(pbf_ctx* ctx, size_t b, size_t e, int substep) {
   if (int rc = need_lists(ctx)) return rc;
   const bool SC = ctx->params.scorr_k > 0.0f;
   const Dev& P = ctx->dev;
-  if (X && SC) k_dp<true, true><<<g, kBlock, 0, ctx->stream>>>(P, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->lamH, ctx->scrH);
-  else if (X) k_dp<true, false><<<g, kBlock, 0, ctx->stream>>>(P, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->lamH, ctx->scrH);
-  else if (SC) k_dp<false, true><<<g, kBlock, 0, ctx->stream>>>(P, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->lamH, ctx->scrH);
-  else k_dp<false, false><<<g, kBlock, 0, ctx->stream>>>(P, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->lamH, ctx->scrH);
+  if (X && SC) k_dp<true, true><<<g, kBlock, 0, ctx->stream>>>(P, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->lamH, ctx->scrH);
+  else if (X) k_dp<true, false><<<g, kBlock, 0, ctx->stream>>>(P, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->lamH, ctx->scrH);
+  else if (SC) k_dp<false, true><<<g, kBlock, 0, ctx->stream>>>(P, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->lamH, ctx->scrH);
+  else k_dp<false, false><<<g, kBlock, 0, ctx->stream>>>(P, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->lamH, ctx->scrH);
   return check_launch(ctx, "compute_pressure_dps");
 }
 
@@ -1449,17 +1733,17 @@ int pbf_apply_surface_tension(pbf_ctx* ctx, size_t cb, size_t ce, size_t sb, siz
   if (int rc = check_span(ctx, sb, se)) return rc;
   STAGE_PROLOGUE(cb, ce);
   if (int rc = need_lists(ctx)) return rc;
-  if (X) k_color<true><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->scrH);
-  else k_color<false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->scrH);
-  k_surface<<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->scrH, ctx->velH);
+  if (X) k_color<true><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->scrH);
+  else k_color<false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->scrH);
+  k_surface<<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->scrH, ctx->velH);
   return check_launch(ctx, "apply_surface_tension");
 }
 
 int pbf_apply_viscosity(pbf_ctx* ctx, size_t b, size_t e) {
   STAGE_PROLOGUE(b, e);
   if (int rc = need_lists(ctx)) return rc;
-  if (X) k_viscosity<true, false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->velT, nullptr, nullptr, nullptr, nullptr);
-  else k_viscosity<false, false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->velT, nullptr, nullptr, nullptr, nullptr);
+  if (X) k_viscosity<true, false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->velT, nullptr, nullptr, nullptr, nullptr);
+  else k_viscosity<false, false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->velT, nullptr, nullptr, nullptr, nullptr);
   CK(cudaMemcpyAsync(ctx->velH, ctx->velT, sizeof(float4) * ctx->n, cudaMemcpyDeviceToDevice, ctx->stream));
   return check_launch(ctx, "apply_viscosity");
 }
@@ -1467,16 +1751,16 @@ int pbf_apply_viscosity(pbf_ctx* ctx, size_t b, size_t e) {
 int pbf_compute_vorticity(pbf_ctx* ctx, size_t b, size_t e) {
   STAGE_PROLOGUE(b, e);
   if (int rc = need_lists(ctx)) return rc;
-  if (X) k_vorticity<true><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->scrH, nullptr);
-  else k_vorticity<false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->scrH, nullptr);
+  if (X) k_vorticity<true><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->scrH, nullptr);
+  else k_vorticity<false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->scrH, nullptr);
   return check_launch(ctx, "compute_vorticity");
 }
 
 int pbf_apply_vorticity(pbf_ctx* ctx, size_t b, size_t e) {
   STAGE_PROLOGUE(b, e);
   if (int rc = need_lists(ctx)) return rc;
-  if (X) k_apply_vorticity<true, false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, nullptr, ctx->pstH, ctx->scrH, ctx->velH);
-  else k_apply_vorticity<false, false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->capacity, ctx->nbr, ctx->cnt, nullptr, ctx->pstH, ctx->scrH, ctx->velH);
+  if (X) k_apply_vorticity<true, false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->lstride, ctx->nbr, ctx->cnt, nullptr, ctx->pstH, ctx->scrH, ctx->velH);
+  else k_apply_vorticity<false, false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->lstride, ctx->nbr, ctx->cnt, nullptr, ctx->pstH, ctx->scrH, ctx->velH);
   return check_launch(ctx, "apply_vorticity");
 }
 
@@ -1542,7 +1826,7 @@ int pbf_get_neighbors(pbf_ctx* ctx, int32_t* idx, int32_t* count) {
   const size_t n = ctx->n, cap = (size_t)ctx->params.neighbor_cap;
   int32_t* di = ctx->stage_i;
   int32_t* dc = ctx->stage_i + n * cap;
-  k_export_neighbors<<<blocks_for(n), kBlock, 0, ctx->stream>>>((int)n, ctx->capacity, (int)cap, ctx->nbr, ctx->cnt,
+  k_export_neighbors<<<blocks_for(n), kBlock, 0, ctx->stream>>>((int)n, ctx->lstride, (int)cap, ctx->nbr, ctx->cnt,
                                                                  ctx->origH, di, dc);
   if (int rc = check_launch(ctx, "export_neighbors")) return rc;
   if (idx) CK(cudaMemcpyAsync(idx, di, n * cap * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1574,7 +1858,7 @@ int pbf_stats(pbf_ctx* ctx, pbf_stats_t* out) {
   CK(cudaMemsetAsync(ctx->maxerr, 0, sizeof(unsigned long long), s));
   CK(cudaMemsetAsync(ctx->hits, 0, sizeof(unsigned long long), s));
   if (ctx->n) {
-    k_stats<<<blocks_for(ctx->n), kBlock, 0, s>>>(ctx->dev, (int)ctx->n, ctx->capacity, ctx->nbr, ctx->cnt, ctx->pstH,
+    k_stats<<<blocks_for(ctx->n), kBlock, 0, s>>>(ctx->dev, (int)ctx->n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH,
                                                   ctx->posH, ctx->velH, ctx->acc, ctx->maxerr, ctx->hits);
     if (int rc = check_launch(ctx, "stats")) return rc;
   }
@@ -1706,7 +1990,7 @@ __global__ void k_noalloc_gather(int n, const unsigned long long* __restrict__ p
   sorted_id[b] = (uint32_t)(pr >> 32);
 }
 
-// Variant of k_fill that writes the lists straight into the caller's output
+// Variant of the list fill that writes the lists straight into the caller's output
 // in reference index space: out[id][k], -1 past the count.
 __global__ void __launch_bounds__(kBlock) k_noalloc_fill(Dev P, int n, const float4* __restrict__ pst,
                                                          const uint32_t* __restrict__ sorted_id,

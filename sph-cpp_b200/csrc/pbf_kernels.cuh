@@ -28,6 +28,7 @@ struct Dev {
   float scorr_k, scorr_n, inv_wdq;
   double vthr;    // 0.000001 * max_speed, compared in double (particles.h:380)
   double h_eps;   // smoothing_radius * 0.000001 in double (particles.h:420)
+  float skip_eps; // margin of the conservative bin skip in the list fill
   int dimx, dimy, dimz, nbins, cap;
 };
 

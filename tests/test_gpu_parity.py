@@ -209,10 +209,11 @@ def test_65k_100_steps_exact_bitwise_vs_oracle():
 # and one more reference run at eps = 600 gave an averaged max error of 3.683
 # against 3.741-3.763 for the others (2.2%): at this eps the max is set by
 # particles piled exactly into wall corners.
-# The bars: 1% wherever the spread is below 1%, else about twice the spread.
+# Four runs bound the spread from below only, so the bars are twice the
+# measured spread, and never tighter than 1%.
 STAT_BARS = {
-    600.0: {"mean_density_error": 0.01, "max_density_error": 0.05, "kinetic_energy": 0.015, "com": 0.01},
-    1.0: {"mean_density_error": 0.01, "max_density_error": 0.06, "kinetic_energy": 0.01, "com": 0.01},
+    600.0: {"mean_density_error": 0.014, "max_density_error": 0.044, "kinetic_energy": 0.02, "com": 0.01},
+    1.0: {"mean_density_error": 0.015, "max_density_error": 0.11, "kinetic_energy": 0.01, "com": 0.01},
 }
 STAT_KEYS = ("mean_density_error", "max_density_error", "kinetic_energy")
 
