@@ -86,7 +86,13 @@ typedef struct pbf_params {
    * (reciprocals, FMA), results within the 1e-5 parity tolerance.  The
    * neighbor search, predict and boundary clamp are always exact. */
   int32_t exact_math;
-  int32_t reserved[3];
+  /* Solver: 0 = the reference's K plain Jacobi iterations; 1 = learned warm
+   * start: iteration 1 takes lambda from the per-particle MLP (pbf_mlp_*),
+   * then plain iterations run while the mean clamped density error exceeds
+   * residual_tol, at most max_iterations in all (fast math only). */
+  int32_t solver;
+  float residual_tol;
+  int32_t max_iterations;
 } pbf_params;
 
 /* Physics statistics of the current state (a residual density pass over the
@@ -100,7 +106,8 @@ typedef struct pbf_stats_t {
   double mean_neighbors;      /* mean list length */
   uint64_t cap_hits;          /* particles whose list is at the cap */
   uint32_t error_flags;       /* PBF_FLAG_* bits raised since the last pbf_stats */
-  uint32_t pad;
+  uint32_t solver_iterations; /* Jacobi iterations the last step ran */
+  double solver_residual;     /* learned solver: mean clamped density error at its last check */
 } pbf_stats_t;
 
 typedef struct pbf_ctx pbf_ctx;
@@ -225,6 +232,41 @@ int pbf_kernel_times(pbf_ctx* ctx, int max_kinds, const char** names, int64_t* l
 int pbf_reset_timing(pbf_ctx* ctx);
 /* Number of kernel launches one pbf_step(ctx, 1) issues. */
 int pbf_launches_per_step(pbf_ctx* ctx, int64_t* out);
+
+/* ---- learned warm start: the per-particle MLP ----
+ * 12 -> 64 -> 64 -> 1, GELU, BF16 tensor-core GEMMs with FP32 accumulation.
+ * Parameters are fp32 masters in the order W1[64][12], b1[64], W2[64][64],
+ * b2[64], w3[64], b3 (PBF_MLP_PARAMS floats); the normalisation block is
+ * mean[12], inv_std[12], label_scale (PBF_MLP_NORM floats).  Features of a
+ * particle at the first Jacobi iteration (raw, before normalisation):
+ *   0 neighbours/64   1 C = max(rho/rho0-1, 0)   2 rho/rho0 - 1
+ *   3 S = sum|grad C_j|^2 + |grad C_i|^2         4 plain lambda -C/(S+eps)
+ *   5 lambda the particle received in the previous step
+ *   6 |grad C_i|^2 / S   7 share of neighbours closer than h
+ *   8 v_y dt/h   9 |v| dt/h   10 height above the floor / h (<= 4)
+ *   11 distance to the nearest wall / h (<= 4)
+ * The label is the sum of the lambdas the plain solver applies over its K
+ * iterations; the network predicts label/label_scale. */
+#define PBF_MLP_FEATURES 12
+#define PBF_MLP_PARAMS 5057
+#define PBF_MLP_NORM 25
+int pbf_mlp_init(pbf_ctx* ctx, uint64_t seed);
+int pbf_mlp_get(pbf_ctx* ctx, float* params, float* norm);
+int pbf_mlp_set(pbf_ctx* ctx, const float* params, const float* norm);
+/* With recording on, fused plain steps keep the last step's features and
+ * labels on the device; pbf_get_training_data copies them out (slot order). */
+int pbf_set_recording(pbf_ctx* ctx, int on);
+int pbf_get_training_data(pbf_ctx* ctx, float* features, float* labels);
+/* adam_steps Adam updates (beta 0.9/0.999, eps 1e-8) on batches of `batch`
+ * samples drawn from the recorded step with a counter-based RNG; the mean
+ * squared error of the last batch is returned in *loss. */
+int pbf_mlp_train(pbf_ctx* ctx, int adam_steps, int batch, float lr, uint64_t seed, float* loss);
+/* Gradient of the mean squared error over n host samples (normalised
+ * features, targets in network units) with the current parameters. */
+int pbf_mlp_gradients(pbf_ctx* ctx, const float* features, const float* targets, size_t n, float* grad,
+                      float* loss);
+/* Network output for n host samples of normalised features. */
+int pbf_mlp_predict(pbf_ctx* ctx, const float* features, size_t n, float* y);
 
 /* ---- neighbor search that allocates nothing ----
  * No counterpart in the reference.  For callers that may not allocate device

@@ -25,7 +25,7 @@ REF_SOURCES = Path(os.environ.get("PBF_REFERENCE_ROOT", "/root/reference"))
 NVCC_ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUDA_SOURCES = ["csrc/pbf_cuda.cu"]
 HOST_SOURCES = ["csrc/pbf_host.cpp"]
-DEPS = ["csrc/pbf_kernels.cuh", "csrc/pbf_fast.cuh", "csrc/pbf_internal.h", "../include/pbf.h"]
+DEPS = ["csrc/pbf_kernels.cuh", "csrc/pbf_fast.cuh", "csrc/pbf_mlp.cuh", "csrc/pbf_learn.cuh", "csrc/pbf_internal.h", "../include/pbf.h"]
 
 
 def _nvcc() -> str:

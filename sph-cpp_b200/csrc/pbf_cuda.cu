@@ -21,6 +21,7 @@
 // Particles are kept in cell order between steps, so neighbours of a warp's
 // particles sit in a few contiguous slot ranges (L1/L2 reuse); the reference
 // index of every slot (origH) maps results back for downloads and parity.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cfloat>
@@ -38,6 +39,7 @@
 #include "pbf_internal.h"
 #include "pbf_kernels.cuh"
 #include "pbf_fast.cuh"
+#include "pbf_learn.cuh"
 
 using pbf::Dev;
 using pbf::Fast;
@@ -291,8 +293,9 @@ __global__ void k_rank_in_bin(int n, const unsigned long long* __restrict__ pair
   sorted[b0 + rank] = pr;
 }
 
-// Gather the state into sorted order.  full = also lambda and scratch (the
-// per-stage path, where every reference array must follow its particle).
+// Gather the state into sorted order.  FULL = also scratch and lambda (the
+// per-stage path, where every reference array must follow its particle); the
+// fused step passes the learned warm start's lambda sums as lamH/lamS.
 template <bool FULL>
 __global__ void k_reorder(int n, const unsigned long long* __restrict__ pairs, const uint32_t* __restrict__ key,
                           const float4* __restrict__ posH, const float4* __restrict__ pstH,
@@ -308,10 +311,8 @@ __global__ void k_reorder(int n, const unsigned long long* __restrict__ pairs, c
   posS[b] = posH[a];
   pstS[b] = pstH[a];
   velS[b] = velH[a];
-  if (FULL) {
-    scrS[b] = scrH[a];
-    lamS[b] = lamH[a];
-  }
+  if (FULL) scrS[b] = scrH[a];
+  if (lamS) lamS[b] = lamH[a];  // FULL: lambda; fused step: last step's lambda sum, when kept
 }
 
 // fill_neighbors (neighbors.h:197-230) over slots in sorted order: the 27
@@ -518,21 +519,38 @@ __global__ void __launch_bounds__(kBlock) k_density_lambda(Dev P, int n, size_t 
 // position by the others from the delta-p pass on — the order in which the
 // reference's parallel builds see it when every neighbour reads before the
 // write; the exact path instead recomputes lambda (k_lambda_fixup).
+// Modes: kDlPlain; kDlRecord also writes the learned warm start's features
+// (first iteration) and sums the applied lambdas into the label; kDlCheck is
+// the learned solver's residual check: skipped once the step has converged,
+// else it adds every particle's clamped density error to io.err_sum.
+enum { kDlPlain = 0, kDlRecord = 1, kDlCheck = 2 };
+
+struct LearnIO {
+  float* feats;           // [N][12] raw features (kDlRecord, first iteration)
+  float* lamsum;          // lambda applied this step (label / next step's feature)
+  const float* lamprev;   // lambda applied last step, in this step's order
+  pbf::SolveState* state; // kDlCheck
+  int first;              // first Jacobi iteration of the step
+};
+
+template <int MODE>
 __global__ void __launch_bounds__(kBlock) kf_density_lambda(Dev P, Fast F, int n, size_t stride,
                                                             const int32_t* __restrict__ nbr,
                                                             const int32_t* __restrict__ cnt,
                                                             const float4* __restrict__ pst, float4* xl, float4* vel,
-                                                            float* lam, uint32_t* nudge) {
+                                                            float* lam, uint32_t* nudge, LearnIO io) {
+  if (MODE == kDlCheck && io.state->done) return;
   const pbf::Group G = pbf::group_of(n);
   const int b = G.b;
   const float4 xp = pst[b];
   const int c = G.live ? cnt[b] : 0;
-  float sw = 0.f, sgx = 0.f, sgy = 0.f, sgz = 0.f, sc = 0.f;
+  float sw = 0.f, sgx = 0.f, sgy = 0.f, sgz = 0.f, sc = 0.f, nh = 0.f;
   int close = 0;
   pbf::gwalk1(nbr + (size_t)b * stride, c, G.lane, pst, [&](int, float4 xq) {
     const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
     const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
     close |= d2 < 4e-16f;
+    if (MODE == kDlRecord) nh += d2 < F.h2 ? 1.f : 0.f;
     sw += pbf::poly_cube(F, d2);
     const float t = F.lam_grad * pbf::spikey_over_r(F, d2);
     sgx = fmaf(-t, dx, sgx);
@@ -545,19 +563,122 @@ __global__ void __launch_bounds__(kBlock) kf_density_lambda(Dev P, Fast F, int n
   sgy = pbf::gsum(sgy);
   sgz = pbf::gsum(sgz);
   sc = pbf::gsum(sc);
+  if (MODE == kDlRecord) nh = pbf::gsum(nh);
   close = pbf::gor(close);
+  const float rho = fmaf(F.m_poly, sw, F.m_w0);
+  if (MODE == kDlCheck) {
+    float e = (G.live && G.lane == 0) ? fmaxf(fmaf(rho, F.inv_rho0, -1.0f), 0.0f) : 0.0f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+    if ((threadIdx.x & 31) == 0 && e > 0.0f) atomicAdd(&io.state->err_sum, (double)e);
+  }
   if (!G.live || G.lane != 0) return;
+  const float g2 = sgx * sgx + sgy * sgy + sgz * sgz;
   if (close) {  // a neighbour (almost) on top: the reference-ordered path decides the nudge
     density_lambda_one<false>(P, b, stride, nbr, cnt, pst, xl, vel, lam, nudge);
+  } else {
+    const float C = fmaxf(fmaf(rho, F.inv_rho0, -1.0f), 0.0f);
+    const float l = -C / (sc + g2 + F.lambda_eps);
+    xl[b] = make_float4(xp.x, xp.y, xp.z, l);
+    vel[b].w = rho;
+    lam[b] = l;
+  }
+  if (MODE == kDlRecord) {
+    if (io.first) {
+      float f[pbf::kMlpIn];
+      pbf::raw_features(P, F, f, c, rho, sc, g2, (int)nh, io.lamprev[b], vel[b], xp);
+#pragma unroll
+      for (int k = 0; k < pbf::kMlpIn; ++k) io.feats[(size_t)b * pbf::kMlpIn + k] = f[k];
+      io.lamsum[b] = lam[b];
+    } else {
+      io.lamsum[b] += lam[b];
+    }
+  }
+}
+
+// Learned warm start, first Jacobi iteration: the gather of kf_density_lambda,
+// the particle's 12 features, then the MLP on the tensor cores for the
+// block's 32 particles (two warps, 16 rows each).  A single over-relaxed
+// iteration on its own overshoots and the overshoot feeds the velocity update
+// (measured on the oracle: 1 iteration at 2.5x lambda ends near 4% density
+// error where 1 plain iteration ends near 1.5%), so the residual-checked plain
+// iterations that follow are part of the method.
+constexpr float kWarmMaxGain = 3.0f;
+__global__ void __launch_bounds__(kBlock) kl_density_lambda(Dev P, Fast F, pbf::MlpDev M, int n, size_t stride,
+                                                            const int32_t* __restrict__ nbr,
+                                                            const int32_t* __restrict__ cnt,
+                                                            const float4* __restrict__ pst, float4* xl, float4* vel,
+                                                            float* lam, uint32_t* nudge, float* lamsum,
+                                                            const float* __restrict__ lamprev) {
+  constexpr int kP = kBlock / pbf::kGL;  // particles per block
+  __shared__ __align__(16) __nv_bfloat16 sf[kP * pbf::kMlpInPad];
+  __shared__ float sy[kP];
+  __shared__ int sclose[kP];
+  const pbf::Group G = pbf::group_of(n);
+  const int b = G.b, p = threadIdx.x / pbf::kGL;
+  const float4 xp = pst[b];
+  const int c = G.live ? cnt[b] : 0;
+  float sw = 0.f, sgx = 0.f, sgy = 0.f, sgz = 0.f, sc = 0.f, nh = 0.f;
+  int close = 0;
+  pbf::gwalk1(nbr + (size_t)b * stride, c, G.lane, pst, [&](int, float4 xq) {
+    const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
+    const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+    close |= d2 < 4e-16f;
+    nh += d2 < F.h2 ? 1.f : 0.f;
+    sw += pbf::poly_cube(F, d2);
+    const float t = F.lam_grad * pbf::spikey_over_r(F, d2);
+    sgx = fmaf(-t, dx, sgx);
+    sgy = fmaf(-t, dy, sgy);
+    sgz = fmaf(-t, dz, sgz);
+    sc = fmaf(t * t, d2, sc);
+  });
+  sw = pbf::gsum(sw);
+  sgx = pbf::gsum(sgx);
+  sgy = pbf::gsum(sgy);
+  sgz = pbf::gsum(sgz);
+  sc = pbf::gsum(sc);
+  nh = pbf::gsum(nh);
+  close = pbf::gor(close);
+  const float rho = fmaf(F.m_poly, sw, F.m_w0);
+  const float g2 = sgx * sgx + sgy * sgy + sgz * sgz;
+  if (G.lane == 0) {
+    float f[pbf::kMlpIn];
+    pbf::raw_features(P, F, f, c, rho, sc, g2, (int)nh, G.live ? lamprev[b] : 0.0f, vel[b], xp);
+#pragma unroll
+    for (int k = 0; k < pbf::kMlpInPad; ++k)
+      sf[p * pbf::kMlpInPad + k] =
+          __float2bfloat16_rn(k < pbf::kMlpIn && G.live ? (f[k] - M.feat_mean[k]) * M.feat_inv_std[k] : 0.0f);
+    sclose[p] = G.live && close;
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp < kP / 16) {
+    uint32_t a[4];
+    pbf::load_a_rows16(a, sf + warp * 16 * pbf::kMlpInPad, lane);
+    float y_lo, y_hi;
+    pbf::mlp_forward16(M, a, lane, y_lo, y_hi);
+    if ((lane & 3) == 0) {
+      sy[warp * 16 + (lane >> 2)] = y_lo;
+      sy[warp * 16 + (lane >> 2) + 8] = y_hi;
+    }
+  }
+  __syncthreads();
+  if (!G.live || G.lane != 0) return;
+  if (sclose[p]) {
+    density_lambda_one<false>(P, b, stride, nbr, cnt, pst, xl, vel, lam, nudge);
+    lamsum[b] = lam[b];
     return;
   }
-  const float rho = fmaf(F.m_poly, sw, F.m_w0);
+  // The network's lambda, kept between the plain first-iteration lambda l1
+  // and kWarmMaxGain * l1 (both <= 0): zero where the constraint is inactive,
+  // as in the plain solver, and an over-relaxation of at most kWarmMaxGain.
   const float C = fmaxf(fmaf(rho, F.inv_rho0, -1.0f), 0.0f);
-  sc = fmaf(sgz, sgz, fmaf(sgy, sgy, fmaf(sgx, sgx, sc)));
-  const float l = -C / (sc + F.lambda_eps);
+  const float l1 = -C / (sc + g2 + F.lambda_eps);
+  const float l = fminf(fmaxf(sy[p] * M.label_scale, kWarmMaxGain * l1), l1);
   xl[b] = make_float4(xp.x, xp.y, xp.z, l);
   vel[b].w = rho;
   lam[b] = l;
+  lamsum[b] = l;
 }
 
 // Lambda recomputed from the (nudged) positions in xl, only when the
@@ -848,13 +969,15 @@ __global__ void __launch_bounds__(kBlock) k_apply_vorticity(Dev P, int n, size_t
 }
 
 // ---- fast gathers (exact_math = 0), kGL lanes per particle, see pbf_fast.cuh ----
-template <bool SCORR, bool LAST>
+// COND: the learned solver's extra iterations, skipped once the step has
+// converged; lamsum (when given) accumulates the applied lambda.
+template <bool SCORR, bool LAST, bool COND>
 __global__ void __launch_bounds__(kBlock) kf_dp_update(Dev P, Fast F, int n, size_t stride,
                                                        const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
                                                        const float4* __restrict__ xl, float4* pst,
                                                        const float4* __restrict__ pos, float4* vel,
-                                                       const float* __restrict__ lam,
-                                                       const uint32_t* __restrict__ nudge) {
+                                                       const pbf::SolveState* __restrict__ state, float* lamsum) {
+  if (COND && state->done) return;
   const pbf::Group G = pbf::group_of(n);
   const int b = G.b;
   const float4 xp = xl[b];
@@ -875,6 +998,7 @@ __global__ void __launch_bounds__(kBlock) kf_dp_update(Dev P, Fast F, int n, siz
   ay = pbf::gsum(ay);
   az = pbf::gsum(az);
   if (!G.live || G.lane != 0) return;
+  if (lamsum) lamsum[b] += xp.w;
   const float3 s = pbf::boundary(P, make_float3(pbf::xadd(xp.x, F.dp_scale * ax), pbf::xadd(xp.y, F.dp_scale * ay),
                                                 pbf::xadd(xp.z, F.dp_scale * az)));
   const float4 ns = make_float4(s.x, s.y, s.z, 0.0f);
@@ -1061,6 +1185,17 @@ struct pbf_ctx {
   double* acc = nullptr;
   unsigned long long *maxerr = nullptr, *hits = nullptr;
 
+  // learned warm start
+  float *lamsumH = nullptr, *lamprevS = nullptr, *feats = nullptr;
+  pbf::SolveState* state = nullptr;
+  bool recording = false;
+  float *mlp_params = nullptr, *mlp_grad = nullptr, *mlp_m = nullptr, *mlp_v = nullptr, *mlp_norm = nullptr;
+  float* mlp_loss = nullptr;
+  __nv_bfloat16 *w1b = nullptr, *w2b = nullptr, *w2tb = nullptr;
+  float label_scale = 1.0f;
+  int adam_t = 0;
+  bool mlp_ready = false;
+
   std::map<int, cudaGraphExec_t> graphs;
   std::vector<void*> allocations;
 
@@ -1112,6 +1247,11 @@ int make_dev(pbf_ctx* ctx, const pbf_params& p, Dev& d, int64_t dims[3]) {
     return fail(ctx, PBF_ERR_PARAMS, "time_step, smoothing_radius, neighbor_bin_spacing, rest_density and "
                                      "rest_mass must be > 0");
   if (p.solve_steps < 0) return fail(ctx, PBF_ERR_PARAMS, "solve_steps must be >= 0");
+  if (p.solver != 0 && p.solver != 1) return fail(ctx, PBF_ERR_PARAMS, "solver must be 0 (plain) or 1 (learned)");
+  if (p.solver == 1 && p.exact_math)
+    return fail(ctx, PBF_ERR_PARAMS, "the learned warm start runs in fast math only (exact_math = 0)");
+  if (p.solver == 1 && (p.max_iterations < 1 || p.max_iterations > 64))
+    return fail(ctx, PBF_ERR_PARAMS, "max_iterations must be in [1, 64]");
   if (p.neighbor_cap < 1 || p.neighbor_cap > 64)
     return fail(ctx, PBF_ERR_PARAMS, "neighbor_cap must be in [1, 64], got %d", p.neighbor_cap);
   const float s = p.neighbor_bin_spacing;
@@ -1297,6 +1437,68 @@ void launch_fill(pbf_ctx* ctx, const float4* pst) {
 }
 
 // ---- the fused step (graph-capturable: fixed pointers, no host sync) ----
+pbf::MlpDev mlp_dev(const pbf_ctx* ctx) {
+  pbf::MlpDev M;
+  M.w1 = ctx->w1b;
+  M.w2 = ctx->w2b;
+  M.w2t = ctx->w2tb;
+  M.b1 = ctx->mlp_params + pbf::kOffB1;
+  M.b2 = ctx->mlp_params + pbf::kOffB2;
+  M.w3 = ctx->mlp_params + pbf::kOffW3;
+  M.b3 = ctx->mlp_params + pbf::kOffB3;
+  M.feat_mean = ctx->mlp_norm;
+  M.feat_inv_std = ctx->mlp_norm + pbf::kMlpIn;
+  M.label_scale = ctx->label_scale;
+  return M;
+}
+
+// The learned warm start's Jacobi loop: iteration 1 with the MLP's lambda,
+// then up to max_iterations-1 plain iterations, each run only while the mean
+// clamped density error at the current x* exceeds residual_tol (a check pass
+// decides; once converged, the remaining launches return at once), a final
+// check recording the step's residual, and the velocity update.
+template <bool SCORR>
+void launch_learned_solve(pbf_ctx* ctx) {
+  const int n = (int)ctx->n;
+  const size_t st = ctx->lstride;
+  const Dev& P = ctx->dev;
+  const Fast& F = ctx->fast;
+  cudaStream_t s = ctx->stream;
+  const int g = blocks_for(n), gg = blocks_for((size_t)n * pbf::kGL);
+  const float tol = ctx->params.residual_tol;
+  const int iters = ctx->params.max_iterations > 0 ? ctx->params.max_iterations : 1;
+  cudaMemsetAsync(ctx->state, 0, sizeof(pbf::SolveState), s);
+  LearnIO io{nullptr, nullptr, nullptr, ctx->state, 0};
+  {
+    Launch L(ctx, "density_lambda_learned");
+    kl_density_lambda<<<gg, kBlock, 0, s>>>(P, F, mlp_dev(ctx), n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl,
+                                            ctx->velS, ctx->lamH, ctx->nudge, ctx->lamsumH, ctx->lamprevS);
+  }
+  {
+    Launch L(ctx, "dp_update");
+    kf_dp_update<SCORR, false, false><<<gg, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS,
+                                                           ctx->posS, ctx->velS, ctx->state, nullptr);
+  }
+  for (int r = 1; r <= iters; ++r) {
+    const bool final_check = r == iters;
+    {
+      Launch L(ctx, "residual_check");
+      kf_density_lambda<kDlCheck><<<gg, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl,
+                                                        ctx->velS, ctx->lamH, ctx->nudge, io);
+    }
+    {
+      Launch L(ctx, "decide");
+      pbf::k_decide<<<1, 1, 0, s>>>(n, tol, final_check ? 1 : 0, ctx->state);
+    }
+    if (final_check) break;
+    Launch L(ctx, "dp_update");
+    kf_dp_update<SCORR, false, true><<<gg, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS,
+                                                          ctx->posS, ctx->velS, ctx->state, ctx->lamsumH);
+  }
+  Launch L(ctx, "update_velocities");
+  k_update_v<<<g, kBlock, 0, s>>>(P, n, ctx->pstS, ctx->posS, ctx->velS);
+}
+
 template <bool X, bool SCORR>
 void launch_step_t(pbf_ctx* ctx) {
   const int n = (int)ctx->n;
@@ -1313,24 +1515,33 @@ void launch_step_t(pbf_ctx* ctx) {
   launch_sort_to_pairs(ctx);
   {
     Launch L(ctx, "reorder");
+    const bool keep = !X && (ctx->recording || ctx->params.solver == 1);
     k_reorder<false><<<g, kBlock, 0, s>>>(n, ctx->pairs_sorted, ctx->key, ctx->posH, ctx->pstH, ctx->velH, nullptr,
-                                          nullptr, ctx->posS, ctx->pstS, ctx->velS, nullptr, nullptr, ctx->origS,
-                                          ctx->keyH);
+                                          keep ? ctx->lamsumH : nullptr, ctx->posS, ctx->pstS, ctx->velS, nullptr,
+                                          keep ? ctx->lamprevS : nullptr, ctx->origS, ctx->keyH);
   }
   launch_fill(ctx, ctx->pstS);
   const int K = ctx->params.solve_steps;
   const Fast& F = ctx->fast;
   const int gg = blocks_for((size_t)n * pbf::kGL);  // kGL lanes per particle
+  if (!X && ctx->params.solver == 1) {
+    launch_learned_solve<SCORR>(ctx);
+  } else {
+  LearnIO io{ctx->feats, ctx->lamsumH, ctx->lamprevS, ctx->state, 0};
   for (int it = 0; it < K; ++it) {
+    io.first = it == 0;
     if (X) cudaMemsetAsync(ctx->nudge, 0, sizeof(uint32_t), s);
     {
       Launch L(ctx, "density_lambda");
       if (X)
         k_density_lambda<X><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl, ctx->velS,
                                                  ctx->lamH, ctx->nudge);
+      else if (ctx->recording)
+        kf_density_lambda<kDlRecord><<<gg, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl,
+                                                           ctx->velS, ctx->lamH, ctx->nudge, io);
       else
-        kf_density_lambda<<<gg, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl, ctx->velS,
-                                               ctx->lamH, ctx->nudge);
+        kf_density_lambda<kDlPlain><<<gg, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl,
+                                                          ctx->velS, ctx->lamH, ctx->nudge, io);
     }
     if (X) {
       Launch L(ctx, "lambda_fixup");
@@ -1348,14 +1559,15 @@ void launch_step_t(pbf_ctx* ctx) {
                                                           ctx->posS, ctx->velS, ctx->lamH, ctx->nudge);
     } else {
       if (last)
-        kf_dp_update<SCORR, true><<<gg, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS,
-                                                       ctx->posS, ctx->velS, ctx->lamH, ctx->nudge);
+        kf_dp_update<SCORR, true, false><<<gg, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS,
+                                                              ctx->posS, ctx->velS, ctx->state, nullptr);
       else
-        kf_dp_update<SCORR, false><<<gg, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS,
-                                                        ctx->posS, ctx->velS, ctx->lamH, ctx->nudge);
+        kf_dp_update<SCORR, false, false><<<gg, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS,
+                                                               ctx->posS, ctx->velS, ctx->state, nullptr);
     }
   }
-  if (K == 0) {
+  }
+  if (K == 0 && !(!X && ctx->params.solver == 1)) {
     Launch L(ctx, "update_velocities");
     k_update_v<<<g, kBlock, 0, s>>>(P, n, ctx->pstS, ctx->posS, ctx->velS);
   }
@@ -1420,8 +1632,14 @@ int launches_per_step(const pbf_ctx* ctx) {
   // fix-up], delta-p) + (K==0: velocity)
   // + 2 if gamma + 4 (visc, vort, apply, visc)
   const int K = ctx->params.solve_steps;
+  const int tail = (ctx->params.gamma != 0.0f ? 2 : 0) + 4;
+  if (ctx->params.solver == 1 && !ctx->params.exact_math) {
+    // learned: warm iteration (2) + (iters-1) x (check, decide, delta-p) + final check, decide + velocity
+    const int it = ctx->params.max_iterations > 0 ? ctx->params.max_iterations : 1;
+    return 1 + 3 + 1 + 1 + 1 + 1 + 2 + 3 * (it - 1) + 2 + 1 + tail;
+  }
   const int per_iter = ctx->params.exact_math ? 3 : 2;
-  return 1 + 3 + 1 + 1 + 1 + 1 + per_iter * K + (K == 0 ? 1 : 0) + (ctx->params.gamma != 0.0f ? 2 : 0) + 4;
+  return 1 + 3 + 1 + 1 + 1 + 1 + per_iter * K + (K == 0 ? 1 : 0) + tail;
 }
 
 }  // namespace
@@ -1481,8 +1699,19 @@ int pbf_create(const pbf_params* p, size_t capacity, pbf_ctx** out) {
       (rc = dalloc(ctx, &ctx->pairs, C)) || (rc = dalloc(ctx, &ctx->pairs_sorted, C)) || (rc = dalloc(ctx, &ctx->nbr, C * cap)) ||
       (rc = dalloc(ctx, &ctx->cnt, C)) || (rc = dalloc(ctx, &ctx->stage, 6 * C)) ||
       (rc = dalloc(ctx, &ctx->stage_i, C * cap + C)) || (rc = dalloc(ctx, &ctx->acc, 8)) ||
-      (rc = dalloc(ctx, &ctx->maxerr, 1)) || (rc = dalloc(ctx, &ctx->hits, 1)))
+      (rc = dalloc(ctx, &ctx->maxerr, 1)) || (rc = dalloc(ctx, &ctx->hits, 1)) ||
+      (rc = dalloc(ctx, &ctx->lamsumH, C)) || (rc = dalloc(ctx, &ctx->lamprevS, C)) ||
+      (rc = dalloc(ctx, &ctx->state, 1)) || (rc = dalloc(ctx, &ctx->mlp_params, pbf::kMlpParams)) ||
+      (rc = dalloc(ctx, &ctx->mlp_grad, pbf::kMlpParams)) || (rc = dalloc(ctx, &ctx->mlp_m, pbf::kMlpParams)) ||
+      (rc = dalloc(ctx, &ctx->mlp_v, pbf::kMlpParams)) || (rc = dalloc(ctx, &ctx->mlp_norm, 32)) ||
+      (rc = dalloc(ctx, &ctx->mlp_loss, 1)) || (rc = dalloc(ctx, &ctx->w1b, pbf::kMlpH * pbf::kMlpInPad)) ||
+      (rc = dalloc(ctx, &ctx->w2b, pbf::kMlpH * pbf::kMlpH)) || (rc = dalloc(ctx, &ctx->w2tb, pbf::kMlpH * pbf::kMlpH)))
     return bail(rc);
+  if (cudaMemsetAsync(ctx->lamsumH, 0, C * sizeof(float), ctx->stream) != cudaSuccess ||
+      cudaMemsetAsync(ctx->state, 0, sizeof(pbf::SolveState), ctx->stream) != cudaSuccess) {
+    fail(ctx, PBF_ERR_CUDA, "initialisation failed");
+    return bail(PBF_ERR_CUDA);
+  }
   if (cudaMemsetAsync(ctx->err, 0, sizeof(uint32_t), ctx->stream) != cudaSuccess ||
       cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
     fail(ctx, PBF_ERR_CUDA, "initialisation failed");
@@ -1546,6 +1775,7 @@ int pbf_upload(pbf_ctx* ctx, const float* x, const float* v, size_t n) {
   float* dv = ctx->stage + 3 * ctx->capacity;
   CK(cudaMemcpyAsync(dx, x, n * 3 * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
   if (v) CK(cudaMemcpyAsync(dv, v, n * 3 * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemsetAsync(ctx->lamsumH, 0, n * sizeof(float), ctx->stream));  // no lambda history yet
   k_upload<<<blocks_for(n), kBlock, 0, ctx->stream>>>((int)n, dx, v ? dv : nullptr, ctx->posH, ctx->pstH,
                                                       ctx->velH, ctx->scrH, ctx->lamH, ctx->origH);
   return check_launch(ctx, "upload");
@@ -1773,6 +2003,8 @@ int pbf_update_positions(pbf_ctx* ctx, size_t b, size_t e) {
 int pbf_step(pbf_ctx* ctx, int nsteps) {
   if (!ctx || nsteps < 0) return PBF_ERR_ARG;
   if (nsteps == 0) return PBF_OK;
+  if (ctx->params.solver == 1 && !ctx->mlp_ready)
+    return fail(ctx, PBF_ERR_STATE, "learned solver without a network: call pbf_mlp_init or pbf_mlp_set");
   if (ctx->n == 0) {
     ctx->lists_valid = true;  // an empty set has (empty) lists
     return PBF_OK;
@@ -1883,6 +2115,157 @@ int pbf_stats(pbf_ctx* ctx, pbf_stats_t* out) {
   out->mean_neighbors = acc[5] / n;
   out->cap_hits = hits;
   out->error_flags = err;
+  if (ctx->params.solver == 1) {
+    pbf::SolveState stt;
+    CK(cudaMemcpy(&stt, ctx->state, sizeof(stt), cudaMemcpyDeviceToHost));
+    out->solver_iterations = 1u + stt.iterations;
+    out->solver_residual = stt.residual;
+  } else {
+    out->solver_iterations = (uint32_t)ctx->params.solve_steps;
+    out->solver_residual = -1.0;
+  }
+  return PBF_OK;
+}
+
+// ---- learned warm start ----
+static int mlp_refresh(pbf_ctx* ctx) {
+  pbf::k_mlp_sync<<<(pbf::kMlpH * pbf::kMlpH + 255) / 256, 256, 0, ctx->stream>>>(ctx->mlp_params, ctx->w1b, ctx->w2b,
+                                                                                ctx->w2tb);
+  return check_launch(ctx, "mlp_sync");
+}
+
+int pbf_mlp_init(pbf_ctx* ctx, uint64_t seed) {
+  if (!ctx) return PBF_ERR_ARG;
+  // Xavier-uniform weights from a SplitMix64 stream, zero biases.
+  std::vector<float> P(pbf::kMlpParams, 0.0f);
+  uint64_t z = seed;
+  auto uni = [&]() {
+    z += 0x9E3779B97F4A7C15ull;
+    uint64_t r = z;
+    r = (r ^ (r >> 30)) * 0xBF58476D1CE4E5B9ull;
+    r = (r ^ (r >> 27)) * 0x94D049BB133111EBull;
+    r ^= r >> 31;
+    return (float)(r >> 40) * 0x1p-24f * 2.0f - 1.0f;
+  };
+  const float a1 = std::sqrt(6.0f / (pbf::kMlpIn + pbf::kMlpH)), a2 = std::sqrt(6.0f / (2 * pbf::kMlpH)),
+              a3 = std::sqrt(6.0f / (pbf::kMlpH + 1));
+  for (int i = 0; i < pbf::kMlpH * pbf::kMlpIn; ++i) P[pbf::kOffW1 + i] = a1 * uni();
+  for (int i = 0; i < pbf::kMlpH * pbf::kMlpH; ++i) P[pbf::kOffW2 + i] = a2 * uni();
+  for (int i = 0; i < pbf::kMlpH; ++i) P[pbf::kOffW3 + i] = a3 * uni();
+  std::vector<float> norm(PBF_MLP_NORM, 0.0f);
+  for (int k = 0; k < pbf::kMlpIn; ++k) norm[pbf::kMlpIn + k] = 1.0f;
+  norm[2 * pbf::kMlpIn] = 1.0f;
+  return pbf_mlp_set(ctx, P.data(), norm.data());
+}
+
+int pbf_mlp_set(pbf_ctx* ctx, const float* params, const float* norm) {
+  if (!ctx || !params || !norm) return PBF_ERR_ARG;
+  if (!(norm[2 * pbf::kMlpIn] != 0.0f)) return fail(ctx, PBF_ERR_ARG, "label_scale must be nonzero");
+  CK(cudaMemcpyAsync(ctx->mlp_params, params, sizeof(float) * pbf::kMlpParams, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->mlp_norm, norm, sizeof(float) * PBF_MLP_NORM, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemsetAsync(ctx->mlp_m, 0, sizeof(float) * pbf::kMlpParams, ctx->stream));
+  CK(cudaMemsetAsync(ctx->mlp_v, 0, sizeof(float) * pbf::kMlpParams, ctx->stream));
+  ctx->label_scale = norm[2 * pbf::kMlpIn];
+  ctx->adam_t = 0;
+  if (int rc = mlp_refresh(ctx)) return rc;
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->mlp_ready = true;
+  drop_graphs(ctx);  // the label scale is a kernel argument of the learned step
+  return PBF_OK;
+}
+
+int pbf_mlp_get(pbf_ctx* ctx, float* params, float* norm) {
+  if (!ctx) return PBF_ERR_ARG;
+  if (params)
+    CK(cudaMemcpyAsync(params, ctx->mlp_params, sizeof(float) * pbf::kMlpParams, cudaMemcpyDeviceToHost, ctx->stream));
+  if (norm) CK(cudaMemcpyAsync(norm, ctx->mlp_norm, sizeof(float) * PBF_MLP_NORM, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PBF_OK;
+}
+
+int pbf_set_recording(pbf_ctx* ctx, int on) {
+  if (!ctx) return PBF_ERR_ARG;
+  if (on && !ctx->feats) {
+    if (int rc = dalloc(ctx, &ctx->feats, ctx->capacity * pbf::kMlpIn)) return rc;
+    CK(cudaMemsetAsync(ctx->feats, 0, ctx->capacity * pbf::kMlpIn * sizeof(float), ctx->stream));
+  }
+  if ((on != 0) != ctx->recording) drop_graphs(ctx);
+  ctx->recording = on != 0;
+  return PBF_OK;
+}
+
+int pbf_get_training_data(pbf_ctx* ctx, float* features, float* labels) {
+  if (!ctx) return PBF_ERR_ARG;
+  if (!ctx->feats) return fail(ctx, PBF_ERR_STATE, "no recorded step: call pbf_set_recording(ctx, 1) and step");
+  const size_t n = ctx->n;
+  if (features && n)
+    CK(cudaMemcpyAsync(features, ctx->feats, n * pbf::kMlpIn * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+  if (labels && n) CK(cudaMemcpyAsync(labels, ctx->lamsumH, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PBF_OK;
+}
+
+int pbf_mlp_train(pbf_ctx* ctx, int adam_steps, int batch, float lr, uint64_t seed, float* loss) {
+  if (!ctx || adam_steps < 0 || batch < 1) return PBF_ERR_ARG;
+  if (!ctx->mlp_ready) return fail(ctx, PBF_ERR_STATE, "no network: call pbf_mlp_init or pbf_mlp_set");
+  if (!ctx->feats || ctx->n == 0) return fail(ctx, PBF_ERR_STATE, "no recorded step to train on");
+  const pbf::MlpDev M = mlp_dev(ctx);
+  const int nb = (batch + pbf::kGradRows - 1) / pbf::kGradRows;
+  for (int it = 0; it < adam_steps; ++it) {
+    CK(cudaMemsetAsync(ctx->mlp_grad, 0, sizeof(float) * pbf::kMlpParams, ctx->stream));
+    CK(cudaMemsetAsync(ctx->mlp_loss, 0, sizeof(float), ctx->stream));
+    pbf::k_mlp_grad<true, true><<<nb, 128, 0, ctx->stream>>>(M, ctx->feats, ctx->lamsumH, (int)ctx->n, batch,
+                                                             seed + 0x632BE59BD9B4E019ull * (uint64_t)it,
+                                                             1.0f / ctx->label_scale, ctx->mlp_grad, ctx->mlp_loss);
+    ctx->adam_t += 1;
+    const float c1 = 1.0f / (1.0f - std::pow(0.9f, (float)ctx->adam_t));
+    const float c2 = 1.0f / (1.0f - std::pow(0.999f, (float)ctx->adam_t));
+    pbf::k_mlp_adam<<<(pbf::kMlpParams + 255) / 256, 256, 0, ctx->stream>>>(ctx->mlp_params, ctx->mlp_grad, ctx->mlp_m,
+                                                                           ctx->mlp_v, pbf::kMlpParams, lr, c1, c2);
+    if (int rc = mlp_refresh(ctx)) return rc;
+  }
+  if (int rc = check_launch(ctx, "mlp_train")) return rc;
+  if (loss) CK(cudaMemcpyAsync(loss, ctx->mlp_loss, sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PBF_OK;
+}
+
+int pbf_mlp_gradients(pbf_ctx* ctx, const float* features, const float* targets, size_t n, float* grad,
+                      float* loss) {
+  if (!ctx || !features || !targets || n == 0) return PBF_ERR_ARG;
+  if (n * (pbf::kMlpIn + 1) > 6 * ctx->capacity)
+    return fail(ctx, PBF_ERR_CAPACITY, "%zu samples exceed the staging area of this context", n);
+  if (!ctx->mlp_ready) return fail(ctx, PBF_ERR_STATE, "no network: call pbf_mlp_init or pbf_mlp_set");
+  float* df = ctx->stage;
+  float* dt = ctx->stage + n * pbf::kMlpIn;
+  CK(cudaMemcpyAsync(df, features, n * pbf::kMlpIn * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(dt, targets, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemsetAsync(ctx->mlp_grad, 0, sizeof(float) * pbf::kMlpParams, ctx->stream));
+  CK(cudaMemsetAsync(ctx->mlp_loss, 0, sizeof(float), ctx->stream));
+  const int nb = (int)((n + pbf::kGradRows - 1) / pbf::kGradRows);
+  pbf::k_mlp_grad<false, false><<<nb, 128, 0, ctx->stream>>>(mlp_dev(ctx), df, dt, (int)n, (int)n, 0, 1.0f,
+                                                             ctx->mlp_grad, ctx->mlp_loss);
+  if (int rc = check_launch(ctx, "mlp_gradients")) return rc;
+  if (grad)
+    CK(cudaMemcpyAsync(grad, ctx->mlp_grad, sizeof(float) * pbf::kMlpParams, cudaMemcpyDeviceToHost, ctx->stream));
+  if (loss) CK(cudaMemcpyAsync(loss, ctx->mlp_loss, sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PBF_OK;
+}
+
+int pbf_mlp_predict(pbf_ctx* ctx, const float* features, size_t n, float* y) {
+  if (!ctx || !features || !y || n == 0) return PBF_ERR_ARG;
+  if (n * (pbf::kMlpIn + 1) > 6 * ctx->capacity)
+    return fail(ctx, PBF_ERR_CAPACITY, "%zu samples exceed the staging area of this context", n);
+  if (!ctx->mlp_ready) return fail(ctx, PBF_ERR_STATE, "no network: call pbf_mlp_init or pbf_mlp_set");
+  float* df = ctx->stage;
+  float* dy = ctx->stage + n * pbf::kMlpIn;
+  CK(cudaMemcpyAsync(df, features, n * pbf::kMlpIn * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  const int warps = (int)((n + 15) / 16);
+  pbf::k_mlp_predict<false><<<(warps + 3) / 4, 128, 0, ctx->stream>>>(mlp_dev(ctx), df, (int)n, dy);
+  if (int rc = check_launch(ctx, "mlp_predict")) return rc;
+  CK(cudaMemcpyAsync(y, dy, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
   return PBF_OK;
 }
 

@@ -70,6 +70,9 @@ void pbf_params_init(pbf_params* p) {
   p->scorr_k = 0.0f;
   p->scorr_n = 4.0f;
   p->scorr_dq = 0.2f;
+  p->solver = 0;
+  p->residual_tol = 0.01f;
+  p->max_iterations = 8;
 }
 
 // parameters.h:123-148

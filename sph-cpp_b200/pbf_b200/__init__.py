@@ -210,6 +210,53 @@ class Particles:
     def set_params(self, p: PbfParams) -> None:
         self._check(self._lib.pbf_set_params(self._ctx, C.byref(p)), "set_params")
 
+    # -- learned warm start (the per-particle MLP) --
+    def mlp_init(self, seed: int = 0) -> None:
+        self._check(self._lib.pbf_mlp_init(self._ctx, int(seed)), "mlp_init")
+
+    def mlp_get(self) -> tuple[np.ndarray, np.ndarray]:
+        params = np.empty(_abi.MLP_PARAMS, np.float32)
+        norm = np.empty(_abi.MLP_NORM, np.float32)
+        self._check(self._lib.pbf_mlp_get(self._ctx, _ptr(params), _ptr(norm)), "mlp_get")
+        return params, norm
+
+    def mlp_set(self, params: np.ndarray, norm: np.ndarray) -> None:
+        params = np.ascontiguousarray(params, np.float32)
+        norm = np.ascontiguousarray(norm, np.float32)
+        assert params.size == _abi.MLP_PARAMS and norm.size == _abi.MLP_NORM
+        self._check(self._lib.pbf_mlp_set(self._ctx, _ptr(params), _ptr(norm)), "mlp_set")
+
+    def set_recording(self, on: bool) -> None:
+        self._check(self._lib.pbf_set_recording(self._ctx, int(on)), "set_recording")
+
+    def training_data(self) -> tuple[np.ndarray, np.ndarray]:
+        n = self.local_count()
+        f = np.empty((n, _abi.MLP_FEATURES), np.float32)
+        lab = np.empty(n, np.float32)
+        self._check(self._lib.pbf_get_training_data(self._ctx, _ptr(f), _ptr(lab)), "get_training_data")
+        return f, lab
+
+    def mlp_train(self, adam_steps: int, batch: int, lr: float, seed: int = 0) -> float:
+        loss = C.c_float()
+        self._check(self._lib.pbf_mlp_train(self._ctx, int(adam_steps), int(batch), float(lr), int(seed),
+                                            C.byref(loss)), "mlp_train")
+        return float(loss.value)
+
+    def mlp_gradients(self, features: np.ndarray, targets: np.ndarray) -> tuple[np.ndarray, float]:
+        f = np.ascontiguousarray(features, np.float32)
+        t = np.ascontiguousarray(targets, np.float32)
+        g = np.empty(_abi.MLP_PARAMS, np.float32)
+        loss = C.c_float()
+        self._check(self._lib.pbf_mlp_gradients(self._ctx, _ptr(f), _ptr(t), t.size, _ptr(g), C.byref(loss)),
+                    "mlp_gradients")
+        return g, float(loss.value)
+
+    def mlp_predict(self, features: np.ndarray) -> np.ndarray:
+        f = np.ascontiguousarray(features, np.float32)
+        y = np.empty(f.shape[0], np.float32)
+        self._check(self._lib.pbf_mlp_predict(self._ctx, _ptr(f), f.shape[0], _ptr(y)), "mlp_predict")
+        return y
+
     # -- instrumentation --
     def set_timing(self, on: bool) -> None:
         self._check(self._lib.pbf_set_timing(self._ctx, int(on)), "set_timing")

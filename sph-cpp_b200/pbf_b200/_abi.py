@@ -27,6 +27,10 @@ ARRAY_SCRATCH = 3
 ARRAY_DENSITIES = 4
 ARRAY_LAMBDAS = 5
 
+MLP_FEATURES = 12
+MLP_PARAMS = 5057
+MLP_NORM = 25
+
 NOALLOC_MAX_PARTICLES = 65536
 NOALLOC_MAX_BINS = 262144
 
@@ -57,7 +61,9 @@ class PbfParams(C.Structure):
         ("scorr_n", C.c_float),
         ("scorr_dq", C.c_float),
         ("exact_math", C.c_int32),
-        ("reserved", C.c_int32 * 3),
+        ("solver", C.c_int32),
+        ("residual_tol", C.c_float),
+        ("max_iterations", C.c_int32),
     ]
 
     def as_dict(self) -> dict:
@@ -78,7 +84,8 @@ class PbfStats(C.Structure):
         ("mean_neighbors", C.c_double),
         ("cap_hits", C.c_uint64),
         ("error_flags", C.c_uint32),
-        ("pad", C.c_uint32),
+        ("solver_iterations", C.c_uint32),
+        ("solver_residual", C.c_double),
     ]
 
     def as_dict(self) -> dict:
@@ -91,6 +98,8 @@ class PbfStats(C.Structure):
             "mean_neighbors": self.mean_neighbors,
             "cap_hits": int(self.cap_hits),
             "error_flags": int(self.error_flags),
+            "solver_iterations": int(self.solver_iterations),
+            "solver_residual": self.solver_residual,
         }
 
 
@@ -145,6 +154,14 @@ SIGNATURES = {
     "pbf_reset_timing": (_i, [_vp]),
     "pbf_launches_per_step": (_i, [_vp, _P(C.c_int64)]),
     "pbf_find_neighbors_noalloc": (_i, [_P(PbfParams), _vp, _sz, _vp, _vp, _vp]),
+    "pbf_mlp_init": (_i, [_vp, C.c_uint64]),
+    "pbf_mlp_get": (_i, [_vp, _vp, _vp]),
+    "pbf_mlp_set": (_i, [_vp, _vp, _vp]),
+    "pbf_set_recording": (_i, [_vp, _i]),
+    "pbf_get_training_data": (_i, [_vp, _vp, _vp]),
+    "pbf_mlp_train": (_i, [_vp, _i, _i, C.c_float, C.c_uint64, _P(C.c_float)]),
+    "pbf_mlp_gradients": (_i, [_vp, _vp, _vp, _sz, _vp, _P(C.c_float)]),
+    "pbf_mlp_predict": (_i, [_vp, _vp, _sz, _vp]),
 }
 
 _lib = None

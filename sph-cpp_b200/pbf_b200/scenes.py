@@ -45,6 +45,9 @@ class Scene:
     mover_center: tuple[float, float, float] = (-1.5, -2.0, -1.5)
     scorr: tuple[float, float, float] = (0.0, 4.0, 0.2)  # (k, n, dq/h); k = 0 is the reference's Δp
     exact_math: int = 0
+    solver: int = 0                        # 0 plain K iterations, 1 learned warm start
+    residual_tol: float = 0.01             # learned solver: mean clamped density error target
+    max_iterations: int = 8                # learned solver: iterations per step at most
 
     @property
     def n(self) -> int:
@@ -79,6 +82,9 @@ class Scene:
             p.mover_center[a] = self.mover_center[a]
         p.scorr_k, p.scorr_n, p.scorr_dq = self.scorr
         p.exact_math = self.exact_math
+        p.solver = self.solver
+        p.residual_tol = self.residual_tol
+        p.max_iterations = self.max_iterations
         rc = lib.pbf_params_derive(C.byref(p), self.spacing, -1.0)
         if rc:
             raise RuntimeError(f"pbf_params_derive failed ({rc})")

@@ -1,0 +1,128 @@
+"""Learned warm start on the GPU: the tensor-core network against the float64
+oracle (forward and gradients), training on the plain solver's own lambdas,
+what the trained network gains over the plain first iteration, and the
+residual-controlled iteration loop."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import mlp_oracle as MO
+from pbf_b200 import Particles, _abi
+from pbf_b200.learn import held_out_loss, normalization, run_solver, train, warm_start_scene
+
+pytestmark = pytest.mark.gpu
+
+# BF16 operands (8-bit mantissa), FP32 accumulation, two hidden layers.
+Y_TOL = 0.03        # forward: max |y_gpu - y_oracle| relative to max |y|
+GRAD_COS = 0.995    # gradient direction
+GRAD_REL = 0.05     # gradient norm-wise relative error
+
+
+def _ctx_with_net(seed=5):
+    sc = warm_start_scene("dam_2k")
+    g = Particles(sc.params(), 8192)  # staging room for 8192 * 6 / 13 host samples
+    g.mlp_init(seed)
+    return g
+
+
+def test_forward_matches_float64_oracle():
+    g = _ctx_with_net()
+    params, norm = g.mlp_get()
+    rng = np.random.default_rng(0)
+    x = rng.normal(0, 1, (1000, _abi.MLP_FEATURES)).astype(np.float32)
+    y = g.mlp_predict(x)
+    ref, _ = MO.forward(params.astype(np.float64), x.astype(np.float64))
+    assert np.abs(y - ref).max() <= Y_TOL * max(np.abs(ref).max(), 0.1)
+
+
+def test_gradients_match_float64_oracle():
+    g = _ctx_with_net(9)
+    params, _ = g.mlp_get()
+    rng = np.random.default_rng(1)
+    x = rng.normal(0, 1, (1024, _abi.MLP_FEATURES)).astype(np.float32)
+    t = rng.normal(0, 1, 1024).astype(np.float32)
+    grad, loss = g.mlp_gradients(x, t)
+    ref_loss, ref = MO.loss_and_grad(params.astype(np.float64), x, t)
+    assert loss == pytest.approx(ref_loss, rel=0.02)
+    cos = float(grad @ ref / (np.linalg.norm(grad) * np.linalg.norm(ref)))
+    assert cos >= GRAD_COS, cos
+    assert np.linalg.norm(grad - ref) <= GRAD_REL * np.linalg.norm(ref)
+    # every parameter block gets its gradient (layer 1 weights, biases, layer 3)
+    for a, b in ((MO.OFF_W1, MO.OFF_B1), (MO.OFF_B1, MO.OFF_W2), (MO.OFF_W2, MO.OFF_B2), (MO.OFF_W3, MO.OFF_B3)):
+        blk, rb = grad[a:b], ref[a:b]
+        assert np.linalg.norm(blk - rb) <= 0.1 * np.linalg.norm(rb) + 1e-7
+
+
+@pytest.fixture(scope="module")
+def trained_8k():
+    sc = warm_start_scene("dam_8k")
+    params, norm, hist = train(sc, seeds=(11, 12, 13, 14), steps=120, adam_per_step=4, batch=8192, lr=1e-3)
+    return sc, params, norm, hist
+
+
+def test_recorded_training_data_are_the_plain_solver_lambdas():
+    sc = warm_start_scene("dam_2k")
+    p = sc.params()
+    g = Particles(p, sc.n)
+    g.set_recording(True)
+    g.upload(sc.positions())
+    g.step(5)
+    f, lab = g.training_data()
+    assert np.isfinite(f).all() and np.isfinite(lab).all()
+    assert (lab <= 0).all() and (lab < 0).any()           # lambdas are never positive
+    assert np.allclose(f[:, 0] * 64, np.round(f[:, 0] * 64))     # neighbour counts
+    assert (f[:, 1] >= 0).all() and np.allclose(np.maximum(f[:, 2], 0), f[:, 1], atol=1e-6)
+    # the plain first-iteration lambda feature, -C/(S+eps)
+    assert np.allclose(f[:, 4], -f[:, 1] / (f[:, 3] + p.lambda_epsilon), rtol=1e-5, atol=1e-12)
+    norm = normalization(f, lab)
+    assert norm.shape == (_abi.MLP_NORM,) and np.isfinite(norm).all()
+
+
+def test_training_reduces_held_out_loss(trained_8k):
+    """Trained on the plain solver's lambdas, the network predicts them on a
+    trajectory it has not seen far better than it did untrained."""
+    sc, params, norm, hist = trained_8k
+    assert np.isfinite(hist[:, 2]).all()
+    g = _ctx_with_net(7)  # the same initial network as train(init_seed=7)
+    init_params, _ = g.mlp_get()
+    before = held_out_loss(sc, init_params, norm, seed=97)
+    after = held_out_loss(sc, params, norm, seed=97)
+    assert after < 0.5 * before, (before, after)
+
+
+def test_trained_warm_start_beats_plain_at_equal_iterations(trained_8k):
+    """What the network gains: with two Jacobi iterations per step, the first
+    seeded by the network's lambda, the density error is lower than with two
+    plain iterations (held-out seed; the residual check never stops early)."""
+    sc, params, norm, _ = trained_8k
+    held = sc.with_(seed=99)
+    plain2 = run_solver(held.with_(solve_steps=2), 60, warmup=20)
+    learned2 = run_solver(held.with_(solver=1, max_iterations=2, residual_tol=0.0), 60, params, norm, warmup=20)
+    assert (learned2["iterations"] == 2).all()
+    assert learned2["residual"].mean() < plain2["residual"].mean(), (learned2["residual"].mean(),
+                                                                     plain2["residual"].mean())
+
+
+def test_residual_controlled_iterations(trained_8k):
+    sc, params, norm, _ = trained_8k
+    held = sc.with_(seed=98)
+    never = run_solver(held.with_(solver=1, max_iterations=5, residual_tol=1e9), 10, params, norm)
+    assert (never["iterations"] == 1).all()
+    always = run_solver(held.with_(solver=1, max_iterations=5, residual_tol=0.0), 10, params, norm)
+    assert (always["iterations"] == 5).all()
+    plain3 = run_solver(held.with_(solve_steps=3), 40, warmup=20)
+    tol = float(plain3["residual"].mean())
+    from pbf_b200 import Particles as P
+    p = held.with_(solver=1, max_iterations=6, residual_tol=tol).params()
+    with P(p, held.n) as g:
+        g.mlp_set(params, norm)
+        g.upload(held.positions())
+        g.step(20)
+        for _ in range(40):
+            g.step(1)
+            st = g.stats()
+            assert st["error_flags"] == 0
+            if st["solver_iterations"] < 6:
+                assert st["solver_residual"] <= tol
+                assert st["mean_density_error"] <= tol * 1.02 + 1e-6

@@ -1,0 +1,28 @@
+"""The float64 network oracle (oracle/mlp_oracle.py) checked against central
+finite differences: its analytic gradient is what the GPU's tensor-core
+backward pass is compared with."""
+import numpy as np
+
+from oracle import mlp_oracle as M
+
+
+def test_oracle_gradient_matches_finite_differences():
+    rng = np.random.default_rng(3)
+    p = rng.normal(0, 0.3, M.N_PARAMS)
+    x = rng.normal(0, 1, (17, M.N_IN))
+    t = rng.normal(0, 1, 17)
+    loss, g = M.loss_and_grad(p, x, t)
+    idx = rng.choice(M.N_PARAMS, 60, replace=False)
+    idx = np.concatenate([idx, [M.OFF_B3, M.OFF_W1, M.OFF_B1, M.OFF_W2 + 5, M.OFF_W3]])
+    for i in idx:
+        e = np.zeros(M.N_PARAMS)
+        e[i] = 1e-6
+        fd = (M.loss_and_grad(p + e, x, t)[0] - M.loss_and_grad(p - e, x, t)[0]) / 2e-6
+        assert abs(fd - g[i]) <= 1e-6 + 1e-5 * abs(g[i]), (i, fd, g[i])
+
+
+def test_oracle_gelu_is_the_erf_form():
+    xs = np.array([-3.0, -1.0, 0.0, 0.5, 2.0])
+    from math import erf, sqrt
+    ref = np.array([0.5 * x * (1 + erf(x / sqrt(2))) for x in xs])
+    assert np.allclose(M.gelu(xs), ref, rtol=0, atol=1e-15)
