@@ -52,6 +52,7 @@ def parse_args():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--exact", action="store_true", help="exact_math=1 (bit-exact arithmetic)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the plain-vs-learned comparison")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU baseline sample")
     return ap.parse_args()
 
@@ -126,7 +127,10 @@ def kernel_bytes(name: str, n: int, nbar: float, K: int, nbins: int) -> float:
         "scan_partials": 0.0,
         "scan_apply": 8.0 * nbins / n,
         "scatter": 4 + 4 + 4 + 8,                               # key, rank, orig in; pair out
-        "cell_sort": 8.0 + 4.0 * nbins / n,                     # pairs in place (read) + bin starts
+        "rank_in_bin": 8 + 4 + 8 + 8,                           # pair, its key, bin bounds in; pair out
+        "density_lambda_learned": 16 + L + 16 + 4 + 4 + 16 + 4 + 4,  # + v (features), last lambda in, lambda sum out
+        "residual_check": 16 + L + 16 + 4 + 4,                  # as density_lambda
+        "decide": 0.0,
         "reorder": 8 + 4 + 3 * 16 + 3 * 16 + 4 + 4,             # pair, key, (x, x*, v) in and out, orig, key
         "fill_neighbors": 16 + 4 * nbar + 4 + 8.0 * nbins / n,  # own x*, list + count out, bin starts
         "density_lambda": 16 + L + 16 + 4 + 4,                  # x* in; list; (x*, lambda), rho, lambda out
@@ -191,6 +195,73 @@ def run_reference_cpu(scene, steps: int, warmup: int, budget_s: float | None) ->
             "sample": f"{scene.name}: {scene.n} particles, {steps} timed full steps after {max(warmup, 0)} warm-up "
                       f"step(s), std::chrono/perf_counter wall time, {dt:.2f} s",
             "steps": steps, "seconds": dt}
+
+
+# ---------------------------------------------------------------- plain vs learned
+def solver_run(scene, steps: int, warmup: int, params=None, norm=None) -> dict:
+    """Throughput of `steps` graph-replayed steps after `warmup`, then the same
+    run replayed (the fast path is deterministic) with the per-step mean clamped
+    density error and iteration count read after every step."""
+    import torch
+    from pbf_b200 import Particles
+    p = scene.params()
+    out = {}
+    with Particles(p, scene.n) as g:
+        if scene.solver == 1:
+            g.mlp_set(params, norm)
+        stream = torch.cuda.ExternalStream(g.stream_handle())
+        x0 = scene.positions()
+        g.upload(x0)
+        for _ in range(warmup):
+            g.step(1)
+        g.sync()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            g.step(1)
+        e1.record(stream)
+        e1.synchronize()
+        t = e0.elapsed_time(e1) / 1e3
+        g.upload(x0)
+        for _ in range(warmup):
+            g.step(1)
+        err, its = [], []
+        for _ in range(steps):
+            g.step(1)
+            st = g.stats()
+            err.append(st["mean_density_error"])
+            its.append(st["solver_iterations"])
+    import numpy as np
+    return {"value": scene.n * steps / t, "ms_per_step": 1e3 * t / steps,
+            "mean_density_error": float(np.mean(err)), "max_step_density_error": float(np.max(err)),
+            "mean_iterations": float(np.mean(its))}
+
+
+def learned_comparison(scene_name: str, steps: int, warmup: int, target: float = 0.01) -> dict:
+    """Plain PBF against the learned warm start at equal mean density error
+    <= target (1% of rest density): plain runs with the smallest K in 3..6
+    that keeps its mean error over the window at or below the target; the
+    learned solver iterates per step until its error is at or below it."""
+    from pbf_b200.learn import DEFAULT_MODEL, load_model, warm_start_scene
+    if not DEFAULT_MODEL.exists():
+        return {"unavailable": f"no trained network at {DEFAULT_MODEL.relative_to(ROOT)}"}
+    params, norm, meta = load_model(DEFAULT_MODEL)
+    base = warm_start_scene(scene_name, seed=4242)  # a jitter seed the network was not trained on
+    tried = {}
+    plain, K = None, None
+    for k in (3, 4, 5, 6):
+        plain = solver_run(base.with_(solve_steps=k), steps, warmup)
+        tried[k] = plain["mean_density_error"]
+        K = k
+        if plain["mean_density_error"] <= target:
+            break
+    learned = solver_run(base.with_(solver=1, residual_tol=target, max_iterations=K), steps, warmup, params, norm)
+    return {"workload": f"{base.name}, relaxation epsilon {base.lambda_epsilon}, steps {warmup}..{warmup + steps}",
+            "target_mean_density_error": target, "plain_errors_by_K": tried,
+            "plain": dict(plain, iterations=K), "learned": dict(learned, residual_tol=target, max_iterations=K),
+            "speedup": learned["value"] / plain["value"],
+            "network": {k: meta.get(k) for k in ("trajectories", "steps", "batch", "lr", "final_loss")}}
 
 
 # ---------------------------------------------------------------- main
@@ -315,6 +386,13 @@ def main():
     ok = bool(np.isfinite(xh).all())
     launches = g.launches_per_step() * K
 
+    learned = None
+    if rank == 0 and world == 1 and not args.no_learned:
+        try:
+            learned = learned_comparison(args.scene, max(K, 20), 100)
+        except Exception as e:  # reported, never fatal for the GPU line
+            learned = {"error": str(e)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -350,6 +428,7 @@ def main():
                         "mean_density_error": st["mean_density_error"], "error_flags": st["error_flags"],
                         "finite": ok},
             "clocks": clk.summary(),
+            "learned_vs_plain": learned,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
