@@ -128,7 +128,8 @@ def kernel_bytes(name: str, n: int, nbar: float, K: int, nbins: int) -> float:
         "scan_apply": 8.0 * nbins / n,
         "scatter": 4 + 4 + 4 + 8,                               # key, rank, orig in; pair out
         "rank_in_bin": 8 + 4 + 8 + 8,                           # pair, its key, bin bounds in; pair out
-        "density_lambda_learned": 16 + L + 16 + 4 + 4 + 16 + 4 + 4,  # + v (features), last lambda in, lambda sum out
+        "warm_features": 16 + L + 16 + 16 + 4 + 16 + 32,       # x*, list, v, last lambda in; (x*, l1), v, bf16 features out
+        "warm_mlp": 32 + 16 + 16 + 4 + 4,                       # features, (x*, l1) in; (x*, lambda), lambda, sum out
         "residual_check": 16 + L + 16 + 4 + 4,                  # as density_lambda
         "decide": 0.0,
         "reorder": 8 + 4 + 3 * 16 + 3 * 16 + 4 + 4,             # pair, key, (x, x*, v) in and out, orig, key
@@ -232,15 +233,26 @@ def solver_run(scene, steps: int, warmup: int, params=None, norm=None) -> dict:
             st = g.stats()
             err.append(st["mean_density_error"])
             its.append(st["solver_iterations"])
+        # per-kernel device time over the same window (eager launches with events)
+        g.upload(x0)
+        for _ in range(warmup):
+            g.step(1)
+        g.set_timing(True)
+        g.reset_timing()
+        g.step(steps)
+        kt = g.kernel_times()
+        g.set_timing(False)
     import numpy as np
     return {"value": scene.n * steps / t, "ms_per_step": 1e3 * t / steps,
             "mean_density_error": float(np.mean(err)), "max_step_density_error": float(np.max(err)),
-            "mean_iterations": float(np.mean(its))}
+            "mean_iterations": float(np.mean(its)),
+            "kernel_ms_per_step": {k: round(v["total_ms"] / steps, 4) for k, v in
+                                   sorted(kt.items(), key=lambda kv: -kv[1]["total_ms"])}}
 
 
 def learned_comparison(scene_name: str, steps: int, warmup: int, target: float = 0.01) -> dict:
     """Plain PBF against the learned warm start at equal mean density error
-    <= target (1% of rest density): plain runs with the smallest K in 3..6
+    <= target (1% of rest density): plain runs with the smallest K in 3..12
     that keeps its mean error over the window at or below the target; the
     learned solver iterates per step until its error is at or below it."""
     from pbf_b200.learn import DEFAULT_MODEL, load_model, warm_start_scene
@@ -250,7 +262,7 @@ def learned_comparison(scene_name: str, steps: int, warmup: int, target: float =
     base = warm_start_scene(scene_name, seed=4242)  # a jitter seed the network was not trained on
     tried = {}
     plain, K = None, None
-    for k in (3, 4, 5, 6):
+    for k in range(3, 13):
         plain = solver_run(base.with_(solve_steps=k), steps, warmup)
         tried[k] = plain["mean_density_error"]
         K = k

@@ -24,6 +24,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstdarg>
@@ -522,7 +523,8 @@ __global__ void __launch_bounds__(kBlock) k_density_lambda(Dev P, int n, size_t 
 // Modes: kDlPlain; kDlRecord also writes the learned warm start's features
 // (first iteration) and sums the applied lambdas into the label; kDlCheck is
 // the learned solver's residual check: skipped once the step has converged,
-// else it adds every particle's clamped density error to io.err_sum.
+// else each block writes the sum of its particles' clamped density errors
+// to io.partials[blockIdx.x].
 enum { kDlPlain = 0, kDlRecord = 1, kDlCheck = 2 };
 
 struct LearnIO {
@@ -530,17 +532,16 @@ struct LearnIO {
   float* lamsum;          // lambda applied this step (label / next step's feature)
   const float* lamprev;   // lambda applied last step, in this step's order
   pbf::SolveState* state; // kDlCheck
+  double* partials;       // kDlCheck: one sum per block of the (persistent) grid
   int first;              // first Jacobi iteration of the step
 };
 
 template <int MODE>
-__global__ void __launch_bounds__(kBlock) kf_density_lambda(Dev P, Fast F, int n, size_t stride,
-                                                            const int32_t* __restrict__ nbr,
-                                                            const int32_t* __restrict__ cnt,
-                                                            const float4* __restrict__ pst, float4* xl, float4* vel,
-                                                            float* lam, uint32_t* nudge, LearnIO io) {
-  if (MODE == kDlCheck && io.state->done) return;
-  const pbf::Group G = pbf::group_of(n);
+__device__ __forceinline__ void density_lambda_tile(int tile, const Dev& P, const Fast& F, int n, size_t stride,
+                                                    const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
+                                                    const float4* __restrict__ pst, float4* xl, float4* vel,
+                                                    float* lam, uint32_t* nudge, const LearnIO& io, float& err) {
+  const pbf::Group G = pbf::group_at(n, tile);
   const int b = G.b;
   const float4 xp = pst[b];
   const int c = G.live ? cnt[b] : 0;
@@ -566,12 +567,7 @@ __global__ void __launch_bounds__(kBlock) kf_density_lambda(Dev P, Fast F, int n
   if (MODE == kDlRecord) nh = pbf::gsum(nh);
   close = pbf::gor(close);
   const float rho = fmaf(F.m_poly, sw, F.m_w0);
-  if (MODE == kDlCheck) {
-    float e = (G.live && G.lane == 0) ? fmaxf(fmaf(rho, F.inv_rho0, -1.0f), 0.0f) : 0.0f;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
-    if ((threadIdx.x & 31) == 0 && e > 0.0f) atomicAdd(&io.state->err_sum, (double)e);
-  }
+  if (MODE == kDlCheck && G.live && G.lane == 0) err += fmaxf(fmaf(rho, F.inv_rho0, -1.0f), 0.0f);
   if (!G.live || G.lane != 0) return;
   const float g2 = sgx * sgx + sgy * sgy + sgz * sgz;
   if (close) {  // a neighbour (almost) on top: the reference-ordered path decides the nudge
@@ -596,26 +592,43 @@ __global__ void __launch_bounds__(kBlock) kf_density_lambda(Dev P, Fast F, int n
   }
 }
 
-// Learned warm start, first Jacobi iteration: the gather of kf_density_lambda,
-// the particle's 12 features, then the MLP on the tensor cores for the
-// block's 32 particles (two warps, 16 rows each).  A single over-relaxed
-// iteration on its own overshoots and the overshoot feeds the velocity update
-// (measured on the oracle: 1 iteration at 2.5x lambda ends near 4% density
-// error where 1 plain iteration ends near 1.5%), so the residual-checked plain
-// iterations that follow are part of the method.
-constexpr float kWarmMaxGain = 3.0f;
-__global__ void __launch_bounds__(kBlock) kl_density_lambda(Dev P, Fast F, pbf::MlpDev M, int n, size_t stride,
+// The residual check runs on a persistent grid walking the tiles, so that
+// once the step has converged the launch costs a few hundred empty blocks.
+template <int MODE>
+__global__ void __launch_bounds__(kBlock) kf_density_lambda(Dev P, Fast F, int n, size_t stride,
                                                             const int32_t* __restrict__ nbr,
                                                             const int32_t* __restrict__ cnt,
                                                             const float4* __restrict__ pst, float4* xl, float4* vel,
-                                                            float* lam, uint32_t* nudge, float* lamsum,
-                                                            const float* __restrict__ lamprev) {
-  constexpr int kP = kBlock / pbf::kGL;  // particles per block
-  __shared__ __align__(16) __nv_bfloat16 sf[kP * pbf::kMlpInPad];
-  __shared__ float sy[kP];
-  __shared__ int sclose[kP];
+                                                            float* lam, uint32_t* nudge, LearnIO io) {
+  if (MODE == kDlCheck && io.state->done) return;
+  const int tiles = (int)(((size_t)n * pbf::kGL + kBlock - 1) / kBlock);
+  float err = 0.0f;
+  for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x)
+    density_lambda_tile<MODE>(tile, P, F, n, stride, nbr, cnt, pst, xl, vel, lam, nudge, io, err);
+  if (MODE == kDlCheck) pbf::block_partial<kBlock>(err, io.partials + blockIdx.x);
+}
+
+// Learned warm start, first Jacobi iteration, in two launches:
+// kl_features: the gather of kf_density_lambda, then per particle the 12
+// normalised features as a BF16 row of 16 (columns 12..15 are padding the
+// network's first layer multiplies by zero; column 15 flags a particle the
+// reference-ordered nudge path handled), and the plain first-iteration
+// lambda l1 in xl.w.
+// kl_mlp: the network on the tensor cores, one warp per 16 particles, every
+// warp busy; lambda = the output kept between l1 and kWarmMaxGain * l1.
+// A single over-relaxed iteration on its own overshoots and the overshoot
+// feeds the velocity update (measured on the oracle: 1 iteration at 2.5x
+// lambda ends near 4% density error where 1 plain iteration ends near 1.5%),
+// so the residual-checked plain iterations that follow are part of the method.
+constexpr float kWarmMaxGain = 3.0f;
+
+__global__ void __launch_bounds__(kBlock) kl_features(Dev P, Fast F, pbf::MlpDev M, int n, size_t stride,
+                                                      const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
+                                                      const float4* __restrict__ pst, float4* xl, float4* vel,
+                                                      float* lam, uint32_t* nudge, const float* __restrict__ lamprev,
+                                                      __nv_bfloat16* featb) {
   const pbf::Group G = pbf::group_of(n);
-  const int b = G.b, p = threadIdx.x / pbf::kGL;
+  const int b = G.b;
   const float4 xp = pst[b];
   const int c = G.live ? cnt[b] : 0;
   float sw = 0.f, sgx = 0.f, sgy = 0.f, sgz = 0.f, sc = 0.f, nh = 0.f;
@@ -639,46 +652,58 @@ __global__ void __launch_bounds__(kBlock) kl_density_lambda(Dev P, Fast F, pbf::
   sc = pbf::gsum(sc);
   nh = pbf::gsum(nh);
   close = pbf::gor(close);
+  if (!G.live || G.lane != 0) return;
   const float rho = fmaf(F.m_poly, sw, F.m_w0);
   const float g2 = sgx * sgx + sgy * sgy + sgz * sgz;
-  if (G.lane == 0) {
-    float f[pbf::kMlpIn];
-    pbf::raw_features(P, F, f, c, rho, sc, g2, (int)nh, G.live ? lamprev[b] : 0.0f, vel[b], xp);
+  const float4 v = vel[b];
+  float f[pbf::kMlpIn];
+  pbf::raw_features(P, F, f, c, rho, sc, g2, (int)nh, lamprev[b], v, xp);
+  uint32_t row[pbf::kMlpInPad / 2];
 #pragma unroll
-    for (int k = 0; k < pbf::kMlpInPad; ++k)
-      sf[p * pbf::kMlpInPad + k] =
-          __float2bfloat16_rn(k < pbf::kMlpIn && G.live ? (f[k] - M.feat_mean[k]) * M.feat_inv_std[k] : 0.0f);
-    sclose[p] = G.live && close;
-  }
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (warp < kP / 16) {
-    uint32_t a[4];
-    pbf::load_a_rows16(a, sf + warp * 16 * pbf::kMlpInPad, lane);
-    float y_lo, y_hi;
-    pbf::mlp_forward16(M, a, lane, y_lo, y_hi);
-    if ((lane & 3) == 0) {
-      sy[warp * 16 + (lane >> 2)] = y_lo;
-      sy[warp * 16 + (lane >> 2) + 8] = y_hi;
-    }
-  }
-  __syncthreads();
-  if (!G.live || G.lane != 0) return;
-  if (sclose[p]) {
+  for (int k = 0; k < pbf::kMlpIn; k += 2)
+    row[k / 2] = pbf::pack_bf16x2((f[k] - M.feat_mean[k]) * M.feat_inv_std[k],
+                                  (f[k + 1] - M.feat_mean[k + 1]) * M.feat_inv_std[k + 1]);
+  row[6] = 0u;
+  row[7] = pbf::pack_bf16x2(0.0f, close ? 1.0f : 0.0f);
+  uint4* dst = reinterpret_cast<uint4*>(featb + (size_t)b * pbf::kMlpInPad);
+  dst[0] = make_uint4(row[0], row[1], row[2], row[3]);
+  dst[1] = make_uint4(row[4], row[5], row[6], row[7]);
+  if (close) {
     density_lambda_one<false>(P, b, stride, nbr, cnt, pst, xl, vel, lam, nudge);
-    lamsum[b] = lam[b];
     return;
   }
-  // The network's lambda, kept between the plain first-iteration lambda l1
-  // and kWarmMaxGain * l1 (both <= 0): zero where the constraint is inactive,
-  // as in the plain solver, and an over-relaxation of at most kWarmMaxGain.
   const float C = fmaxf(fmaf(rho, F.inv_rho0, -1.0f), 0.0f);
   const float l1 = -C / (sc + g2 + F.lambda_eps);
-  const float l = fminf(fmaxf(sy[p] * M.label_scale, kWarmMaxGain * l1), l1);
-  xl[b] = make_float4(xp.x, xp.y, xp.z, l);
-  vel[b].w = rho;
-  lam[b] = l;
-  lamsum[b] = l;
+  xl[b] = make_float4(xp.x, xp.y, xp.z, l1);
+  vel[b] = make_float4(v.x, v.y, v.z, rho);
+  lam[b] = l1;
+}
+
+__global__ void __launch_bounds__(128) kl_mlp(pbf::MlpDev M, int n, const __nv_bfloat16* __restrict__ featb,
+                                              float4* xl, float* lam, float* lamsum) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const int r0 = warp * 16;
+  if (r0 >= n) return;  // whole warp
+  const int ra = min(r0 + g, n - 1), rb = min(r0 + g + 8, n - 1);
+  const uint32_t* fa = reinterpret_cast<const uint32_t*>(featb + (size_t)ra * pbf::kMlpInPad);
+  const uint32_t* fb = reinterpret_cast<const uint32_t*>(featb + (size_t)rb * pbf::kMlpInPad);
+  uint32_t a[4] = {__ldg(fa + t), __ldg(fb + t), __ldg(fa + t + 4), __ldg(fb + t + 4)};
+  float y_lo, y_hi;
+  pbf::mlp_forward16(M, a, lane, y_lo, y_hi);
+  if (t != 0) return;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int r = r0 + g + 8 * h;
+    if (r >= n) break;
+    const uint32_t flag = __ldg(reinterpret_cast<const uint32_t*>(featb + (size_t)r * pbf::kMlpInPad) + 7);
+    const float4 x = xl[r];
+    float l = x.w;  // l1, or the nudge path's lambda
+    if ((flag >> 16) == 0u) l = fminf(fmaxf((h ? y_hi : y_lo) * M.label_scale, kWarmMaxGain * x.w), x.w);
+    xl[r] = make_float4(x.x, x.y, x.z, l);
+    lam[r] = l;
+    lamsum[r] = l;
+  }
 }
 
 // Lambda recomputed from the (nudged) positions in xl, only when the
@@ -971,14 +996,12 @@ __global__ void __launch_bounds__(kBlock) k_apply_vorticity(Dev P, int n, size_t
 // ---- fast gathers (exact_math = 0), kGL lanes per particle, see pbf_fast.cuh ----
 // COND: the learned solver's extra iterations, skipped once the step has
 // converged; lamsum (when given) accumulates the applied lambda.
-template <bool SCORR, bool LAST, bool COND>
-__global__ void __launch_bounds__(kBlock) kf_dp_update(Dev P, Fast F, int n, size_t stride,
-                                                       const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
-                                                       const float4* __restrict__ xl, float4* pst,
-                                                       const float4* __restrict__ pos, float4* vel,
-                                                       const pbf::SolveState* __restrict__ state, float* lamsum) {
-  if (COND && state->done) return;
-  const pbf::Group G = pbf::group_of(n);
+template <bool SCORR, bool LAST>
+__device__ __forceinline__ void dp_update_tile(int tile, const Dev& P, const Fast& F, int n, size_t stride,
+                                               const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
+                                               const float4* __restrict__ xl, float4* pst,
+                                               const float4* __restrict__ pos, float4* vel, float* lamsum) {
+  const pbf::Group G = pbf::group_at(n, tile);
   const int b = G.b;
   const float4 xp = xl[b];
   const int c = G.live ? cnt[b] : 0;
@@ -1007,6 +1030,20 @@ __global__ void __launch_bounds__(kBlock) kf_dp_update(Dev P, Fast F, int n, siz
     const float3 v = velocity_of(P, ns, pos[b]);
     vel[b] = make_float4(v.x, v.y, v.z, vel[b].w);
   }
+}
+
+// COND launches (the learned solver's extra iterations) use a persistent grid
+// and skip the whole launch once the step has converged.
+template <bool SCORR, bool LAST, bool COND>
+__global__ void __launch_bounds__(kBlock) kf_dp_update(Dev P, Fast F, int n, size_t stride,
+                                                       const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
+                                                       const float4* __restrict__ xl, float4* pst,
+                                                       const float4* __restrict__ pos, float4* vel,
+                                                       const pbf::SolveState* __restrict__ state, float* lamsum) {
+  if (COND && state->done) return;
+  const int tiles = (int)(((size_t)n * pbf::kGL + kBlock - 1) / kBlock);
+  for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x)
+    dp_update_tile<SCORR, LAST>(tile, P, F, n, stride, nbr, cnt, xl, pst, pos, vel, lamsum);
 }
 
 template <bool FINAL>
@@ -1187,7 +1224,9 @@ struct pbf_ctx {
 
   // learned warm start
   float *lamsumH = nullptr, *lamprevS = nullptr, *feats = nullptr;
+  __nv_bfloat16* featb = nullptr;  // [C][16] normalised features of the warm iteration
   pbf::SolveState* state = nullptr;
+  double* partials = nullptr;  // [persistent_blocks] residual check sums
   bool recording = false;
   float *mlp_params = nullptr, *mlp_grad = nullptr, *mlp_m = nullptr, *mlp_v = nullptr, *mlp_norm = nullptr;
   float* mlp_loss = nullptr;
@@ -1195,6 +1234,7 @@ struct pbf_ctx {
   float label_scale = 1.0f;
   int adam_t = 0;
   bool mlp_ready = false;
+  int persistent_blocks = 148 * 4;  // SMs x resident check blocks, set at creation
 
   std::map<int, cudaGraphExec_t> graphs;
   std::vector<void*> allocations;
@@ -1465,14 +1505,21 @@ void launch_learned_solve(pbf_ctx* ctx) {
   const Fast& F = ctx->fast;
   cudaStream_t s = ctx->stream;
   const int g = blocks_for(n), gg = blocks_for((size_t)n * pbf::kGL);
+  const int gp = std::min(gg, ctx->persistent_blocks);  // skippable launches: persistent grid
   const float tol = ctx->params.residual_tol;
   const int iters = ctx->params.max_iterations > 0 ? ctx->params.max_iterations : 1;
   cudaMemsetAsync(ctx->state, 0, sizeof(pbf::SolveState), s);
-  LearnIO io{nullptr, nullptr, nullptr, ctx->state, 0};
+  LearnIO io{nullptr, nullptr, nullptr, ctx->state, ctx->partials, 0};
+  const pbf::MlpDev M = mlp_dev(ctx);
   {
-    Launch L(ctx, "density_lambda_learned");
-    kl_density_lambda<<<gg, kBlock, 0, s>>>(P, F, mlp_dev(ctx), n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl,
-                                            ctx->velS, ctx->lamH, ctx->nudge, ctx->lamsumH, ctx->lamprevS);
+    Launch L(ctx, "warm_features");
+    kl_features<<<gg, kBlock, 0, s>>>(P, F, M, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl, ctx->velS, ctx->lamH,
+                                      ctx->nudge, ctx->lamprevS, ctx->featb);
+  }
+  {
+    Launch L(ctx, "warm_mlp");
+    const int warps = (n + 15) / 16;
+    kl_mlp<<<(warps + 3) / 4, 128, 0, s>>>(M, n, ctx->featb, ctx->xl, ctx->lamH, ctx->lamsumH);
   }
   {
     Launch L(ctx, "dp_update");
@@ -1483,16 +1530,16 @@ void launch_learned_solve(pbf_ctx* ctx) {
     const bool final_check = r == iters;
     {
       Launch L(ctx, "residual_check");
-      kf_density_lambda<kDlCheck><<<gg, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl,
+      kf_density_lambda<kDlCheck><<<gp, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl,
                                                         ctx->velS, ctx->lamH, ctx->nudge, io);
     }
     {
       Launch L(ctx, "decide");
-      pbf::k_decide<<<1, 1, 0, s>>>(n, tol, final_check ? 1 : 0, ctx->state);
+      pbf::k_decide<<<1, pbf::kDecideThreads, 0, s>>>(n, tol, final_check ? 1 : 0, ctx->partials, gp, ctx->state);
     }
     if (final_check) break;
     Launch L(ctx, "dp_update");
-    kf_dp_update<SCORR, false, true><<<gg, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS,
+    kf_dp_update<SCORR, false, true><<<gp, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS,
                                                           ctx->posS, ctx->velS, ctx->state, ctx->lamsumH);
   }
   Launch L(ctx, "update_velocities");
@@ -1527,7 +1574,7 @@ void launch_step_t(pbf_ctx* ctx) {
   if (!X && ctx->params.solver == 1) {
     launch_learned_solve<SCORR>(ctx);
   } else {
-  LearnIO io{ctx->feats, ctx->lamsumH, ctx->lamprevS, ctx->state, 0};
+  LearnIO io{ctx->feats, ctx->lamsumH, ctx->lamprevS, ctx->state, nullptr, 0};
   for (int it = 0; it < K; ++it) {
     io.first = it == 0;
     if (X) cudaMemsetAsync(ctx->nudge, 0, sizeof(uint32_t), s);
@@ -1634,9 +1681,10 @@ int launches_per_step(const pbf_ctx* ctx) {
   const int K = ctx->params.solve_steps;
   const int tail = (ctx->params.gamma != 0.0f ? 2 : 0) + 4;
   if (ctx->params.solver == 1 && !ctx->params.exact_math) {
-    // learned: warm iteration (2) + (iters-1) x (check, decide, delta-p) + final check, decide + velocity
+    // learned: warm iteration (features, network, delta-p) + (iters-1) x (check, decide, delta-p)
+    // + final check, decide + velocity
     const int it = ctx->params.max_iterations > 0 ? ctx->params.max_iterations : 1;
-    return 1 + 3 + 1 + 1 + 1 + 1 + 2 + 3 * (it - 1) + 2 + 1 + tail;
+    return 1 + 3 + 1 + 1 + 1 + 1 + 3 + 3 * (it - 1) + 2 + 1 + tail;
   }
   const int per_iter = ctx->params.exact_math ? 3 : 2;
   return 1 + 3 + 1 + 1 + 1 + 1 + per_iter * K + (K == 0 ? 1 : 0) + tail;
@@ -1679,6 +1727,14 @@ int pbf_create(const pbf_params* p, size_t capacity, pbf_ctx** out) {
     fail(ctx, PBF_ERR_CUDA, "no CUDA device");
     return bail(PBF_ERR_CUDA);
   }
+  {
+    int sms = 0;
+    int per_sm = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device) == cudaSuccess && sms > 0 &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kf_density_lambda<kDlCheck>, kBlock, 0) ==
+            cudaSuccess && per_sm > 0)
+      ctx->persistent_blocks = sms * per_sm;
+  }
   if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
     fail(ctx, PBF_ERR_CUDA, "cudaStreamCreate failed");
     return bail(PBF_ERR_CUDA);
@@ -1701,7 +1757,9 @@ int pbf_create(const pbf_params* p, size_t capacity, pbf_ctx** out) {
       (rc = dalloc(ctx, &ctx->stage_i, C * cap + C)) || (rc = dalloc(ctx, &ctx->acc, 8)) ||
       (rc = dalloc(ctx, &ctx->maxerr, 1)) || (rc = dalloc(ctx, &ctx->hits, 1)) ||
       (rc = dalloc(ctx, &ctx->lamsumH, C)) || (rc = dalloc(ctx, &ctx->lamprevS, C)) ||
-      (rc = dalloc(ctx, &ctx->state, 1)) || (rc = dalloc(ctx, &ctx->mlp_params, pbf::kMlpParams)) ||
+      (rc = dalloc(ctx, &ctx->featb, C * pbf::kMlpInPad)) ||
+      (rc = dalloc(ctx, &ctx->state, 1)) || (rc = dalloc(ctx, &ctx->partials, (size_t)ctx->persistent_blocks)) ||
+      (rc = dalloc(ctx, &ctx->mlp_params, pbf::kMlpParams)) ||
       (rc = dalloc(ctx, &ctx->mlp_grad, pbf::kMlpParams)) || (rc = dalloc(ctx, &ctx->mlp_m, pbf::kMlpParams)) ||
       (rc = dalloc(ctx, &ctx->mlp_v, pbf::kMlpParams)) || (rc = dalloc(ctx, &ctx->mlp_norm, 32)) ||
       (rc = dalloc(ctx, &ctx->mlp_loss, 1)) || (rc = dalloc(ctx, &ctx->w1b, pbf::kMlpH * pbf::kMlpInPad)) ||

@@ -60,6 +60,18 @@ struct Group {
   bool live;  // b < n
 };
 
+// Group of this thread in block-sized tile `tile` (grid-stride kernels walk
+// several tiles per block).
+__device__ __forceinline__ Group group_at(int n, int tile) {
+  const int gid = tile * blockDim.x + threadIdx.x;
+  Group g;
+  g.b = gid / kGL;
+  g.lane = gid % kGL;
+  g.live = g.b < n;
+  if (!g.live) g.b = 0;
+  return g;
+}
+
 __device__ __forceinline__ Group group_of(int n) {
   const int gid = blockIdx.x * blockDim.x + threadIdx.x;
   Group g;

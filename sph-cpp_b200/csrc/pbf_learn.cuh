@@ -297,19 +297,51 @@ __device__ __forceinline__ void raw_features(const Dev& P, const Fast& F, float 
 
 // Solver state of the learned warm start, reset each step.
 struct SolveState {
-  double err_sum;       // sum of clamped density errors of the current check pass
   double residual;      // mean clamped density error at the last check
   uint32_t done;        // residual at or below the tolerance: the rest of the step's iterations skip
   uint32_t iterations;  // Jacobi iterations applied this step
 };
 
-// After a check pass: mean error, then either stop or allow one more
-// iteration (the final check of a step only records the residual).
-__global__ void k_decide(int n, float tol, int final_check, SolveState* st) {
-  if (st->done) return;
-  const double mean = st->err_sum / (double)(n > 0 ? n : 1);
+// Sum of v over the block (every thread calls it), written by thread 0 to
+// *out.  Warp sums in float, the warps' sums added in double in warp order:
+// the same inputs give the same bits on every run.
+template <int THREADS>
+__device__ __forceinline__ void block_partial(float v, double* out) {
+  __shared__ float warp_sum[THREADS / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+#pragma unroll
+    for (int w = 0; w < THREADS / 32; ++w) s += (double)warp_sum[w];
+    *out = s;
+  }
+}
+
+// After a check pass: the mean error from the check's per-block partial sums
+// (added in a fixed order, so the decision is the same on every run), then
+// either stop or allow one more iteration (the final check of a step only
+// records the residual).  One block of kDecideThreads.
+constexpr int kDecideThreads = 256;
+__global__ void __launch_bounds__(kDecideThreads) k_decide(int n, float tol, int final_check,
+                                                           const double* __restrict__ partials, int nparts,
+                                                           SolveState* st) {
+  if (st->done) return;  // uniform: read by every thread before thread 0 writes
+  __shared__ double red[kDecideThreads];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < nparts; i += kDecideThreads) s += partials[i];
+  red[threadIdx.x] = s;
+  __syncthreads();
+#pragma unroll
+  for (int o = kDecideThreads / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  const double mean = red[0] / (double)(n > 0 ? n : 1);
   st->residual = mean;
-  st->err_sum = 0.0;
   if (mean <= (double)tol) st->done = 1u;
   else if (!final_check) st->iterations += 1u;
 }
