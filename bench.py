@@ -17,6 +17,9 @@ JSON line on rank 0.
                bandwidth
   cpu_baseline the reference's own OpenMP build (oracle/_ref) on this host's
                cores, a bounded sample of the same workload
+  tuning       the launch shapes (lanes per particle, threads per block) of the
+               gather kernel families the library's autotuner picked during
+               the warm-up (pbf_autotune; --no-autotune keeps the defaults)
 Multi-GPU: the path does not shard in this build (replicas only): every rank
 runs its own full scene on its own GPU; value sums the ranks' particle-steps
 over the slowest rank's time.
@@ -54,6 +57,7 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the plain-vs-learned comparison")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU baseline sample")
+    ap.add_argument("--no-autotune", action="store_true", help="default launch shapes instead of the autotuner's")
     return ap.parse_args()
 
 
@@ -199,10 +203,11 @@ def run_reference_cpu(scene, steps: int, warmup: int, budget_s: float | None) ->
 
 
 # ---------------------------------------------------------------- plain vs learned
-def solver_run(scene, steps: int, warmup: int, params=None, norm=None) -> dict:
-    """Throughput of `steps` graph-replayed steps after `warmup`, then the same
-    run replayed (the fast path is deterministic) with the per-step mean clamped
-    density error and iteration count read after every step."""
+def solver_run(scene, steps: int, warmup: int, params=None, norm=None, autotune: bool = True) -> dict:
+    """Throughput of `steps` graph-replayed steps after `warmup` (the launch
+    shapes autotuned half way through the warm-up), then the same run replayed
+    (the fast path is deterministic) with the per-step mean clamped density
+    error and iteration count read after every step."""
     import torch
     from pbf_b200 import Particles
     p = scene.params()
@@ -213,7 +218,10 @@ def solver_run(scene, steps: int, warmup: int, params=None, norm=None) -> dict:
         stream = torch.cuda.ExternalStream(g.stream_handle())
         x0 = scene.positions()
         g.upload(x0)
-        for _ in range(warmup):
+        tuning = None
+        for i in range(warmup):
+            if autotune and i == warmup // 2:
+                tuning, _ = g.autotune(2)
             g.step(1)
         g.sync()
         e0 = torch.cuda.Event(enable_timing=True)
@@ -245,12 +253,13 @@ def solver_run(scene, steps: int, warmup: int, params=None, norm=None) -> dict:
     import numpy as np
     return {"value": scene.n * steps / t, "ms_per_step": 1e3 * t / steps,
             "mean_density_error": float(np.mean(err)), "max_step_density_error": float(np.max(err)),
-            "mean_iterations": float(np.mean(its)),
+            "mean_iterations": float(np.mean(its)), "tuning": tuning,
             "kernel_ms_per_step": {k: round(v["total_ms"] / steps, 4) for k, v in
                                    sorted(kt.items(), key=lambda kv: -kv[1]["total_ms"])}}
 
 
-def learned_comparison(scene_name: str, steps: int, warmup: int, target: float = 0.01) -> dict:
+def learned_comparison(scene_name: str, steps: int, warmup: int, target: float = 0.01,
+                       autotune: bool = True) -> dict:
     """Plain PBF against the learned warm start at equal mean density error
     <= target (1% of rest density): plain runs with the smallest K in 3..12
     that keeps its mean error over the window at or below the target; the
@@ -263,12 +272,13 @@ def learned_comparison(scene_name: str, steps: int, warmup: int, target: float =
     tried = {}
     plain, K = None, None
     for k in range(3, 13):
-        plain = solver_run(base.with_(solve_steps=k), steps, warmup)
+        plain = solver_run(base.with_(solve_steps=k), steps, warmup, autotune=autotune)
         tried[k] = plain["mean_density_error"]
         K = k
         if plain["mean_density_error"] <= target:
             break
-    learned = solver_run(base.with_(solver=1, residual_tol=target, max_iterations=K), steps, warmup, params, norm)
+    learned = solver_run(base.with_(solver=1, residual_tol=target, max_iterations=K), steps, warmup, params, norm,
+                         autotune=autotune)
     return {"workload": f"{base.name}, relaxation epsilon {base.lambda_epsilon}, steps {warmup}..{warmup + steps}",
             "target_mean_density_error": target, "plain_errors_by_K": tried,
             "plain": dict(plain, iterations=K), "learned": dict(learned, residual_tol=target, max_iterations=K),
@@ -330,7 +340,11 @@ def main():
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         return float(t.item())
 
-    # warm-up (also captures the one-step graph)
+    # warm-up: 3 steps, the autotuner (times each launch shape on 3 steps from
+    # this state, then restores it), then W steps (the last captures the graph)
+    for _ in range(3):
+        g.step(1)
+    tuning, tune_table = (None, None) if args.no_autotune else g.autotune(3)
     for _ in range(max(W, 3)):
         g.step(1)
     barrier()
@@ -401,7 +415,7 @@ def main():
     learned = None
     if rank == 0 and world == 1 and not args.no_learned:
         try:
-            learned = learned_comparison(args.scene, max(K, 20), 100)
+            learned = learned_comparison(args.scene, max(K, 20), 100, autotune=not args.no_autotune)
         except Exception as e:  # reported, never fatal for the GPU line
             learned = {"error": str(e)}
 
@@ -425,6 +439,7 @@ def main():
                        "lambda_epsilon": scene.lambda_epsilon, "neighbor_cap": scene.neighbor_cap,
                        "exact_math": scene.exact_math, "scorr": "off (reference has none)",
                        "parallelism": f"replicas x{world}",
+                       "tuning": g.tuning(), "autotuned": not args.no_autotune,
                        "l2": "no flush: per-step working set (lists %.0f MB + state) > 126 MB L2" % (
                            scene.n * (4 * nbar + 4) / 1e6)},
             "e2e": {"value": scene.n * K * world / t_e2e, "unit": UNIT, "h2d_bytes_per_step": scene.n * 24,
@@ -436,6 +451,8 @@ def main():
                          "algorithmic_bytes_per_launch": dom_bytes, "peak_source": peaks["source"],
                          "step_gbs": step_bytes / (t_dev / K) / 1e9},
             "kernels": kernels,
+            "autotune_ms_per_step": None if tune_table is None else
+            {f"{l}x{b}": v for (l, b), v in tune_table.items()},
             "physics": {"mean_neighbors": nbar, "cap_hits": st["cap_hits"],
                         "mean_density_error": st["mean_density_error"], "error_flags": st["error_flags"],
                         "finite": ok},

@@ -222,8 +222,8 @@ int pbf_sync(pbf_ctx* ctx);
 int pbf_get_stream(pbf_ctx* ctx, void** stream_out);
 
 /* ---- instrumentation ---- */
-/* Per-kernel device time: with timing on, pbf_step records a CUDA event
- * around every kernel of every step on the context stream (inside the graph).
+/* Per-kernel device time: with timing on, pbf_step launches the step's
+ * kernels one by one (no graph) and records a CUDA event around each.
  * pbf_kernel_times returns, per kernel family, launches and total ms since
  * the last reset.  names[i] points to static strings. */
 int pbf_set_timing(pbf_ctx* ctx, int on);
@@ -232,6 +232,39 @@ int pbf_kernel_times(pbf_ctx* ctx, int max_kinds, const char** names, int64_t* l
 int pbf_reset_timing(pbf_ctx* ctx);
 /* Number of kernel launches one pbf_step(ctx, 1) issues. */
 int pbf_launches_per_step(pbf_ctx* ctx, int64_t* out);
+
+/* ---- launch shapes of the fast-math gather kernels ----
+ * No counterpart in the reference (its loops are OpenMP for_each_index).
+ * Each family of gather kernels runs with `lanes` threads per particle
+ * walking one neighbor list together (4 or 8) in blocks of `block` threads
+ * (128 or 256).  The shape changes only the order of floating-point sums
+ * inside a particle (fast math), never the lists; exact_math kernels run one
+ * thread per particle and ignore it.  Default: 8 lanes, 256 threads. */
+enum {
+  PBF_TUNE_DENSITY = 0,          /* density + lambda, and the learned solver's residual check */
+  PBF_TUNE_DELTA_P = 1,          /* position delta + x* update */
+  PBF_TUNE_VISCOSITY = 2,        /* both XSPH passes */
+  PBF_TUNE_VORTICITY = 3,
+  PBF_TUNE_APPLY_VORTICITY = 4,
+  PBF_TUNE_FAMILIES = 5
+};
+#define PBF_TUNE_CANDIDATES 4  /* (lanes, block) = (4,128) (4,256) (8,128) (8,256) */
+typedef struct {
+  int lanes[PBF_TUNE_FAMILIES];
+  int block[PBF_TUNE_FAMILIES];
+} pbf_tuning;
+int pbf_get_tuning(const pbf_ctx* ctx, pbf_tuning* out);
+/* PBF_ERR_ARG for a shape outside the candidates; drops captured graphs. */
+int pbf_set_tuning(pbf_ctx* ctx, const pbf_tuning* t);
+/* Autotuner: from the current particle state, runs `steps` (>= 1) timed
+ * steps per candidate shape after one untimed step, restoring the state before
+ * each candidate and at the end; applies and returns (chosen, may be NULL) the
+ * fastest shape of each family.  ms (may be NULL) receives
+ * [PBF_TUNE_CANDIDATES][PBF_TUNE_FAMILIES] device ms per step.  The particle
+ * state (positions, velocities, the learned solver's lambda history) is left
+ * as found; neighbor lists and statistics need a new step.  Kernel timing
+ * totals are reset. */
+int pbf_autotune(pbf_ctx* ctx, int steps, pbf_tuning* chosen, double* ms);
 
 /* ---- learned warm start: the per-particle MLP ----
  * 12 -> 64 -> 64 -> 1, GELU, BF16 tensor-core GEMMs with FP32 accumulation.

@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <cfloat>
 #include <cmath>
 #include <cstdarg>
@@ -536,40 +537,59 @@ struct LearnIO {
   int first;              // first Jacobi iteration of the step
 };
 
-template <int MODE>
+// The sums a density + lambda gather produces for one particle, combined
+// over its lane group: sw = sum (h^2 - d^2)^3, s1 = sum (h-r)^2/r * r_vec,
+// s2 = sum ((h-r)^2/r)^2 d^2 (the constant factors of grad C are applied once,
+// after the walk), the smallest d^2 and (NH) the count of neighbours inside h.
+struct DensitySums {
+  float sw, s1x, s1y, s1z, s2, dmin, nh;
+};
+
+template <int GL, bool NH>
+__device__ __forceinline__ DensitySums density_sums(const Fast& F, const pbf::Group& G, const int32_t* row, int c,
+                                                    const float4* __restrict__ pst, float4 xp) {
+  DensitySums S{0.f, 0.f, 0.f, 0.f, 0.f, FLT_MAX, 0.f};
+  pbf::gwalk1<GL>(row, c, G.lane, pst, [&](int, float4 xq) {
+    const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
+    const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+    S.dmin = fminf(S.dmin, d2);
+    if (NH) S.nh += d2 < F.h2 ? 1.f : 0.f;
+    const float a = fmaxf(F.h2 - d2, 0.0f);
+    S.sw = fmaf(a * a, a, S.sw);
+    const float t = pbf::spikey_over_r(F, d2);
+    S.s1x = fmaf(t, dx, S.s1x);
+    S.s1y = fmaf(t, dy, S.s1y);
+    S.s1z = fmaf(t, dz, S.s1z);
+    S.s2 = fmaf(t * t, d2, S.s2);
+  });
+  S.sw = pbf::gsum<GL>(S.sw);
+  S.s1x = pbf::gsum<GL>(S.s1x);
+  S.s1y = pbf::gsum<GL>(S.s1y);
+  S.s1z = pbf::gsum<GL>(S.s1z);
+  S.s2 = pbf::gsum<GL>(S.s2);
+  if (NH) S.nh = pbf::gsum<GL>(S.nh);
+  S.dmin = pbf::gmin<GL>(S.dmin);
+  return S;
+}
+
+template <int MODE, int GL>
 __device__ __forceinline__ void density_lambda_tile(int tile, const Dev& P, const Fast& F, int n, size_t stride,
                                                     const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
                                                     const float4* __restrict__ pst, float4* xl, float4* vel,
                                                     float* lam, uint32_t* nudge, const LearnIO& io, float& err) {
-  const pbf::Group G = pbf::group_at(n, tile);
+  const pbf::Group G = pbf::group_at<GL>(n, tile);
   const int b = G.b;
   const float4 xp = pst[b];
   const int c = G.live ? cnt[b] : 0;
-  float sw = 0.f, sgx = 0.f, sgy = 0.f, sgz = 0.f, sc = 0.f, nh = 0.f;
-  int close = 0;
-  pbf::gwalk1(nbr + (size_t)b * stride, c, G.lane, pst, [&](int, float4 xq) {
-    const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
-    const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-    close |= d2 < 4e-16f;
-    if (MODE == kDlRecord) nh += d2 < F.h2 ? 1.f : 0.f;
-    sw += pbf::poly_cube(F, d2);
-    const float t = F.lam_grad * pbf::spikey_over_r(F, d2);
-    sgx = fmaf(-t, dx, sgx);
-    sgy = fmaf(-t, dy, sgy);
-    sgz = fmaf(-t, dz, sgz);
-    sc = fmaf(t * t, d2, sc);
-  });
-  sw = pbf::gsum(sw);
-  sgx = pbf::gsum(sgx);
-  sgy = pbf::gsum(sgy);
-  sgz = pbf::gsum(sgz);
-  sc = pbf::gsum(sc);
-  if (MODE == kDlRecord) nh = pbf::gsum(nh);
-  close = pbf::gor(close);
-  const float rho = fmaf(F.m_poly, sw, F.m_w0);
+  const DensitySums S = density_sums<GL, MODE == kDlRecord>(F, G, nbr + (size_t)b * stride, c, pst, xp);
+  const float rho = fmaf(F.m_poly, S.sw, F.m_w0);
   if (MODE == kDlCheck && G.live && G.lane == 0) err += fmaxf(fmaf(rho, F.inv_rho0, -1.0f), 0.0f);
   if (!G.live || G.lane != 0) return;
-  const float g2 = sgx * sgx + sgy * sgy + sgz * sgz;
+  const float L2 = F.lam_grad * F.lam_grad;
+  const float sc = L2 * S.s2;  // sum |grad_q C|^2
+  const float g2 = L2 * fmaf(S.s1z, S.s1z, fmaf(S.s1y, S.s1y, S.s1x * S.s1x));  // |grad_p C|^2
+  const bool close = S.dmin < 4e-16f;
+  const float nh = S.nh;
   if (close) {  // a neighbour (almost) on top: the reference-ordered path decides the nudge
     density_lambda_one<false>(P, b, stride, nbr, cnt, pst, xl, vel, lam, nudge);
   } else {
@@ -594,17 +614,17 @@ __device__ __forceinline__ void density_lambda_tile(int tile, const Dev& P, cons
 
 // The residual check runs on a persistent grid walking the tiles, so that
 // once the step has converged the launch costs a few hundred empty blocks.
-template <int MODE>
+template <int MODE, int GL>
 __global__ void __launch_bounds__(kBlock) kf_density_lambda(Dev P, Fast F, int n, size_t stride,
                                                             const int32_t* __restrict__ nbr,
                                                             const int32_t* __restrict__ cnt,
                                                             const float4* __restrict__ pst, float4* xl, float4* vel,
                                                             float* lam, uint32_t* nudge, LearnIO io) {
   if (MODE == kDlCheck && io.state->done) return;
-  const int tiles = (int)(((size_t)n * pbf::kGL + kBlock - 1) / kBlock);
+  const int tiles = pbf::tiles_of<GL>(n);
   float err = 0.0f;
   for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x)
-    density_lambda_tile<MODE>(tile, P, F, n, stride, nbr, cnt, pst, xl, vel, lam, nudge, io, err);
+    density_lambda_tile<MODE, GL>(tile, P, F, n, stride, nbr, cnt, pst, xl, vel, lam, nudge, io, err);
   if (MODE == kDlCheck) pbf::block_partial<kBlock>(err, io.partials + blockIdx.x);
 }
 
@@ -631,30 +651,14 @@ __global__ void __launch_bounds__(kBlock) kl_features(Dev P, Fast F, pbf::MlpDev
   const int b = G.b;
   const float4 xp = pst[b];
   const int c = G.live ? cnt[b] : 0;
-  float sw = 0.f, sgx = 0.f, sgy = 0.f, sgz = 0.f, sc = 0.f, nh = 0.f;
-  int close = 0;
-  pbf::gwalk1(nbr + (size_t)b * stride, c, G.lane, pst, [&](int, float4 xq) {
-    const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
-    const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-    close |= d2 < 4e-16f;
-    nh += d2 < F.h2 ? 1.f : 0.f;
-    sw += pbf::poly_cube(F, d2);
-    const float t = F.lam_grad * pbf::spikey_over_r(F, d2);
-    sgx = fmaf(-t, dx, sgx);
-    sgy = fmaf(-t, dy, sgy);
-    sgz = fmaf(-t, dz, sgz);
-    sc = fmaf(t * t, d2, sc);
-  });
-  sw = pbf::gsum(sw);
-  sgx = pbf::gsum(sgx);
-  sgy = pbf::gsum(sgy);
-  sgz = pbf::gsum(sgz);
-  sc = pbf::gsum(sc);
-  nh = pbf::gsum(nh);
-  close = pbf::gor(close);
+  const DensitySums S = density_sums<pbf::kGL, true>(F, G, nbr + (size_t)b * stride, c, pst, xp);
   if (!G.live || G.lane != 0) return;
-  const float rho = fmaf(F.m_poly, sw, F.m_w0);
-  const float g2 = sgx * sgx + sgy * sgy + sgz * sgz;
+  const float rho = fmaf(F.m_poly, S.sw, F.m_w0);
+  const float L2 = F.lam_grad * F.lam_grad;
+  const float sc = L2 * S.s2;
+  const float g2 = L2 * fmaf(S.s1z, S.s1z, fmaf(S.s1y, S.s1y, S.s1x * S.s1x));
+  const bool close = S.dmin < 4e-16f;
+  const float nh = S.nh;
   const float4 v = vel[b];
   float f[pbf::kMlpIn];
   pbf::raw_features(P, F, f, c, rho, sc, g2, (int)nh, lamprev[b], v, xp);
@@ -996,18 +1000,18 @@ __global__ void __launch_bounds__(kBlock) k_apply_vorticity(Dev P, int n, size_t
 // ---- fast gathers (exact_math = 0), kGL lanes per particle, see pbf_fast.cuh ----
 // COND: the learned solver's extra iterations, skipped once the step has
 // converged; lamsum (when given) accumulates the applied lambda.
-template <bool SCORR, bool LAST>
+template <bool SCORR, bool LAST, int GL>
 __device__ __forceinline__ void dp_update_tile(int tile, const Dev& P, const Fast& F, int n, size_t stride,
                                                const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
                                                const float4* __restrict__ xl, float4* pst,
                                                const float4* __restrict__ pos, float4* vel, float* lamsum) {
-  const pbf::Group G = pbf::group_at(n, tile);
+  const pbf::Group G = pbf::group_at<GL>(n, tile);
   const int b = G.b;
   const float4 xp = xl[b];
   const int c = G.live ? cnt[b] : 0;
   float ax = 0.f, ay = 0.f, az = 0.f;
   const float lp = xp.w;
-  pbf::gwalk1(nbr + (size_t)b * stride, c, G.lane, xl, [&](int, float4 xq) {
+  pbf::gwalk1<GL>(nbr + (size_t)b * stride, c, G.lane, xl, [&](int, float4 xq) {
     const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
     const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
     float l = lp + xq.w;
@@ -1017,9 +1021,9 @@ __device__ __forceinline__ void dp_update_tile(int tile, const Dev& P, const Fas
     ay = fmaf(t, dy, ay);
     az = fmaf(t, dz, az);
   });
-  ax = pbf::gsum(ax);
-  ay = pbf::gsum(ay);
-  az = pbf::gsum(az);
+  ax = pbf::gsum<GL>(ax);
+  ay = pbf::gsum<GL>(ay);
+  az = pbf::gsum<GL>(az);
   if (!G.live || G.lane != 0) return;
   if (lamsum) lamsum[b] += xp.w;
   const float3 s = pbf::boundary(P, make_float3(pbf::xadd(xp.x, F.dp_scale * ax), pbf::xadd(xp.y, F.dp_scale * ay),
@@ -1034,30 +1038,30 @@ __device__ __forceinline__ void dp_update_tile(int tile, const Dev& P, const Fas
 
 // COND launches (the learned solver's extra iterations) use a persistent grid
 // and skip the whole launch once the step has converged.
-template <bool SCORR, bool LAST, bool COND>
+template <bool SCORR, bool LAST, bool COND, int GL>
 __global__ void __launch_bounds__(kBlock) kf_dp_update(Dev P, Fast F, int n, size_t stride,
                                                        const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
                                                        const float4* __restrict__ xl, float4* pst,
                                                        const float4* __restrict__ pos, float4* vel,
                                                        const pbf::SolveState* __restrict__ state, float* lamsum) {
   if (COND && state->done) return;
-  const int tiles = (int)(((size_t)n * pbf::kGL + kBlock - 1) / kBlock);
+  const int tiles = pbf::tiles_of<GL>(n);
   for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x)
-    dp_update_tile<SCORR, LAST>(tile, P, F, n, stride, nbr, cnt, xl, pst, pos, vel, lamsum);
+    dp_update_tile<SCORR, LAST, GL>(tile, P, F, n, stride, nbr, cnt, xl, pst, pos, vel, lamsum);
 }
 
-template <bool FINAL>
+template <bool FINAL, int GL>
 __global__ void __launch_bounds__(kBlock) kf_viscosity(Dev P, Fast F, int n, size_t stride,
                                                        const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
                                                        const float4* __restrict__ pst, const float4* __restrict__ vin,
                                                        float4* vout, float4* posH, float4* pstH,
                                                        const uint32_t* __restrict__ origS, uint32_t* origH) {
-  const pbf::Group G = pbf::group_of(n);
+  const pbf::Group G = pbf::group_of<GL>(n);
   const int b = G.b;
   const float4 xp = pst[b], vp = vin[b];
   const int c = G.live ? cnt[b] : 0;
   float ax = 0.f, ay = 0.f, az = 0.f;
-  pbf::gwalk2(nbr + (size_t)b * stride, c, G.lane, pst, vin, [&](int, float4 xq, float4 vq) {
+  pbf::gwalk2<GL>(nbr + (size_t)b * stride, c, G.lane, pst, vin, [&](int, float4 xq, float4 vq) {
     const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
     const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
     const float wr = __fdividef(pbf::poly_cube(F, d2), vq.w);
@@ -1065,9 +1069,9 @@ __global__ void __launch_bounds__(kBlock) kf_viscosity(Dev P, Fast F, int n, siz
     ay = fmaf(vq.y - vp.y, wr, ay);
     az = fmaf(vq.z - vp.z, wr, az);
   });
-  ax = pbf::gsum(ax);
-  ay = pbf::gsum(ay);
-  az = pbf::gsum(az);
+  ax = pbf::gsum<GL>(ax);
+  ay = pbf::gsum<GL>(ay);
+  az = pbf::gsum<GL>(az);
   if (!G.live || G.lane != 0) return;
   const float k = F.visc_c * F.visc_poly;
   vout[b] = make_float4(fmaf(k, ax, vp.x), fmaf(k, ay, vp.y), fmaf(k, az, vp.z), vp.w);
@@ -1078,16 +1082,17 @@ __global__ void __launch_bounds__(kBlock) kf_viscosity(Dev P, Fast F, int n, siz
   }
 }
 
+template <int GL>
 __global__ void __launch_bounds__(kBlock) kf_vorticity(Dev P, Fast F, int n, size_t stride,
                                                        const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
                                                        const float4* __restrict__ pst, const float4* __restrict__ vel,
                                                        float4* scr, float4* xl) {
-  const pbf::Group G = pbf::group_of(n);
+  const pbf::Group G = pbf::group_of<GL>(n);
   const int b = G.b;
   const float4 xp = pst[b], vp = vel[b];
   const int c = G.live ? cnt[b] : 0;
   float wx = 0.f, wy = 0.f, wz = 0.f;
-  pbf::gwalk2(nbr + (size_t)b * stride, c, G.lane, pst, vel, [&](int, float4 xq, float4 vq) {
+  pbf::gwalk2<GL>(nbr + (size_t)b * stride, c, G.lane, pst, vel, [&](int, float4 xq, float4 vq) {
     const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
     const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
     const float t = pbf::spikey_over_r(F, d2);
@@ -1097,26 +1102,27 @@ __global__ void __launch_bounds__(kBlock) kf_vorticity(Dev P, Fast F, int n, siz
     wy = fmaf(t, fmaf(uz, dx, -ux * dz), wy);
     wz = fmaf(t, fmaf(ux, dy, -uy * dx), wz);
   });
-  wx = pbf::gsum(wx) * F.spikey;
-  wy = pbf::gsum(wy) * F.spikey;
-  wz = pbf::gsum(wz) * F.spikey;
+  wx = pbf::gsum<GL>(wx) * F.spikey;
+  wy = pbf::gsum<GL>(wy) * F.spikey;
+  wz = pbf::gsum<GL>(wz) * F.spikey;
   if (!G.live || G.lane != 0) return;
   const float wm = sqrtf(fmaf(wz, wz, fmaf(wy, wy, wx * wx)));
   scr[b] = make_float4(wx, wy, wz, wm);
   xl[b] = make_float4(xp.x, xp.y, xp.z, wm);
 }
 
+template <int GL>
 __global__ void __launch_bounds__(kBlock) kf_apply_vorticity(Dev P, Fast F, int n, size_t stride,
                                                              const int32_t* __restrict__ nbr,
                                                              const int32_t* __restrict__ cnt,
                                                              const float4* __restrict__ xl,
                                                              const float4* __restrict__ scr, float4* vel) {
-  const pbf::Group G = pbf::group_of(n);
+  const pbf::Group G = pbf::group_of<GL>(n);
   const int b = G.b;
   const float4 xp = xl[b];
   const int c = G.live ? cnt[b] : 0;
   float ex = 0.f, ey = 0.f, ez = 0.f;
-  pbf::gwalk1(nbr + (size_t)b * stride, c, G.lane, xl, [&](int, float4 xq) {
+  pbf::gwalk1<GL>(nbr + (size_t)b * stride, c, G.lane, xl, [&](int, float4 xq) {
     const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
     const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
     const float t = xq.w * pbf::spikey_over_r(F, d2);
@@ -1124,9 +1130,9 @@ __global__ void __launch_bounds__(kBlock) kf_apply_vorticity(Dev P, Fast F, int 
     ey = fmaf(t, dy, ey);
     ez = fmaf(t, dz, ez);
   });
-  ex = pbf::gsum(ex) * F.spikey;
-  ey = pbf::gsum(ey) * F.spikey;
-  ez = pbf::gsum(ez) * F.spikey;
+  ex = pbf::gsum<GL>(ex) * F.spikey;
+  ey = pbf::gsum<GL>(ey) * F.spikey;
+  ez = pbf::gsum<GL>(ez) * F.spikey;
   if (!G.live || G.lane != 0) return;
   const float inv = __fdividef(1.0f, sqrtf(fmaf(ez, ez, fmaf(ey, ey, ex * ex))) + FLT_EPSILON);
   const float Nx = ex * inv, Ny = ey * inv, Nz = ez * inv;
@@ -1226,7 +1232,7 @@ struct pbf_ctx {
   float *lamsumH = nullptr, *lamprevS = nullptr, *feats = nullptr;
   __nv_bfloat16* featb = nullptr;  // [C][16] normalised features of the warm iteration
   pbf::SolveState* state = nullptr;
-  double* partials = nullptr;  // [persistent_blocks] residual check sums
+  double* partials = nullptr;  // [partials_cap] residual check sums, one per block
   bool recording = false;
   float *mlp_params = nullptr, *mlp_grad = nullptr, *mlp_m = nullptr, *mlp_v = nullptr, *mlp_norm = nullptr;
   float* mlp_loss = nullptr;
@@ -1234,7 +1240,12 @@ struct pbf_ctx {
   float label_scale = 1.0f;
   int adam_t = 0;
   bool mlp_ready = false;
-  int persistent_blocks = 148 * 4;  // SMs x resident check blocks, set at creation
+  // launch shapes of the fast gather families, and the persistent grids of
+  // the learned solver's skippable launches (SMs x resident blocks)
+  pbf_tuning tune{{8, 8, 8, 8, 8}, {kBlock, kBlock, kBlock, kBlock, kBlock}};
+  int sms = 148;
+  int pgrid_check = 148, pgrid_dp = 148;
+  int partials_cap = 0;
 
   std::map<int, cudaGraphExec_t> graphs;
   std::vector<void*> allocations;
@@ -1399,6 +1410,44 @@ int need_lists(pbf_ctx* ctx) {
   return PBF_OK;
 }
 
+// ---- launch shapes of the fast gather kernels ----
+// fn(std::integral_constant<int, GL>) for the lanes-per-particle of a shape.
+template <class Fn>
+void with_lanes(int lanes, Fn&& fn) {
+  if (lanes == 4)
+    fn(std::integral_constant<int, 4>{});
+  else
+    fn(std::integral_constant<int, 8>{});
+}
+
+bool shape_ok(int lanes, int block) { return (lanes == 4 || lanes == 8) && (block == 128 || block == 256); }
+
+int grid_of(const pbf_ctx* ctx, int family) {
+  return blocks_for(ctx->n * (size_t)ctx->tune.lanes[family], ctx->tune.block[family]);
+}
+
+// Persistent grids of the residual check and the conditional delta-p pass for
+// the current shapes: SMs x resident blocks, at most partials_cap.
+int update_shapes(pbf_ctx* ctx) {
+  auto resident = [&](const void* fn, int block) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, 0) != cudaSuccess || per_sm <= 0)
+      per_sm = 1;
+    return std::min(ctx->sms * per_sm, ctx->partials_cap);
+  };
+  const pbf_tuning& t = ctx->tune;
+  with_lanes(t.lanes[PBF_TUNE_DENSITY], [&](auto gl) {
+    ctx->pgrid_check = resident((const void*)kf_density_lambda<kDlCheck, decltype(gl)::value>,
+                                t.block[PBF_TUNE_DENSITY]);
+  });
+  with_lanes(t.lanes[PBF_TUNE_DELTA_P], [&](auto gl) {
+    ctx->pgrid_dp = resident((const void*)kf_dp_update<false, false, true, decltype(gl)::value>,
+                             t.block[PBF_TUNE_DELTA_P]);
+  });
+  cudaGetLastError();  // occupancy queries leave no error behind
+  return PBF_OK;
+}
+
 // ---- launch bookkeeping: per-kernel CUDA events when timing is on ----
 struct Launch {
   pbf_ctx* ctx;
@@ -1504,8 +1553,12 @@ void launch_learned_solve(pbf_ctx* ctx) {
   const Dev& P = ctx->dev;
   const Fast& F = ctx->fast;
   cudaStream_t s = ctx->stream;
+  const pbf_tuning& T = ctx->tune;
   const int g = blocks_for(n), gg = blocks_for((size_t)n * pbf::kGL);
-  const int gp = std::min(gg, ctx->persistent_blocks);  // skippable launches: persistent grid
+  // skippable launches: persistent grids
+  const int gpc = std::min(grid_of(ctx, PBF_TUNE_DENSITY), ctx->pgrid_check);
+  const int gpd = std::min(grid_of(ctx, PBF_TUNE_DELTA_P), ctx->pgrid_dp);
+  const int bd = T.block[PBF_TUNE_DENSITY], bp = T.block[PBF_TUNE_DELTA_P];
   const float tol = ctx->params.residual_tol;
   const int iters = ctx->params.max_iterations > 0 ? ctx->params.max_iterations : 1;
   cudaMemsetAsync(ctx->state, 0, sizeof(pbf::SolveState), s);
@@ -1521,26 +1574,28 @@ void launch_learned_solve(pbf_ctx* ctx) {
     const int warps = (n + 15) / 16;
     kl_mlp<<<(warps + 3) / 4, 128, 0, s>>>(M, n, ctx->featb, ctx->xl, ctx->lamH, ctx->lamsumH);
   }
-  {
+  with_lanes(T.lanes[PBF_TUNE_DELTA_P], [&](auto gl) {
     Launch L(ctx, "dp_update");
-    kf_dp_update<SCORR, false, false><<<gg, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS,
-                                                           ctx->posS, ctx->velS, ctx->state, nullptr);
-  }
+    kf_dp_update<SCORR, false, false, decltype(gl)::value><<<grid_of(ctx, PBF_TUNE_DELTA_P), bp, 0, s>>>(
+        P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS, ctx->posS, ctx->velS, ctx->state, nullptr);
+  });
   for (int r = 1; r <= iters; ++r) {
     const bool final_check = r == iters;
-    {
+    with_lanes(T.lanes[PBF_TUNE_DENSITY], [&](auto gl) {
       Launch L(ctx, "residual_check");
-      kf_density_lambda<kDlCheck><<<gp, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl,
-                                                        ctx->velS, ctx->lamH, ctx->nudge, io);
-    }
+      kf_density_lambda<kDlCheck, decltype(gl)::value><<<gpc, bd, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS,
+                                                                         ctx->xl, ctx->velS, ctx->lamH, ctx->nudge, io);
+    });
     {
       Launch L(ctx, "decide");
-      pbf::k_decide<<<1, pbf::kDecideThreads, 0, s>>>(n, tol, final_check ? 1 : 0, ctx->partials, gp, ctx->state);
+      pbf::k_decide<<<1, pbf::kDecideThreads, 0, s>>>(n, tol, final_check ? 1 : 0, ctx->partials, gpc, ctx->state);
     }
     if (final_check) break;
-    Launch L(ctx, "dp_update");
-    kf_dp_update<SCORR, false, true><<<gp, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS,
-                                                          ctx->posS, ctx->velS, ctx->state, ctx->lamsumH);
+    with_lanes(T.lanes[PBF_TUNE_DELTA_P], [&](auto gl) {
+      Launch L(ctx, "dp_update");
+      kf_dp_update<SCORR, false, true, decltype(gl)::value><<<gpd, bp, 0, s>>>(
+          P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS, ctx->posS, ctx->velS, ctx->state, ctx->lamsumH);
+    });
   }
   Launch L(ctx, "update_velocities");
   k_update_v<<<g, kBlock, 0, s>>>(P, n, ctx->pstS, ctx->posS, ctx->velS);
@@ -1570,7 +1625,7 @@ void launch_step_t(pbf_ctx* ctx) {
   launch_fill(ctx, ctx->pstS);
   const int K = ctx->params.solve_steps;
   const Fast& F = ctx->fast;
-  const int gg = blocks_for((size_t)n * pbf::kGL);  // kGL lanes per particle
+  const pbf_tuning& T = ctx->tune;
   if (!X && ctx->params.solver == 1) {
     launch_learned_solve<SCORR>(ctx);
   } else {
@@ -1583,12 +1638,17 @@ void launch_step_t(pbf_ctx* ctx) {
       if (X)
         k_density_lambda<X><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl, ctx->velS,
                                                  ctx->lamH, ctx->nudge);
-      else if (ctx->recording)
-        kf_density_lambda<kDlRecord><<<gg, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl,
-                                                           ctx->velS, ctx->lamH, ctx->nudge, io);
       else
-        kf_density_lambda<kDlPlain><<<gg, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl,
-                                                          ctx->velS, ctx->lamH, ctx->nudge, io);
+        with_lanes(T.lanes[PBF_TUNE_DENSITY], [&](auto gl) {
+          constexpr int GL = decltype(gl)::value;
+          const int gd = grid_of(ctx, PBF_TUNE_DENSITY), bd = T.block[PBF_TUNE_DENSITY];
+          if (ctx->recording)
+            kf_density_lambda<kDlRecord, GL><<<gd, bd, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl,
+                                                               ctx->velS, ctx->lamH, ctx->nudge, io);
+          else
+            kf_density_lambda<kDlPlain, GL><<<gd, bd, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl,
+                                                              ctx->velS, ctx->lamH, ctx->nudge, io);
+        });
     }
     if (X) {
       Launch L(ctx, "lambda_fixup");
@@ -1605,12 +1665,16 @@ void launch_step_t(pbf_ctx* ctx) {
         k_dp_update<X, SCORR, false><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS,
                                                           ctx->posS, ctx->velS, ctx->lamH, ctx->nudge);
     } else {
-      if (last)
-        kf_dp_update<SCORR, true, false><<<gg, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS,
-                                                              ctx->posS, ctx->velS, ctx->state, nullptr);
-      else
-        kf_dp_update<SCORR, false, false><<<gg, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS,
-                                                               ctx->posS, ctx->velS, ctx->state, nullptr);
+      with_lanes(T.lanes[PBF_TUNE_DELTA_P], [&](auto gl) {
+        constexpr int GL = decltype(gl)::value;
+        const int gd = grid_of(ctx, PBF_TUNE_DELTA_P), bd = T.block[PBF_TUNE_DELTA_P];
+        if (last)
+          kf_dp_update<SCORR, true, false, GL><<<gd, bd, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS,
+                                                                 ctx->posS, ctx->velS, ctx->state, nullptr);
+        else
+          kf_dp_update<SCORR, false, false, GL><<<gd, bd, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl,
+                                                                  ctx->pstS, ctx->posS, ctx->velS, ctx->state, nullptr);
+      });
     }
   }
   }
@@ -1645,22 +1709,30 @@ void launch_step_t(pbf_ctx* ctx) {
     k_viscosity<X, true><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->velT, ctx->velH,
                                               ctx->posH, ctx->pstH, ctx->origS, ctx->origH);
   } else {
-    {
+    const int gv = grid_of(ctx, PBF_TUNE_VISCOSITY), bv = T.block[PBF_TUNE_VISCOSITY];
+    with_lanes(T.lanes[PBF_TUNE_VISCOSITY], [&](auto gl) {
       Launch L(ctx, "viscosity");
-      kf_viscosity<false><<<gg, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->velS, ctx->velT,
-                                               nullptr, nullptr, nullptr, nullptr);
-    }
-    {
+      kf_viscosity<false, decltype(gl)::value><<<gv, bv, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS,
+                                                                 ctx->velS, ctx->velT, nullptr, nullptr, nullptr,
+                                                                 nullptr);
+    });
+    with_lanes(T.lanes[PBF_TUNE_VORTICITY], [&](auto gl) {
       Launch L(ctx, "vorticity");
-      kf_vorticity<<<gg, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->velT, ctx->scrH, ctx->xl);
-    }
-    {
+      kf_vorticity<decltype(gl)::value><<<grid_of(ctx, PBF_TUNE_VORTICITY), T.block[PBF_TUNE_VORTICITY], 0, s>>>(
+          P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->velT, ctx->scrH, ctx->xl);
+    });
+    with_lanes(T.lanes[PBF_TUNE_APPLY_VORTICITY], [&](auto gl) {
       Launch L(ctx, "apply_vorticity");
-      kf_apply_vorticity<<<gg, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->scrH, ctx->velT);
-    }
-    Launch L(ctx, "viscosity_final");
-    kf_viscosity<true><<<gg, kBlock, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->velT, ctx->velH,
-                                            ctx->posH, ctx->pstH, ctx->origS, ctx->origH);
+      kf_apply_vorticity<decltype(gl)::value>
+          <<<grid_of(ctx, PBF_TUNE_APPLY_VORTICITY), T.block[PBF_TUNE_APPLY_VORTICITY], 0, s>>>(
+              P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->scrH, ctx->velT);
+    });
+    with_lanes(T.lanes[PBF_TUNE_VISCOSITY], [&](auto gl) {
+      Launch L(ctx, "viscosity_final");
+      kf_viscosity<true, decltype(gl)::value><<<gv, bv, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->velT,
+                                                                ctx->velH, ctx->posH, ctx->pstH, ctx->origS,
+                                                                ctx->origH);
+    });
   }
 }
 
@@ -1728,12 +1800,14 @@ int pbf_create(const pbf_params* p, size_t capacity, pbf_ctx** out) {
     return bail(PBF_ERR_CUDA);
   }
   {
-    int sms = 0;
-    int per_sm = 0;
-    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device) == cudaSuccess && sms > 0 &&
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kf_density_lambda<kDlCheck>, kBlock, 0) ==
-            cudaSuccess && per_sm > 0)
-      ctx->persistent_blocks = sms * per_sm;
+    int sms = 0, per_sm = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device) == cudaSuccess && sms > 0)
+      ctx->sms = sms;
+    if (cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxBlocksPerMultiprocessor, ctx->device) != cudaSuccess ||
+        per_sm <= 0)
+      per_sm = 32;
+    ctx->partials_cap = ctx->sms * per_sm;
+    if ((rc = update_shapes(ctx))) return bail(rc);
   }
   if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
     fail(ctx, PBF_ERR_CUDA, "cudaStreamCreate failed");
@@ -1758,7 +1832,7 @@ int pbf_create(const pbf_params* p, size_t capacity, pbf_ctx** out) {
       (rc = dalloc(ctx, &ctx->maxerr, 1)) || (rc = dalloc(ctx, &ctx->hits, 1)) ||
       (rc = dalloc(ctx, &ctx->lamsumH, C)) || (rc = dalloc(ctx, &ctx->lamprevS, C)) ||
       (rc = dalloc(ctx, &ctx->featb, C * pbf::kMlpInPad)) ||
-      (rc = dalloc(ctx, &ctx->state, 1)) || (rc = dalloc(ctx, &ctx->partials, (size_t)ctx->persistent_blocks)) ||
+      (rc = dalloc(ctx, &ctx->state, 1)) || (rc = dalloc(ctx, &ctx->partials, (size_t)ctx->partials_cap)) ||
       (rc = dalloc(ctx, &ctx->mlp_params, pbf::kMlpParams)) ||
       (rc = dalloc(ctx, &ctx->mlp_grad, pbf::kMlpParams)) || (rc = dalloc(ctx, &ctx->mlp_m, pbf::kMlpParams)) ||
       (rc = dalloc(ctx, &ctx->mlp_v, pbf::kMlpParams)) || (rc = dalloc(ctx, &ctx->mlp_norm, 32)) ||
@@ -2054,7 +2128,7 @@ int pbf_apply_vorticity(pbf_ctx* ctx, size_t b, size_t e) {
 
 int pbf_update_positions(pbf_ctx* ctx, size_t b, size_t e) {
   STAGE_PROLOGUE(b, e);
-  CK(cudaMemcpyAsync(ctx->posH, ctx->pstH, sizeof(float4) * ctx->n, cudaMemcpyDeviceToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->posH, ctx->pstH, sizeof(float4) * (size_t)n, cudaMemcpyDeviceToDevice, ctx->stream));
   return PBF_OK;
 }
 
@@ -2361,6 +2435,129 @@ int pbf_kernel_times(pbf_ctx* ctx, int max_kinds, const char** names, int64_t* l
   }
   if (n_kinds) *n_kinds = i;
   return PBF_OK;
+}
+
+// ---- launch shapes and the autotuner ----
+int pbf_get_tuning(const pbf_ctx* ctx, pbf_tuning* out) {
+  if (!ctx || !out) return PBF_ERR_ARG;
+  *out = ctx->tune;
+  return PBF_OK;
+}
+
+int pbf_set_tuning(pbf_ctx* ctx, const pbf_tuning* t) {
+  if (!ctx || !t) return PBF_ERR_ARG;
+  for (int f = 0; f < PBF_TUNE_FAMILIES; ++f)
+    if (!shape_ok(t->lanes[f], t->block[f]))
+      return fail(ctx, PBF_ERR_ARG, "gather family %d: %d lanes x %d threads is not a supported shape "
+                  "(lanes 4 or 8, block 128 or 256)", f, t->lanes[f], t->block[f]);
+  ctx->tune = *t;
+  drop_graphs(ctx);
+  return update_shapes(ctx);
+}
+
+namespace {
+constexpr int kCandLanes[PBF_TUNE_CANDIDATES] = {4, 4, 8, 8};
+constexpr int kCandBlock[PBF_TUNE_CANDIDATES] = {128, 256, 128, 256};
+
+int family_of(const char* name) {
+  if (!std::strcmp(name, "density_lambda") || !std::strcmp(name, "residual_check")) return PBF_TUNE_DENSITY;
+  if (!std::strcmp(name, "dp_update")) return PBF_TUNE_DELTA_P;
+  if (!std::strcmp(name, "viscosity") || !std::strcmp(name, "viscosity_final")) return PBF_TUNE_VISCOSITY;
+  if (!std::strcmp(name, "vorticity")) return PBF_TUNE_VORTICITY;
+  if (!std::strcmp(name, "apply_vorticity")) return PBF_TUNE_APPLY_VORTICITY;
+  return -1;
+}
+
+// Device copies of the particle state an autotune must hand back unchanged.
+struct StateSnapshot {
+  std::vector<std::pair<void*, void*>> pairs;  // (live buffer, copy)
+  std::vector<size_t> bytes;
+  ~StateSnapshot() {
+    for (auto& p : pairs) cudaFree(p.second);
+  }
+  int take(pbf_ctx* ctx, void* live, size_t nbytes) {
+    void* copy = nullptr;
+    if (cudaMalloc(&copy, nbytes) != cudaSuccess)
+      return fail(ctx, PBF_ERR_CUDA, "autotune: cudaMalloc(%zu bytes) for the state copy failed", nbytes);
+    pairs.emplace_back(live, copy);
+    bytes.push_back(nbytes);
+    CK(cudaMemcpyAsync(copy, live, nbytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    return PBF_OK;
+  }
+  int restore(pbf_ctx* ctx) {
+    for (size_t i = 0; i < pairs.size(); ++i)
+      CK(cudaMemcpyAsync(pairs[i].first, pairs[i].second, bytes[i], cudaMemcpyDeviceToDevice, ctx->stream));
+    return PBF_OK;
+  }
+};
+}  // namespace
+
+int pbf_autotune(pbf_ctx* ctx, int steps, pbf_tuning* chosen, double* ms) {
+  if (!ctx) return PBF_ERR_ARG;
+  if (steps < 1) return fail(ctx, PBF_ERR_ARG, "autotune needs steps >= 1");
+  if (ms) std::fill(ms, ms + PBF_TUNE_CANDIDATES * PBF_TUNE_FAMILIES, 0.0);
+  if (ctx->params.solver == 1 && !ctx->mlp_ready)
+    return fail(ctx, PBF_ERR_STATE, "learned solver without a network: call pbf_mlp_init or pbf_mlp_set");
+  const size_t n = ctx->n;
+  if (n == 0 || ctx->params.exact_math) {  // nothing to tune
+    if (chosen) *chosen = ctx->tune;
+    return PBF_OK;
+  }
+  StateSnapshot snap;
+  int rc;
+  if ((rc = snap.take(ctx, ctx->posH, n * sizeof(float4))) || (rc = snap.take(ctx, ctx->pstH, n * sizeof(float4))) ||
+      (rc = snap.take(ctx, ctx->velH, n * sizeof(float4))) || (rc = snap.take(ctx, ctx->scrH, n * sizeof(float4))) ||
+      (rc = snap.take(ctx, ctx->lamH, n * sizeof(float))) || (rc = snap.take(ctx, ctx->origH, n * sizeof(uint32_t))) ||
+      (rc = snap.take(ctx, ctx->lamsumH, n * sizeof(float))))
+    return rc;
+  const bool timing = ctx->timing;
+  const pbf_tuning before = ctx->tune;
+  double t[PBF_TUNE_CANDIDATES][PBF_TUNE_FAMILIES] = {};
+  ctx->timing = true;
+  auto finish = [&](int code) {
+    ctx->timing = timing;
+    ctx->times.clear();
+    ctx->time_order.clear();
+    ctx->marks_used = 0;
+    ctx->lists_valid = false;
+    drop_graphs(ctx);
+    return code;
+  };
+  for (int c = 0; c < PBF_TUNE_CANDIDATES; ++c) {
+    for (int f = 0; f < PBF_TUNE_FAMILIES; ++f) {
+      ctx->tune.lanes[f] = kCandLanes[c];
+      ctx->tune.block[f] = kCandBlock[c];
+    }
+    if ((rc = update_shapes(ctx)) || (rc = snap.restore(ctx))) return finish(rc);
+    launch_step(ctx);  // untimed: first touch of this shape
+    if ((rc = check_launch(ctx, "autotune")) || (rc = harvest_times(ctx))) return finish(rc);
+    ctx->times.clear();
+    ctx->time_order.clear();
+    for (int i = 0; i < steps; ++i) launch_step(ctx);
+    if ((rc = check_launch(ctx, "autotune")) || (rc = harvest_times(ctx))) return finish(rc);
+    for (const auto& kv : ctx->times) {
+      const int f = family_of(kv.first.c_str());
+      if (f >= 0) t[c][f] += kv.second.second / steps;
+    }
+  }
+  pbf_tuning best = before;
+  for (int f = 0; f < PBF_TUNE_FAMILIES; ++f) {
+    int bc = 0;
+    for (int c = 1; c < PBF_TUNE_CANDIDATES; ++c)
+      if (t[c][f] < t[bc][f]) bc = c;
+    if (t[bc][f] > 0.0) {  // a family the step never launches keeps its shape
+      best.lanes[f] = kCandLanes[bc];
+      best.block[f] = kCandBlock[bc];
+    }
+  }
+  if (ms)
+    for (int c = 0; c < PBF_TUNE_CANDIDATES; ++c)
+      for (int f = 0; f < PBF_TUNE_FAMILIES; ++f) ms[c * PBF_TUNE_FAMILIES + f] = t[c][f];
+  ctx->tune = best;
+  if ((rc = update_shapes(ctx)) || (rc = snap.restore(ctx))) return finish(rc);
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (chosen) *chosen = best;
+  return finish(PBF_OK);
 }
 
 int pbf_launches_per_step(pbf_ctx* ctx, int64_t* out) {

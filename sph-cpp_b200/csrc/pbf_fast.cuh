@@ -47,68 +47,80 @@ inline Fast make_fast(const Dev& d) {
   return f;
 }
 
-// Lane groups: kGL consecutive threads share one particle.  Lane l walks
-// entries l, l + kGL, ... of the particle's row-major list, so one warp-wide
-// load touches kGL consecutive entries of each of 32/kGL lists (one sector
-// each), and the neighbours those entries name are mostly consecutive slots of
-// one bin (coalesced gathers).  Partial sums are combined with shuffles.
+// Lane groups: GL consecutive threads share one particle (GL = 4 or 8, the
+// launch shape the autotuner picks per kernel family; kGL is the default).
+// Lane l walks entries l, l + GL, ... of the particle's row-major list, so one
+// warp-wide load touches GL consecutive entries of each of 32/GL lists, and
+// the neighbours those entries name are mostly consecutive slots of one bin
+// (coalesced gathers).  Partial sums are combined with shuffles.
 constexpr int kGL = 8;
 
 struct Group {
   int b;      // particle slot (0 for threads past the end, which walk nothing)
-  int lane;   // 0 .. kGL-1
+  int lane;   // 0 .. GL-1
   bool live;  // b < n
 };
 
 // Group of this thread in block-sized tile `tile` (grid-stride kernels walk
 // several tiles per block).
+template <int GL = kGL>
 __device__ __forceinline__ Group group_at(int n, int tile) {
   const int gid = tile * blockDim.x + threadIdx.x;
   Group g;
-  g.b = gid / kGL;
-  g.lane = gid % kGL;
+  g.b = gid / GL;
+  g.lane = gid % GL;
   g.live = g.b < n;
   if (!g.live) g.b = 0;
   return g;
 }
 
+template <int GL = kGL>
 __device__ __forceinline__ Group group_of(int n) {
-  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-  Group g;
-  g.b = gid / kGL;
-  g.lane = gid % kGL;
-  g.live = g.b < n;
-  if (!g.live) g.b = 0;
-  return g;
+  return group_at<GL>(n, blockIdx.x);
 }
 
-// Sum over the kGL lanes of a group (every lane of the warp must call it).
+// Tiles of blockDim.x threads covering n particles at GL lanes each.
+template <int GL>
+__device__ __forceinline__ int tiles_of(int n) {
+  return (int)(((size_t)n * GL + blockDim.x - 1) / blockDim.x);
+}
+
+// Sum over the GL lanes of a group (every lane of the warp must call it).
+template <int GL = kGL>
 __device__ __forceinline__ float gsum(float v) {
 #pragma unroll
-  for (int o = kGL / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, kGL);
+  for (int o = GL / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, GL);
   return v;
 }
 
+template <int GL = kGL>
 __device__ __forceinline__ int gor(int v) {
 #pragma unroll
-  for (int o = kGL / 2; o > 0; o >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, o, kGL);
+  for (int o = GL / 2; o > 0; o >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, o, GL);
   return v;
 }
 
-// Walk entries lane, lane + kGL, ... of a list row, kB entries per batch:
+template <int GL = kGL>
+__device__ __forceinline__ float gmin(float v) {
+#pragma unroll
+  for (int o = GL / 2; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o, GL));
+  return v;
+}
+
+// Walk entries lane, lane + GL, ... of a list row, kB entries per batch:
 // the batch's indices are loaded first, then its neighbour records, then the
 // bodies run (predicated past the count), keeping 2*kB loads in flight.
 constexpr int kB = 4;
 
-template <class Body>
+template <int GL = kGL, class Body>
 __device__ __forceinline__ void gwalk1(const int32_t* __restrict__ row, int c, int lane,
                                        const float4* __restrict__ a, Body&& body) {
-  for (int k0 = lane; k0 < c; k0 += kB * kGL) {
+  for (int k0 = lane; k0 < c; k0 += kB * GL) {
     int q[kB];
     float4 v[kB];
 #pragma unroll
     for (int u = 0; u < kB; ++u) {
-      const int k = k0 + u * kGL;
+      const int k = k0 + u * GL;
       q[u] = k < c ? __ldg(row + k) : -1;
     }
 #pragma unroll
@@ -124,17 +136,17 @@ __device__ __forceinline__ void gwalk1(const int32_t* __restrict__ row, int c, i
 // the occupancy) of the one-record walk.
 constexpr int kB2 = 2;
 
-template <class Body>
+template <int GL = kGL, class Body>
 __device__ __forceinline__ void gwalk2(const int32_t* __restrict__ row, int c, int lane,
                                        const float4* __restrict__ a, const float4* __restrict__ bsrc,
                                        Body&& body) {
   constexpr int kB = kB2;
-  for (int k0 = lane; k0 < c; k0 += kB * kGL) {
+  for (int k0 = lane; k0 < c; k0 += kB * GL) {
     int q[kB];
     float4 va[kB], vb[kB];
 #pragma unroll
     for (int u = 0; u < kB; ++u) {
-      const int k = k0 + u * kGL;
+      const int k = k0 + u * GL;
       q[u] = k < c ? __ldg(row + k) : -1;
     }
 #pragma unroll
@@ -152,7 +164,7 @@ __device__ __forceinline__ void gwalk2(const int32_t* __restrict__ row, int c, i
 // (h - r)^2 / r for r < h, else 0 (the Del_Spikey magnitude over r, no norm).
 __device__ __forceinline__ float spikey_over_r(const Fast& F, float d2) {
   const float rinv = rsqrtf(fmaxf(d2, 1e-30f));
-  const float hr = fmaxf(F.h - d2 * rinv, 0.0f);
+  const float hr = fmaxf(fmaf(-d2, rinv, F.h), 0.0f);  // h - r
   return hr * hr * rinv;
 }
 

@@ -302,9 +302,10 @@ struct SolveState {
   uint32_t iterations;  // Jacobi iterations applied this step
 };
 
-// Sum of v over the block (every thread calls it), written by thread 0 to
-// *out.  Warp sums in float, the warps' sums added in double in warp order:
-// the same inputs give the same bits on every run.
+// Sum of v over the block (every thread calls it; blockDim.x a multiple of 32,
+// at most THREADS), written by thread 0 to *out.  Warp sums in float, the
+// warps' sums added in double in warp order: the same inputs give the same
+// bits on every run.
 template <int THREADS>
 __device__ __forceinline__ void block_partial(float v, double* out) {
   __shared__ float warp_sum[THREADS / 32];
@@ -314,8 +315,8 @@ __device__ __forceinline__ void block_partial(float v, double* out) {
   __syncthreads();
   if (threadIdx.x == 0) {
     double s = 0.0;
-#pragma unroll
-    for (int w = 0; w < THREADS / 32; ++w) s += (double)warp_sum[w];
+    const int warps = (int)(blockDim.x >> 5);
+    for (int w = 0; w < warps; ++w) s += (double)warp_sum[w];
     *out = s;
   }
 }

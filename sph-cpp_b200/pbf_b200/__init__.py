@@ -277,3 +277,29 @@ class Particles:
         out = C.c_int64()
         self._check(self._lib.pbf_launches_per_step(self._ctx, C.byref(out)), "launches_per_step")
         return int(out.value)
+
+    # launch shapes of the fast gather kernels: {family: (lanes, block)}
+    def tuning(self) -> dict:
+        t = _abi.PbfTuning()
+        self._check(self._lib.pbf_get_tuning(self._ctx, C.byref(t)), "get_tuning")
+        return t.as_dict()
+
+    def set_tuning(self, shapes: dict) -> None:
+        t = _abi.PbfTuning()
+        cur = self.tuning()
+        cur.update(shapes)
+        for i, f in enumerate(_abi.TUNE_FAMILIES):
+            t.lanes[i], t.block[i] = cur[f]
+        self._check(self._lib.pbf_set_tuning(self._ctx, C.byref(t)), "set_tuning")
+
+    def autotune(self, steps: int = 3) -> tuple[dict, dict]:
+        """Time every candidate shape on `steps` steps of the current state
+        (restored afterwards), apply the fastest per family; returns (chosen,
+        {(lanes, block): {family: ms per step}})."""
+        t = _abi.PbfTuning()
+        nc, nf = len(_abi.TUNE_CANDIDATES), len(_abi.TUNE_FAMILIES)
+        ms = (C.c_double * (nc * nf))()
+        self._check(self._lib.pbf_autotune(self._ctx, int(steps), C.byref(t), ms), "autotune")
+        table = {cand: {f: float(ms[c * nf + i]) for i, f in enumerate(_abi.TUNE_FAMILIES)}
+                 for c, cand in enumerate(_abi.TUNE_CANDIDATES)}
+        return t.as_dict(), table

@@ -31,6 +31,9 @@ MLP_FEATURES = 12
 MLP_PARAMS = 5057
 MLP_NORM = 25
 
+TUNE_FAMILIES = ("density", "delta_p", "viscosity", "vorticity", "apply_vorticity")
+TUNE_CANDIDATES = ((4, 128), (4, 256), (8, 128), (8, 256))  # (lanes per particle, threads per block)
+
 NOALLOC_MAX_PARTICLES = 65536
 NOALLOC_MAX_BINS = 262144
 
@@ -103,6 +106,13 @@ class PbfStats(C.Structure):
         }
 
 
+class PbfTuning(C.Structure):
+    _fields_ = [("lanes", C.c_int * 5), ("block", C.c_int * 5)]
+
+    def as_dict(self) -> dict:
+        return {f: (int(self.lanes[i]), int(self.block[i])) for i, f in enumerate(TUNE_FAMILIES)}
+
+
 _P = C.POINTER
 _vp = C.c_void_p
 _i = C.c_int
@@ -153,6 +163,9 @@ SIGNATURES = {
     "pbf_kernel_times": (_i, [_vp, _i, _P(C.c_char_p), _P(C.c_int64), _P(C.c_double), _P(C.c_int)]),
     "pbf_reset_timing": (_i, [_vp]),
     "pbf_launches_per_step": (_i, [_vp, _P(C.c_int64)]),
+    "pbf_get_tuning": (_i, [_vp, _P(PbfTuning)]),
+    "pbf_set_tuning": (_i, [_vp, _P(PbfTuning)]),
+    "pbf_autotune": (_i, [_vp, _i, _P(PbfTuning), _P(C.c_double)]),
     "pbf_find_neighbors_noalloc": (_i, [_P(PbfParams), _vp, _sz, _vp, _vp, _vp]),
     "pbf_mlp_init": (_i, [_vp, C.c_uint64]),
     "pbf_mlp_get": (_i, [_vp, _vp, _vp]),
