@@ -58,6 +58,7 @@ def parse_args():
     ap.add_argument("--no-learned", action="store_true", help="skip the plain-vs-learned comparison")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU baseline sample")
     ap.add_argument("--no-autotune", action="store_true", help="default launch shapes instead of the autotuner's")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 64-scene batch measurement")
     return ap.parse_args()
 
 
@@ -286,6 +287,81 @@ def learned_comparison(scene_name: str, steps: int, warmup: int, target: float =
             "network": {k: meta.get(k) for k in ("trajectories", "steps", "batch", "lr", "final_loss")}}
 
 
+# ---------------------------------------------------------------- batched scenes
+def batched_run(steps: int = 200, autotune: bool = True) -> dict:
+    """The 64-scene batch (make_batch: counts log-uniform in [4096, 262144])
+    advanced `steps` steps from its initial state by ONE graph launch
+    (pbf_step(ctx, steps); the graph is captured by an untimed run of the same
+    call first), against the same scenes and the same steps as 64
+    single-scene contexts, each replaying its own one-step graph on its own
+    stream (the streams run concurrently)."""
+    import numpy as np
+    import torch
+    from pbf_b200 import Particles, make_batch
+    b = make_batch()
+    x0 = b.positions()
+    out = {"workload": f"{b.name}: {len(b.scenes)} scenes, {b.n} particles (counts {min(b.counts)}.."
+                       f"{max(b.counts)}), K = {b.scenes[0].solve_steps}, eps {b.scenes[0].lambda_epsilon}"}
+    with Particles.batch(b) as g:
+        g.upload(x0)
+        g.step(3)
+        tuning = g.autotune(2)[0] if autotune else g.tuning()
+        g.upload(x0)
+        g.step(steps)          # captures the steps-step graph (untimed)
+        g.upload(x0)
+        g.sync()
+        stream = torch.cuda.ExternalStream(g.stream_handle())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        g.step(steps)
+        e1.record(stream)
+        e1.synchronize()
+        t = e0.elapsed_time(e1) / 1e3
+        errs = [g.scene_stats(i)["mean_density_error"] for i in range(len(b.scenes))]
+        flags = g.stats()["error_flags"]
+        launches = g.launches_per_step()
+    out.update({"value": b.n * steps / t, "unit": UNIT, "steps": steps, "ms_per_step": 1e3 * t / steps,
+                "graph_launches": 1, "kernel_launches_per_step": launches, "tuning": tuning,
+                "scene_mean_density_error": {"min": float(np.min(errs)), "max": float(np.max(errs))},
+                "error_flags": flags})
+    # the same scenes as independent contexts
+    ctxs = []
+    try:
+        for sc in b.scenes:
+            c = Particles(sc.params(), sc.n)
+            c.set_tuning(tuning)
+            c.upload(sc.positions())
+            c.step(1)  # captures the one-step graph
+            c.upload(sc.positions())
+            ctxs.append(c)
+        torch.cuda.synchronize()
+        for c in ctxs:
+            c.sync()
+        s0 = torch.cuda.ExternalStream(ctxs[0].stream_handle())
+        e0 = torch.cuda.Event(enable_timing=True)
+        e0.record(s0)
+        for c in ctxs:  # every context's stream starts after e0
+            torch.cuda.ExternalStream(c.stream_handle()).wait_event(e0)
+        for _ in range(steps):
+            for c in ctxs:
+                c.step(1)
+        ends = []
+        for c in ctxs:
+            e = torch.cuda.Event(enable_timing=True)
+            e.record(torch.cuda.ExternalStream(c.stream_handle()))
+            ends.append(e)
+        for e in ends:
+            e.synchronize()
+        ts = max(e0.elapsed_time(e) for e in ends) / 1e3
+    finally:
+        for c in ctxs:
+            c.close()
+    out["independent_contexts"] = {"value": b.n * steps / ts, "ms_per_step": 1e3 * ts / steps,
+                                   "steps": steps, "graph_launches_per_step": len(b.scenes)}
+    out["speedup_vs_independent"] = out["value"] / out["independent_contexts"]["value"]
+    return out
+
+
 # ---------------------------------------------------------------- main
 def main():
     args = parse_args()
@@ -419,6 +495,13 @@ def main():
         except Exception as e:  # reported, never fatal for the GPU line
             learned = {"error": str(e)}
 
+    batched = None
+    if rank == 0 and world == 1 and not args.no_batched:
+        try:
+            batched = batched_run(autotune=not args.no_autotune)
+        except Exception as e:  # reported, never fatal for the GPU line
+            batched = {"error": str(e)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -458,6 +541,7 @@ def main():
                         "finite": ok},
             "clocks": clk.summary(),
             "learned_vs_plain": learned,
+            "batched": batched,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)

@@ -233,6 +233,32 @@ int pbf_reset_timing(pbf_ctx* ctx);
 /* Number of kernel launches one pbf_step(ctx, 1) issues. */
 int pbf_launches_per_step(pbf_ctx* ctx, int64_t* out);
 
+/* ---- batched scenes ----
+ * No counterpart in the reference (one scene per process there).  One context
+ * advances `nscenes` independent scenes in the same launches: each scene has
+ * its own box (boundary_min/max, with the single-scene rules: min >= 0, the
+ * grid must cover the box) and its own bin grid; all share the physics of the
+ * parameter block, whose boundary fields are ignored.  Particles are
+ * uploaded, downloaded and indexed as the scenes concatenated in order (scene
+ * i holds particles [sum of the counts before i, + count_i)); pbf_upload takes
+ * exactly the sum of the counts.  The bin keys of scene i follow those of
+ * scenes 0..i-1, so sorted keys and bin bounds (pbf_get_bins) are in that
+ * global key space.  A scene's bins, lists and particle arithmetic are those
+ * of a context created for it alone with the same launch shapes.  The learned
+ * solver's residual check is the batch's mean.  pbf_set_params keeps the
+ * scenes' boxes. */
+typedef struct {
+  float boundary_min[3];
+  float boundary_max[3];
+  size_t count;  /* particles of the scene */
+} pbf_scene;
+int pbf_create_batch(const pbf_params* p, const pbf_scene* scenes, int nscenes, pbf_ctx** out);
+/* Scenes of a batch context; 0 for a single-scene context. */
+int pbf_scene_count(const pbf_ctx* ctx);
+/* pbf_stats over one scene's particles (scene 0 of a single-scene context is
+ * the whole set); the error flags are reported, not cleared. */
+int pbf_scene_stats(pbf_ctx* ctx, int scene, pbf_stats_t* out);
+
 /* ---- launch shapes of the fast-math gather kernels ----
  * No counterpart in the reference (its loops are OpenMP for_each_index).
  * Each family of gather kernels runs with `lanes` threads per particle

@@ -123,19 +123,19 @@ __global__ void k_external(Dev P, int n, float4* vel) {
 }
 
 // predict_positions (particles.h:275-287): x* = BC(x + v*dt)
-__device__ __forceinline__ float3 predict(const Dev& P, float4 x, float4 v) {
+__device__ __forceinline__ float3 predict(const Dev& P, const pbf::Region& R, float4 x, float4 v) {
   float3 s;
   s.x = pbf::xadd(x.x, pbf::xmul(v.x, P.dt));
   s.y = pbf::xadd(x.y, pbf::xmul(v.y, P.dt));
   s.z = pbf::xadd(x.z, pbf::xmul(v.z, P.dt));
-  return pbf::boundary(P, s);
+  return pbf::boundary(P, R, s);
 }
 
 __global__ void k_predict(Dev P, int n, const float4* __restrict__ pos, const float4* __restrict__ vel,
                           float4* pst) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= n) return;
-  const float3 s = predict(P, pos[a], vel[a]);
+  const float3 s = predict(P, pbf::region_of(P, a), pos[a], vel[a]);
   pst[a] = make_float4(s.x, s.y, s.z, 0.0f);
 }
 
@@ -146,7 +146,7 @@ __global__ void k_hash(Dev P, int n, const float4* __restrict__ pst, uint32_t* k
   if (a >= n) return;
   const float4 s = pst[a];
   uint32_t k;
-  if (!pbf::bin_of(P, s.x, s.y, s.z, k)) atomicOr(err, PBF_FLAG_KEY_RANGE);
+  if (!pbf::bin_of(P, pbf::region_of(P, a), s.x, s.y, s.z, k)) atomicOr(err, PBF_FLAG_KEY_RANGE);
   key[a] = k;
   rank[a] = atomicAdd(&cell_count[k], 1u);
 }
@@ -160,10 +160,11 @@ __global__ void k_ext_predict_hash(Dev P, int n, const float4* __restrict__ pos,
   float4 v = vel[a];
   v.y = pbf::xadd(v.y, P.gdt);
   vel[a] = v;
-  const float3 s = predict(P, pos[a], v);
+  const pbf::Region R = pbf::region_of(P, a);
+  const float3 s = predict(P, R, pos[a], v);
   pst[a] = make_float4(s.x, s.y, s.z, 0.0f);
   uint32_t k;
-  if (!pbf::bin_of(P, s.x, s.y, s.z, k)) atomicOr(err, PBF_FLAG_KEY_RANGE);
+  if (!pbf::bin_of(P, R, s.x, s.y, s.z, k)) atomicOr(err, PBF_FLAG_KEY_RANGE);
   key[a] = k;
   rank[a] = atomicAdd(&cell_count[k], 1u);
 }
@@ -337,6 +338,7 @@ __global__ void __launch_bounds__(kFillBlock) k_fill2(Dev P, int n, size_t strid
   const float4 xp = pst[b];
   const int cap = P.cap;
   const float s = P.s;
+  const pbf::Region R = pbf::region_of(P, b);
   int32_t* row = nbr + (size_t)b * stride;
   // calculate_neighbor_indices (neighbors.h:172-185): the bin of coord + i*s
   // per axis for i = -1, 0, 1, in the reference's float operations.  The 27
@@ -366,7 +368,7 @@ __global__ void __launch_bounds__(kFillBlock) k_fill2(Dev P, int n, size_t strid
       for (int k = 0; k < 3; k++) {
         const float ez = k == 0 ? lo[2] : (k == 2 ? hi[2] : 0.f);
         const int cx = bx[i], cy = by[j], cz = bz[k];
-        if (!finite || cx < 0 || cy < 0 || cz < 0 || cx >= P.dimx || cy >= P.dimy || cz >= P.dimz) {
+        if (!finite || cx < 0 || cy < 0 || cz < 0 || cx >= R.dimx || cy >= R.dimy || cz >= R.dimz) {
           atomicOr(err, PBF_FLAG_KEY_RANGE);
           continue;
         }
@@ -374,7 +376,8 @@ __global__ void __launch_bounds__(kFillBlock) k_fill2(Dev P, int n, size_t strid
         if (cx == bx[1] + i - 1 && cy == by[1] + j - 1 && cz == bz[1] + k - 1 &&
             ex * ex + ey * ey + ez * ez > P.s2)
           continue;
-        const uint32_t nb = (uint32_t)(P.dimx * P.dimy) * (uint32_t)cz + ((uint32_t)cy * (uint32_t)P.dimx + (uint32_t)cx);
+        const uint32_t nb =
+            R.key0 + (uint32_t)(R.dimx * R.dimy) * (uint32_t)cz + ((uint32_t)cy * (uint32_t)R.dimx + (uint32_t)cx);
         const uint32_t q1 = cell_start[nb + 1];
         for (uint32_t q = cell_start[nb]; q < q1; ++q) {
           const float4 xq = pst[q];
@@ -602,7 +605,7 @@ __device__ __forceinline__ void density_lambda_tile(int tile, const Dev& P, cons
   if (MODE == kDlRecord) {
     if (io.first) {
       float f[pbf::kMlpIn];
-      pbf::raw_features(P, F, f, c, rho, sc, g2, (int)nh, io.lamprev[b], vel[b], xp);
+      pbf::raw_features(P, pbf::region_of(P, b), F, f, c, rho, sc, g2, (int)nh, io.lamprev[b], vel[b], xp);
 #pragma unroll
       for (int k = 0; k < pbf::kMlpIn; ++k) io.feats[(size_t)b * pbf::kMlpIn + k] = f[k];
       io.lamsum[b] = lam[b];
@@ -661,7 +664,7 @@ __global__ void __launch_bounds__(kBlock) kl_features(Dev P, Fast F, pbf::MlpDev
   const float nh = S.nh;
   const float4 v = vel[b];
   float f[pbf::kMlpIn];
-  pbf::raw_features(P, F, f, c, rho, sc, g2, (int)nh, lamprev[b], v, xp);
+  pbf::raw_features(P, pbf::region_of(P, b), F, f, c, rho, sc, g2, (int)nh, lamprev[b], v, xp);
   uint32_t row[pbf::kMlpInPad / 2];
 #pragma unroll
   for (int k = 0; k < pbf::kMlpIn; k += 2)
@@ -773,7 +776,8 @@ __global__ void k_update_xs(Dev P, int n, float4* pst, const float4* __restrict_
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= n) return;
   const float4 x = pst[b], d = scr[b];
-  const float3 s = pbf::boundary(P, make_float3(pbf::xadd(x.x, d.x), pbf::xadd(x.y, d.y), pbf::xadd(x.z, d.z)));
+  const float3 s = pbf::boundary(P, pbf::region_of(P, b),
+                                 make_float3(pbf::xadd(x.x, d.x), pbf::xadd(x.y, d.y), pbf::xadd(x.z, d.z)));
   pst[b] = make_float4(s.x, s.y, s.z, 0.0f);
 }
 
@@ -823,7 +827,8 @@ __global__ void __launch_bounds__(kBlock) k_dp_update(Dev P, int n, size_t strid
     }
   }
   const float dx = pbf::M<X>(P.inv_rho0, dp.x), dy = pbf::M<X>(P.inv_rho0, dp.y), dz = pbf::M<X>(P.inv_rho0, dp.z);
-  const float3 s = pbf::boundary(P, make_float3(pbf::xadd(xp.x, dx), pbf::xadd(xp.y, dy), pbf::xadd(xp.z, dz)));
+  const float3 s = pbf::boundary(P, pbf::region_of(P, b),
+                                 make_float3(pbf::xadd(xp.x, dx), pbf::xadd(xp.y, dy), pbf::xadd(xp.z, dz)));
   const float4 ns = make_float4(s.x, s.y, s.z, 0.0f);
   pst[b] = ns;
   if (LAST) {
@@ -1026,7 +1031,8 @@ __device__ __forceinline__ void dp_update_tile(int tile, const Dev& P, const Fas
   az = pbf::gsum<GL>(az);
   if (!G.live || G.lane != 0) return;
   if (lamsum) lamsum[b] += xp.w;
-  const float3 s = pbf::boundary(P, make_float3(pbf::xadd(xp.x, F.dp_scale * ax), pbf::xadd(xp.y, F.dp_scale * ay),
+  const float3 s = pbf::boundary(P, pbf::region_of(P, b),
+                                 make_float3(pbf::xadd(xp.x, F.dp_scale * ax), pbf::xadd(xp.y, F.dp_scale * ay),
                                                 pbf::xadd(xp.z, F.dp_scale * az)));
   const float4 ns = make_float4(s.x, s.y, s.z, 0.0f);
   pst[b] = ns;
@@ -1152,14 +1158,15 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-__global__ void __launch_bounds__(kBlock) k_stats(Dev P, int n, size_t stride, const int32_t* __restrict__ nbr,
+__global__ void __launch_bounds__(kBlock) k_stats(Dev P, int b0, int b1, size_t stride,
+                                                  const int32_t* __restrict__ nbr,
                                                   const int32_t* __restrict__ cnt, const float4* __restrict__ pst,
                                                   const float4* __restrict__ pos, const float4* __restrict__ vel,
                                                   double* acc, unsigned long long* maxerr,
                                                   unsigned long long* hits) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = b0 + blockIdx.x * blockDim.x + threadIdx.x;
   double e = 0.0, ke = 0.0, cx = 0.0, cy = 0.0, cz = 0.0, nn = 0.0;
-  if (b < n) {
+  if (b < b1) {
     const float4 xp = pst[b];
     const int c = cnt[b];
     float d = pbf::xmul(P.m, P.W0);
@@ -1211,7 +1218,9 @@ struct pbf_ctx {
   size_t capacity = 0, n = 0;
   int64_t dims[3] = {0, 0, 0};
   int nbins = 0, nscan_parts = 0;
-  size_t lstride = 0;  // list row stride: neighbor_cap rounded up to 8 (whole 32-byte sectors)
+  int nbins_cap = 0;   // bins the cell arrays were allocated for
+  size_t lstride = 0;
+  size_t lstride_cap = 0;  // list row stride the list buffer was allocated for  // list row stride: neighbor_cap rounded up to 8 (whole 32-byte sectors)
   int device = 0;
   cudaStream_t stream = nullptr;
   bool lists_valid = false;
@@ -1246,6 +1255,14 @@ struct pbf_ctx {
   int sms = 148;
   int pgrid_check = 148, pgrid_dp = 148;
   int partials_cap = 0;
+
+  // batch of scenes (empty: one scene, the parameter block's box); the device
+  // copies back Dev::scenes and Dev::scene_first
+  std::vector<pbf_scene> scenes;
+  std::vector<pbf::Region> regions;
+  std::vector<uint32_t> scene_first;
+  pbf::Region* d_regions = nullptr;
+  uint32_t* d_scene_first = nullptr;
 
   std::map<int, cudaGraphExec_t> graphs;
   std::vector<void*> allocations;
@@ -1379,6 +1396,66 @@ int make_dev(pbf_ctx* ctx, const pbf_params& p, Dev& d, int64_t dims[3]) {
   d.dimz = (int)dims[2];
   d.nbins = (int)(dims[0] * dims[1] * dims[2]);
   d.cap = p.neighbor_cap;
+  return PBF_OK;
+}
+
+// Dev of a batch: every scene validated as a single scene with its own box;
+// the physics of scene 0 (the same for all: only the box differs), the total
+// bin count, the widest bin-skip margin, and the host tables of regions and
+// first slots.
+int make_dev_batch(pbf_ctx* ctx, const pbf_params& p, const std::vector<pbf_scene>& sc, Dev& d,
+                   std::vector<pbf::Region>& regions, std::vector<uint32_t>& first) {
+  regions.clear();
+  first.clear();
+  int64_t total = 0;
+  size_t slot = 0;
+  float skip = 0.0f;
+  for (size_t i = 0; i < sc.size(); ++i) {
+    pbf_params q = p;
+    for (int a = 0; a < 3; ++a) {
+      q.boundary_min[a] = sc[i].boundary_min[a];
+      q.boundary_max[a] = sc[i].boundary_max[a];
+    }
+    Dev di;
+    int64_t dims[3];
+    if (int rc = make_dev(ctx, q, di, dims)) {
+      const std::string why = ctx->error;
+      return fail(ctx, rc, "scene %zu: %s", i, why.c_str());
+    }
+    if (i == 0) d = di;
+    pbf::Region r;
+    for (int a = 0; a < 3; ++a) {
+      r.bmin[a] = q.boundary_min[a];
+      r.bmax[a] = q.boundary_max[a];
+    }
+    r.dimx = di.dimx;
+    r.dimy = di.dimy;
+    r.dimz = di.dimz;
+    r.key0 = (uint32_t)total;
+    regions.push_back(r);
+    first.push_back((uint32_t)slot);
+    total += di.nbins;
+    slot += sc[i].count;
+    skip = std::max(skip, di.skip_eps);
+    if (total >= 2147483647ll) return fail(ctx, PBF_ERR_PARAMS, "the batch's grids exceed 2^31 bins");
+  }
+  first.push_back((uint32_t)slot);
+  d.nbins = (int)total;
+  d.skip_eps = skip;
+  d.nscenes = (int)sc.size();
+  return PBF_OK;
+}
+
+// Copy the batch's tables to the device and point Dev at them.
+int upload_scenes(pbf_ctx* ctx) {
+  if (ctx->scenes.empty()) return PBF_OK;
+  CK(cudaMemcpy(ctx->d_regions, ctx->regions.data(), ctx->regions.size() * sizeof(pbf::Region),
+                cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->d_scene_first, ctx->scene_first.data(), ctx->scene_first.size() * sizeof(uint32_t),
+                cudaMemcpyHostToDevice));
+  ctx->dev.scenes = ctx->d_regions;
+  ctx->dev.scene_first = ctx->d_scene_first;
+  ctx->dev.nscenes = (int)ctx->scenes.size();
   return PBF_OK;
 }
 
@@ -1772,7 +1849,7 @@ extern "C" {
 const char* pbf_create_error(void) { return g_create_error.c_str(); }
 const char* pbf_last_error(const pbf_ctx* ctx) { return ctx ? ctx->error.c_str() : g_create_error.c_str(); }
 
-int pbf_create(const pbf_params* p, size_t capacity, pbf_ctx** out) {
+static int create_ctx(const pbf_params* p, size_t capacity, const pbf_scene* scenes, int nscenes, pbf_ctx** out) {
   pbf_ctx* ctx = nullptr;
   if (!p || !out) return fail(nullptr, PBF_ERR_ARG, "null argument");
   *out = nullptr;
@@ -1780,7 +1857,9 @@ int pbf_create(const pbf_params* p, size_t capacity, pbf_ctx** out) {
     return fail(nullptr, PBF_ERR_ARG, "capacity must be in [1, 2^31)");
   ctx = new pbf_ctx();
   ctx->params = *p;
-  int rc = make_dev(ctx, *p, ctx->dev, ctx->dims);
+  if (scenes) ctx->scenes.assign(scenes, scenes + nscenes);
+  int rc = scenes ? make_dev_batch(ctx, *p, ctx->scenes, ctx->dev, ctx->regions, ctx->scene_first)
+                  : make_dev(ctx, *p, ctx->dev, ctx->dims);
   if (rc) {
     g_create_error = ctx->error;
     delete ctx;
@@ -1789,6 +1868,7 @@ int pbf_create(const pbf_params* p, size_t capacity, pbf_ctx** out) {
   ctx->fast = pbf::make_fast(ctx->dev);
   ctx->capacity = capacity;
   ctx->nbins = ctx->dev.nbins;
+  ctx->nbins_cap = ctx->nbins;
   ctx->nscan_parts = (int)(((size_t)ctx->nbins + 1 + kScanTile - 1) / kScanTile);
   auto bail = [&](int code) {
     g_create_error = ctx->error;
@@ -1815,6 +1895,7 @@ int pbf_create(const pbf_params* p, size_t capacity, pbf_ctx** out) {
   }
   const size_t C = capacity;
   ctx->lstride = ((size_t)p->neighbor_cap + 7) / 8 * 8;
+  ctx->lstride_cap = ctx->lstride;
   const size_t cap = ctx->lstride;
   if ((rc = dalloc(ctx, &ctx->posH, C)) || (rc = dalloc(ctx, &ctx->pstH, C)) || (rc = dalloc(ctx, &ctx->velH, C)) ||
       (rc = dalloc(ctx, &ctx->scrH, C)) || (rc = dalloc(ctx, &ctx->posS, C)) || (rc = dalloc(ctx, &ctx->pstS, C)) ||
@@ -1839,6 +1920,10 @@ int pbf_create(const pbf_params* p, size_t capacity, pbf_ctx** out) {
       (rc = dalloc(ctx, &ctx->mlp_loss, 1)) || (rc = dalloc(ctx, &ctx->w1b, pbf::kMlpH * pbf::kMlpInPad)) ||
       (rc = dalloc(ctx, &ctx->w2b, pbf::kMlpH * pbf::kMlpH)) || (rc = dalloc(ctx, &ctx->w2tb, pbf::kMlpH * pbf::kMlpH)))
     return bail(rc);
+  if (!ctx->scenes.empty() &&
+      ((rc = dalloc(ctx, &ctx->d_regions, ctx->regions.size())) ||
+       (rc = dalloc(ctx, &ctx->d_scene_first, ctx->scene_first.size())) || (rc = upload_scenes(ctx))))
+    return bail(rc);
   if (cudaMemsetAsync(ctx->lamsumH, 0, C * sizeof(float), ctx->stream) != cudaSuccess ||
       cudaMemsetAsync(ctx->state, 0, sizeof(pbf::SolveState), ctx->stream) != cudaSuccess) {
     fail(ctx, PBF_ERR_CUDA, "initialisation failed");
@@ -1851,6 +1936,18 @@ int pbf_create(const pbf_params* p, size_t capacity, pbf_ctx** out) {
   }
   *out = ctx;
   return PBF_OK;
+}
+
+int pbf_create(const pbf_params* p, size_t capacity, pbf_ctx** out) {
+  return create_ctx(p, capacity, nullptr, 0, out);
+}
+
+int pbf_create_batch(const pbf_params* p, const pbf_scene* scenes, int nscenes, pbf_ctx** out) {
+  if (!scenes || nscenes < 1) return fail(nullptr, PBF_ERR_ARG, "a batch needs at least one scene");
+  size_t total = 0;
+  for (int i = 0; i < nscenes; ++i) total += scenes[i].count;
+  if (total == 0) return fail(nullptr, PBF_ERR_ARG, "a batch needs at least one particle");
+  return create_ctx(p, total, scenes, nscenes, out);
 }
 
 void pbf_destroy(pbf_ctx* ctx) {
@@ -1869,19 +1966,29 @@ void pbf_destroy(pbf_ctx* ctx) {
 int pbf_set_params(pbf_ctx* ctx, const pbf_params* p) {
   if (!ctx || !p) return PBF_ERR_ARG;
   Dev d;
-  int64_t dims[3];
-  int rc = make_dev(ctx, *p, d, dims);
+  int64_t dims[3] = {0, 0, 0};
+  std::vector<pbf::Region> regions;
+  std::vector<uint32_t> first;
+  const bool batch = !ctx->scenes.empty();
+  int rc = batch ? make_dev_batch(ctx, *p, ctx->scenes, d, regions, first) : make_dev(ctx, *p, d, dims);
   if (rc) return rc;
-  if (d.nbins > ctx->nbins || p->neighbor_cap > ctx->params.neighbor_cap)
+  const size_t lstride = ((size_t)p->neighbor_cap + 7) / 8 * 8;
+  if (d.nbins > ctx->nbins_cap || lstride > ctx->lstride_cap)
     return fail(ctx, PBF_ERR_PARAMS, "new parameters need a larger grid or neighbor cap than allocated");
-  if (d.nbins != ctx->nbins || p->neighbor_cap != ctx->params.neighbor_cap) ctx->lists_valid = false;
+  if (d.nbins != ctx->nbins || p->neighbor_cap != ctx->params.neighbor_cap || d.s != ctx->dev.s)
+    ctx->lists_valid = false;
   ctx->params = *p;
   ctx->dev = d;
   ctx->fast = pbf::make_fast(d);
-  ctx->lstride = ((size_t)p->neighbor_cap + 7) / 8 * 8;
+  ctx->lstride = lstride;
   std::memcpy(ctx->dims, dims, sizeof(dims));
   ctx->nbins = d.nbins;
   ctx->nscan_parts = (int)(((size_t)ctx->nbins + 1 + kScanTile - 1) / kScanTile);
+  if (batch) {
+    ctx->regions = regions;
+    ctx->scene_first = first;
+    if ((rc = upload_scenes(ctx))) return rc;
+  }
   drop_graphs(ctx);
   return PBF_OK;
 }
@@ -1899,6 +2006,9 @@ int pbf_upload(pbf_ctx* ctx, const float* x, const float* v, size_t n) {
   if (!ctx || (!x && n)) return ctx ? fail(ctx, PBF_ERR_ARG, "null positions") : PBF_ERR_ARG;
   if (n > ctx->capacity)
     return fail(ctx, PBF_ERR_CAPACITY, "Not enough capacity: %zu particles > capacity %zu", n, ctx->capacity);
+  if (!ctx->scenes.empty() && n != ctx->scene_first.back())
+    return fail(ctx, PBF_ERR_ARG, "a batch of %zu scenes takes exactly %u particles (its scenes' counts), got %zu",
+                ctx->scenes.size(), ctx->scene_first.back(), n);
   if (n != ctx->n) drop_graphs(ctx);
   ctx->n = n;
   ctx->lists_valid = false;
@@ -2212,18 +2322,20 @@ int pbf_get_bins(pbf_ctx* ctx, uint32_t* sorted_keys, uint32_t* sorted_ids, uint
   return PBF_OK;
 }
 
-int pbf_stats(pbf_ctx* ctx, pbf_stats_t* out) {
-  if (!ctx || !out) return PBF_ERR_ARG;
+// Statistics over the particles in slots [b0, b1) (one scene of a batch, or
+// all); the error flags are read, and cleared when `clear_flags`.
+static int stats_range(pbf_ctx* ctx, size_t b0, size_t b1, bool clear_flags, pbf_stats_t* out) {
   std::memset(out, 0, sizeof(*out));
-  out->n = ctx->n;
+  out->n = b1 - b0;
   if (int rc = need_lists(ctx)) return rc;
   cudaStream_t s = ctx->stream;
   CK(cudaMemsetAsync(ctx->acc, 0, 8 * sizeof(double), s));
   CK(cudaMemsetAsync(ctx->maxerr, 0, sizeof(unsigned long long), s));
   CK(cudaMemsetAsync(ctx->hits, 0, sizeof(unsigned long long), s));
-  if (ctx->n) {
-    k_stats<<<blocks_for(ctx->n), kBlock, 0, s>>>(ctx->dev, (int)ctx->n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH,
-                                                  ctx->posH, ctx->velH, ctx->acc, ctx->maxerr, ctx->hits);
+  if (b1 > b0) {
+    k_stats<<<blocks_for(b1 - b0), kBlock, 0, s>>>(ctx->dev, (int)b0, (int)b1, ctx->lstride, ctx->nbr, ctx->cnt,
+                                                   ctx->pstH, ctx->posH, ctx->velH, ctx->acc, ctx->maxerr,
+                                                   ctx->hits);
     if (int rc = check_launch(ctx, "stats")) return rc;
   }
   double acc[8];
@@ -2233,9 +2345,9 @@ int pbf_stats(pbf_ctx* ctx, pbf_stats_t* out) {
   CK(cudaMemcpyAsync(&mx, ctx->maxerr, sizeof(mx), cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(&hits, ctx->hits, sizeof(hits), cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(&err, ctx->err, sizeof(err), cudaMemcpyDeviceToHost, s));
-  CK(cudaMemsetAsync(ctx->err, 0, sizeof(uint32_t), s));
+  if (clear_flags) CK(cudaMemsetAsync(ctx->err, 0, sizeof(uint32_t), s));
   CK(cudaStreamSynchronize(s));
-  const double n = ctx->n ? (double)ctx->n : 1.0;
+  const double n = b1 > b0 ? (double)(b1 - b0) : 1.0;
   double maxerr;
   std::memcpy(&maxerr, &mx, sizeof(double));
   out->mean_density_error = acc[0] / n;
@@ -2257,6 +2369,25 @@ int pbf_stats(pbf_ctx* ctx, pbf_stats_t* out) {
     out->solver_residual = -1.0;
   }
   return PBF_OK;
+}
+
+int pbf_stats(pbf_ctx* ctx, pbf_stats_t* out) {
+  if (!ctx || !out) return PBF_ERR_ARG;
+  return stats_range(ctx, 0, ctx->n, true, out);
+}
+
+int pbf_scene_count(const pbf_ctx* ctx) { return ctx ? (int)ctx->scenes.size() : 0; }
+
+int pbf_scene_stats(pbf_ctx* ctx, int scene, pbf_stats_t* out) {
+  if (!ctx || !out) return PBF_ERR_ARG;
+  if (ctx->scenes.empty()) {
+    if (scene != 0) return fail(ctx, PBF_ERR_ARG, "scene %d of a single-scene context", scene);
+    return stats_range(ctx, 0, ctx->n, false, out);
+  }
+  if (scene < 0 || scene >= (int)ctx->scenes.size())
+    return fail(ctx, PBF_ERR_ARG, "scene %d out of [0, %zu)", scene, ctx->scenes.size());
+  if (ctx->n == 0) return stats_range(ctx, 0, 0, false, out);
+  return stats_range(ctx, ctx->scene_first[scene], ctx->scene_first[scene + 1], false, out);
 }
 
 // ---- learned warm start ----
@@ -2611,7 +2742,7 @@ __global__ void k_noalloc_hash(Dev P, int n, const float* __restrict__ x, uint32
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= n) return;
   uint32_t k;
-  if (!pbf::bin_of(P, x[3 * (size_t)a], x[3 * (size_t)a + 1], x[3 * (size_t)a + 2], k))
+  if (!pbf::bin_of(P, pbf::region_of(P, 0), x[3 * (size_t)a], x[3 * (size_t)a + 1], x[3 * (size_t)a + 2], k))
     atomicOr(err, PBF_FLAG_KEY_RANGE);
   key[a] = k;
   ident[a] = (uint32_t)a;
@@ -2647,7 +2778,7 @@ __global__ void __launch_bounds__(kBlock) k_noalloc_fill(Dev P, int n, const flo
       for (int k = -1; k < 2 && count < cap; k++) {
         const float cz = pbf::xadd(xp.z, pbf::xmul((float)k, P.s));
         uint32_t nb;
-        if (!pbf::bin_of(P, cx, cy, cz, nb)) {
+        if (!pbf::bin_of(P, pbf::region_of(P, 0), cx, cy, cz, nb)) {
           atomicOr(err, PBF_FLAG_KEY_RANGE);
           continue;
         }

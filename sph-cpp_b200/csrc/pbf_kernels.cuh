@@ -15,6 +15,17 @@
 
 namespace pbf {
 
+// Box and bin grid of one scene.  A context advances one scene (the box and
+// grid of Dev itself) or a batch of independent scenes, each with its own box
+// and grid; the bin keys of a batch's scene i start at key0, so the sort by
+// key keeps every scene's particles in one slot range, [first[i],
+// first[i+1]), in every order the step uses.
+struct Region {
+  float bmin[3], bmax[3];
+  int dimx, dimy, dimz;
+  uint32_t key0;
+};
+
 // Per-launch constant block (kernel argument, < 4 KB).
 struct Dev {
   float dt, gdt;  // time step; g*dt rounded in float (particles.h:264-268)
@@ -30,7 +41,36 @@ struct Dev {
   double h_eps;   // smoothing_radius * 0.000001 in double (particles.h:420)
   float skip_eps; // margin of the conservative bin skip in the list fill
   int dimx, dimy, dimz, nbins, cap;
+  // batch of scenes (nscenes > 0): per-scene regions and first slots
+  // (nscenes + 1 entries); nscenes = 0 is the single scene of the fields above
+  const Region* scenes;
+  const uint32_t* scene_first;
+  int nscenes;
 };
+
+// The region of the particle in `slot` (any order the step uses).
+__device__ __forceinline__ Region region_of(const Dev& P, int slot) {
+  if (P.nscenes == 0) {
+    Region r;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      r.bmin[a] = P.bmin[a];
+      r.bmax[a] = P.bmax[a];
+    }
+    r.dimx = P.dimx;
+    r.dimy = P.dimy;
+    r.dimz = P.dimz;
+    r.key0 = 0u;
+    return r;
+  }
+  int lo = 0, hi = P.nscenes - 1;  // the last scene whose first slot is <= slot
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(P.scene_first + mid) <= (uint32_t)slot) lo = mid;
+    else hi = mid - 1;
+  }
+  return P.scenes[lo];
+}
 
 // ---------------- exact scalar helpers ----------------
 __device__ __forceinline__ float xadd(float a, float b) { return __fadd_rn(a, b); }
@@ -104,8 +144,9 @@ template <bool X> __device__ __forceinline__ float c_spline(const Dev& P, float 
   return __fmul_rn(v, r);
 }
 
-// apply_boundary_conditions (particles.h:510-526), always exact.
-__device__ __forceinline__ float3 boundary(const Dev& P, float3 p) {
+// apply_boundary_conditions (particles.h:510-526), always exact; the mover
+// sphere is shared, the box is the particle's scene's.
+__device__ __forceinline__ float3 boundary(const Dev& P, const Region& R, float3 p) {
   const float dx = xsub(p.x, P.mc[0]), dy = xsub(p.y, P.mc[1]), dz = xsub(p.z, P.mc[2]);
   const float dr2 = mag2<true>(dx, dy, dz);
   if (dr2 < P.mr2) {
@@ -116,9 +157,9 @@ __device__ __forceinline__ float3 boundary(const Dev& P, float3 p) {
     p.z = xadd(p.z, xdiv(xmul(a, dz), dr));
   }
   // clamp_in_place (utility_math.h:52-57)
-  p.x = p.x < P.bmin[0] ? P.bmin[0] : (p.x > P.bmax[0] ? P.bmax[0] : p.x);
-  p.y = p.y < P.bmin[1] ? P.bmin[1] : (p.y > P.bmax[1] ? P.bmax[1] : p.y);
-  p.z = p.z < P.bmin[2] ? P.bmin[2] : (p.z > P.bmax[2] ? P.bmax[2] : p.z);
+  p.x = p.x < R.bmin[0] ? R.bmin[0] : (p.x > R.bmax[0] ? R.bmax[0] : p.x);
+  p.y = p.y < R.bmin[1] ? R.bmin[1] : (p.y > R.bmax[1] ? R.bmax[1] : p.y);
+  p.z = p.z < R.bmin[2] ? R.bmin[2] : (p.z > R.bmax[2] ? R.bmax[2] : p.z);
   return p;
 }
 
@@ -129,13 +170,15 @@ __device__ __forceinline__ int dev_axis_bin(float c, float s) {
   return (int)floorf(xdiv(xadd(c, s), s));
 }
 
-__device__ __forceinline__ bool bin_of(const Dev& P, float x, float y, float z, uint32_t& out) {
+// Bin key in the particle's scene's grid (id = Dx*Dy*z + (y*Dx + x),
+// neighbors.h:109-114), offset by the scene's first key.
+__device__ __forceinline__ bool bin_of(const Dev& P, const Region& R, float x, float y, float z, uint32_t& out) {
   const int bx = dev_axis_bin(x, P.s), by = dev_axis_bin(y, P.s), bz = dev_axis_bin(z, P.s);
-  const bool ok = bx >= 0 && by >= 0 && bz >= 0 && bx < P.dimx && by < P.dimy && bz < P.dimz &&
+  const bool ok = bx >= 0 && by >= 0 && bz >= 0 && bx < R.dimx && by < R.dimy && bz < R.dimz &&
                   isfinite(x) && isfinite(y) && isfinite(z);
-  const int cx = min(max(bx, 0), P.dimx - 1), cy = min(max(by, 0), P.dimy - 1),
-            cz = min(max(bz, 0), P.dimz - 1);
-  out = (uint32_t)(P.dimx * P.dimy) * (uint32_t)cz + ((uint32_t)cy * (uint32_t)P.dimx + (uint32_t)cx);
+  const int cx = min(max(bx, 0), R.dimx - 1), cy = min(max(by, 0), R.dimy - 1),
+            cz = min(max(bz, 0), R.dimz - 1);
+  out = R.key0 + (uint32_t)(R.dimx * R.dimy) * (uint32_t)cz + ((uint32_t)cy * (uint32_t)R.dimx + (uint32_t)cx);
   return ok;
 }
 

@@ -273,8 +273,9 @@ __global__ void __launch_bounds__(128) k_mlp_predict(MlpDev M, const float* __re
 
 // Raw features of a particle at its first Jacobi iteration (order documented
 // in pbf.h).  sc_nb = sum_j |grad C_j|^2, g2 = |grad C_i|^2.
-__device__ __forceinline__ void raw_features(const Dev& P, const Fast& F, float f[kMlpIn], int c, float rho,
-                                             float sc_nb, float g2, int nh, float lamprev, float4 v, float4 xp) {
+__device__ __forceinline__ void raw_features(const Dev& P, const Region& R, const Fast& F, float f[kMlpIn], int c,
+                                             float rho, float sc_nb, float g2, int nh, float lamprev, float4 v,
+                                             float4 xp) {
   const float rel = rho * F.inv_rho0 - 1.0f;
   const float C = fmaxf(rel, 0.0f);
   const float S = sc_nb + g2;
@@ -289,9 +290,9 @@ __device__ __forceinline__ void raw_features(const Dev& P, const Fast& F, float 
   f[7] = c > 0 ? (float)nh / (float)c : 0.0f;
   f[8] = v.y * P.dt * inv_h;
   f[9] = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z) * P.dt * inv_h;
-  f[10] = fminf((xp.y - P.bmin[1]) * inv_h, 4.0f);
-  float wall = fminf(fminf(xp.x - P.bmin[0], P.bmax[0] - xp.x), fminf(xp.y - P.bmin[1], P.bmax[1] - xp.y));
-  wall = fminf(wall, fminf(xp.z - P.bmin[2], P.bmax[2] - xp.z));
+  f[10] = fminf((xp.y - R.bmin[1]) * inv_h, 4.0f);
+  float wall = fminf(fminf(xp.x - R.bmin[0], R.bmax[0] - xp.x), fminf(xp.y - R.bmin[1], R.bmax[1] - xp.y));
+  wall = fminf(wall, fminf(xp.z - R.bmin[2], R.bmax[2] - xp.z));
   f[11] = fminf(wall * inv_h, 4.0f);
 }
 

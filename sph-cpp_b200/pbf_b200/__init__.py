@@ -14,7 +14,7 @@ import numpy as np
 
 from . import _abi
 from ._abi import PbfParams, PbfStats  # noqa: F401
-from .scenes import Scene, make_scene, SCENES  # noqa: F401
+from .scenes import SCENES, Batch, Scene, make_batch, make_scene  # noqa: F401
 
 __all__ = ["Particles", "PbfParams", "PbfStats", "Scene", "make_scene", "SCENES", "lib", "params_init"]
 
@@ -34,15 +34,43 @@ def params_init() -> PbfParams:
 
 
 class Particles:
-    """A device-resident particle set plus its PBF solver (one pbf_ctx)."""
+    """A device-resident particle set plus its PBF solver (one pbf_ctx).
 
-    def __init__(self, params: PbfParams, capacity: int):
+    Particles(params, capacity) holds one scene; Particles.batch(batch) holds
+    the independent scenes of a scenes.Batch, advanced in the same launches
+    (particles indexed as the scenes concatenated in order)."""
+
+    def __init__(self, params: PbfParams, capacity: int, scenes=None):
         self._lib = lib()
         self._ctx = C.c_void_p()
-        rc = self._lib.pbf_create(C.byref(params), int(capacity), C.byref(self._ctx))
+        self.scene_offsets = None
+        if scenes is None:
+            rc = self._lib.pbf_create(C.byref(params), int(capacity), C.byref(self._ctx))
+        else:
+            arr = (_abi.PbfScene * len(scenes))(*scenes)
+            rc = self._lib.pbf_create_batch(C.byref(params), arr, len(scenes), C.byref(self._ctx))
+            self.scene_offsets = np.concatenate([[0], np.cumsum([int(sc.count) for sc in scenes])])
+            capacity = int(self.scene_offsets[-1])
         if rc != 0:
             raise RuntimeError(f"pbf_create failed ({rc}): {self._lib.pbf_create_error().decode()}")
         self.capacity = int(capacity)
+
+    @classmethod
+    def batch(cls, batch) -> "Particles":
+        return cls(batch.params(), 0, scenes=batch.scene_structs())
+
+    def scene_count(self) -> int:
+        return int(self._lib.pbf_scene_count(self._ctx))
+
+    def scene_stats(self, scene: int) -> dict:
+        st = PbfStats()
+        self._check(self._lib.pbf_scene_stats(self._ctx, int(scene), C.byref(st)), "scene_stats")
+        return st.as_dict()
+
+    def split(self, a: np.ndarray) -> list[np.ndarray]:
+        """Per-scene views of an array indexed by particle (a batch's order)."""
+        o = self.scene_offsets if self.scene_offsets is not None else np.array([0, len(a)])
+        return [a[o[i]:o[i + 1]] for i in range(len(o) - 1)]
 
     # -- lifetime --
     def close(self) -> None:

@@ -106,6 +106,10 @@ class PbfStats(C.Structure):
         }
 
 
+class PbfScene(C.Structure):
+    _fields_ = [("boundary_min", F3), ("boundary_max", F3), ("count", C.c_size_t)]
+
+
 class PbfTuning(C.Structure):
     _fields_ = [("lanes", C.c_int * 5), ("block", C.c_int * 5)]
 
@@ -163,6 +167,9 @@ SIGNATURES = {
     "pbf_kernel_times": (_i, [_vp, _i, _P(C.c_char_p), _P(C.c_int64), _P(C.c_double), _P(C.c_int)]),
     "pbf_reset_timing": (_i, [_vp]),
     "pbf_launches_per_step": (_i, [_vp, _P(C.c_int64)]),
+    "pbf_create_batch": (_i, [_P(PbfParams), _P(PbfScene), _i, _P(_vp)]),
+    "pbf_scene_count": (_i, [_vp]),
+    "pbf_scene_stats": (_i, [_vp, _i, _P(PbfStats)]),
     "pbf_get_tuning": (_i, [_vp, _P(PbfTuning)]),
     "pbf_set_tuning": (_i, [_vp, _P(PbfTuning)]),
     "pbf_autotune": (_i, [_vp, _i, _P(PbfTuning), _P(C.c_double)]),

@@ -11,7 +11,9 @@ particle, and a seeded +-0.005h jitter on the construct_fluid lattice.
   dam_65k    65,536 particles, 32x32x64 lattice in a 40^3 box, K = 3
   dam_1m     1,048,576 particles, 128x128x64 lattice, 160x160x80 box, K = 3
   dam_16m    16,777,216 particles, 256^3 lattice, 320^3 box, K = 4, cap 64
-plus small cases for tests.
+plus small cases for tests, and batches of independent dam-break scenes
+(make_batch): counts drawn log-uniform from a seed, lattice blocks of random
+aspect ratio, each in its own box 1.5x its extent.
 """
 from __future__ import annotations
 
@@ -125,3 +127,81 @@ SCENES: dict[str, Scene] = {
 def make_scene(name: str, **overrides) -> Scene:
     s = SCENES[name]
     return s.with_(**overrides) if overrides else s
+
+
+# ---------------------------------------------------------------- batches
+@dataclass(frozen=True)
+class Batch:
+    """Independent scenes advanced by one context (pbf_create_batch), sharing
+    the physics of scenes[0]; particles are the scenes' concatenated in order."""
+    name: str
+    scenes: tuple[Scene, ...]
+
+    @property
+    def n(self) -> int:
+        return sum(s.n for s in self.scenes)
+
+    @property
+    def counts(self) -> list[int]:
+        return [s.n for s in self.scenes]
+
+    @property
+    def offsets(self) -> np.ndarray:
+        return np.concatenate([[0], np.cumsum(self.counts)]).astype(np.int64)
+
+    def with_(self, **kw) -> "Batch":
+        return Batch(self.name, tuple(s.with_(**kw) for s in self.scenes))
+
+    def params(self) -> _abi.PbfParams:
+        return self.scenes[0].params()
+
+    def scene_structs(self) -> list:
+        out = []
+        for s in self.scenes:
+            sc = _abi.PbfScene()
+            for a in range(3):
+                sc.boundary_min[a] = 0.0
+                sc.boundary_max[a] = s.box_max[a]
+            sc.count = s.n
+            out.append(sc)
+        return out
+
+    def positions(self) -> np.ndarray:
+        return np.concatenate([s.positions() for s in self.scenes])
+
+
+def _box_extent(extent: float, s: float = 1.2) -> float:
+    """1.5x the fluid extent, moved off a multiple of the bin spacing s (a box
+    max that is a multiple of s leaves its +s re-hash outside the reference's
+    grid, neighbors.h:69-71)."""
+    b = round(1.5 * extent, 3)
+    while abs(b / s - round(b / s)) < 1e-3:
+        b += 0.05
+    return b
+
+
+def make_batch(scenes: int = 64, seed: int = 20161202, n_min: int = 4096, n_max: int = 262144,
+               name: str = "batch_64", **physics) -> Batch:
+    """Seeded batch of dam breaks: particle counts log-uniform in [n_min,
+    n_max], each a lattice block (spacing 0.5h) with y/x and z/x aspect ratios
+    uniform in [0.5, 2], the block at the origin of its own box 1.5x its
+    extent; scene i jitters with seed + i."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(scenes):
+        target = float(np.exp(rng.uniform(np.log(n_min), np.log(n_max))))
+        ay, az = rng.uniform(0.5, 2.0, 2)
+        nx = max(1, int(round((target / (ay * az)) ** (1.0 / 3.0))))
+
+        def dims(nx):
+            return nx, max(1, int(round(ay * nx))), max(1, int(round(az * nx)))
+
+        while np.prod(dims(nx)) < n_min:
+            nx += 1
+        while np.prod(dims(nx)) > n_max and nx > 1:
+            nx -= 1
+        lat = dims(nx)
+        sp = physics.get("spacing", 0.5)
+        box = tuple(_box_extent(lat[a] * sp) for a in range(3))
+        out.append(Scene(f"{name}[{i}]", lat, box, seed=seed + i, **physics))
+    return Batch(name, tuple(out))
