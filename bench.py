@@ -131,8 +131,9 @@ def kernel_bytes(name: str, n: int, nbar: float, K: int, nbins: int) -> float:
         "scan_reduce": 4.0 * nbins / n,
         "scan_partials": 0.0,
         "scan_apply": 8.0 * nbins / n,
-        "scatter": 4 + 4 + 4 + 8,                               # key, rank, orig in; pair out
-        "rank_in_bin": 8 + 4 + 8 + 8,                           # pair, its key, bin bounds in; pair out
+        "radix_hist": 4 + 2048.0 * 4 / 4096,                    # key in; per-tile digit counts out
+        "radix_scan": 2048.0 * 4 / 4096,                        # digit counts (3 launches, per launch)
+        "radix_scatter": 4 + 8 + 4 + 8,                         # key, pair in; key, pair out
         "warm_features": 16 + L + 16 + 16 + 4 + 16 + 32,       # x*, list, v, last lambda in; (x*, l1), v, bf16 features out
         "warm_mlp": 32 + 16 + 16 + 4 + 4,                       # features, (x*, l1) in; (x*, lambda), lambda, sum out
         "residual_check": 16 + L + 16 + 4 + 4,                  # as density_lambda

@@ -55,6 +55,20 @@ constexpr int kScanTile = kScanThreads * kScanItems;
 
 inline int blocks_for(size_t n, int b = kBlock) { return (int)((n + b - 1) / b); }
 
+// Digit histogram entries of the radix sort for up to `capacity` particles
+// (2^kRadixBits digits per 2^kRadixTileLog2-element tile); the constants are
+// checked against the kernels' below.
+constexpr int kRadixBitsHost = 11, kRadixTileHost = 4096;
+inline size_t radix_entries(size_t capacity) {
+  return ((capacity + kRadixTileHost - 1) / kRadixTileHost) * ((size_t)1 << kRadixBitsHost);
+}
+// Passes to sort keys < nbins.
+inline int radix_passes_for(int nbins) {
+  int bits = 0;
+  while (bits < 31 && ((int64_t)1 << bits) < (int64_t)nbins) ++bits;
+  return (bits + kRadixBitsHost - 1) / kRadixBitsHost;
+}
+
 // ============================================================================
 // Kernels
 // ============================================================================
@@ -139,22 +153,32 @@ __global__ void k_predict(Dev P, int n, const float4* __restrict__ pos, const fl
   pst[a] = make_float4(s.x, s.y, s.z, 0.0f);
 }
 
-// calculate_bins (neighbors.h:120-125) + bin histogram with per-particle rank.
-__global__ void k_hash(Dev P, int n, const float4* __restrict__ pst, uint32_t* key, uint32_t* rank,
-                       uint32_t* cell_count, uint32_t* err) {
+// calculate_bins (neighbors.h:120-125) + bin histogram; the radix sort's
+// input (key, pair) goes to the particle's reference index.
+__device__ __forceinline__ void hash_out(int a, uint32_t k, const uint32_t* __restrict__ orig, uint32_t* key,
+                                         uint32_t* cell_count, uint32_t* key_ref, unsigned long long* pair_ref) {
+  key[a] = k;
+  atomicAdd(&cell_count[k], 1u);
+  const uint32_t o = orig[a];
+  key_ref[o] = k;
+  pair_ref[o] = ((unsigned long long)o << 32) | (unsigned long long)(uint32_t)a;
+}
+
+__global__ void k_hash(Dev P, int n, const float4* __restrict__ pst, const uint32_t* __restrict__ orig,
+                       uint32_t* key, uint32_t* cell_count, uint32_t* key_ref, unsigned long long* pair_ref,
+                       uint32_t* err) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= n) return;
   const float4 s = pst[a];
   uint32_t k;
   if (!pbf::bin_of(P, pbf::region_of(P, a), s.x, s.y, s.z, k)) atomicOr(err, PBF_FLAG_KEY_RANGE);
-  key[a] = k;
-  rank[a] = atomicAdd(&cell_count[k], 1u);
+  hash_out(a, k, orig, key, cell_count, key_ref, pair_ref);
 }
 
 // Fused apply_external_forces + predict_positions + calculate_bins + histogram.
-__global__ void k_ext_predict_hash(Dev P, int n, const float4* __restrict__ pos, float4* vel,
-                                   float4* pst, uint32_t* key, uint32_t* rank, uint32_t* cell_count,
-                                   uint32_t* err) {
+__global__ void k_ext_predict_hash(Dev P, int n, const float4* __restrict__ pos, float4* vel, float4* pst,
+                                   const uint32_t* __restrict__ orig, uint32_t* key, uint32_t* cell_count,
+                                   uint32_t* key_ref, unsigned long long* pair_ref, uint32_t* err) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= n) return;
   float4 v = vel[a];
@@ -165,8 +189,7 @@ __global__ void k_ext_predict_hash(Dev P, int n, const float4* __restrict__ pos,
   pst[a] = make_float4(s.x, s.y, s.z, 0.0f);
   uint32_t k;
   if (!pbf::bin_of(P, R, s.x, s.y, s.z, k)) atomicOr(err, PBF_FLAG_KEY_RANGE);
-  key[a] = k;
-  rank[a] = atomicAdd(&cell_count[k], 1u);
+  hash_out(a, k, orig, key, cell_count, key_ref, pair_ref);
 }
 
 // ---- exclusive scan of cell_count[0..m-1] (+ total at [m]) -> cell_start ----
@@ -250,9 +273,10 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_apply(const uint32_t* __r
   }
 }
 
-// Stable counting-sort scatter: slot = start(bin) + rank; the fix-up below
-// orders every bin by reference index, which makes the whole permutation equal
-// to the reference's stable sort_by_key (neighbors.h:130-132).
+// Counting-sort scatter of the no-allocation neighbor search: slot =
+// start(bin) + atomic rank; k_cell_sort then orders every bin by reference
+// index (the permutation of the reference's stable sort_by_key,
+// neighbors.h:130-132).
 __global__ void k_scatter(int n, const uint32_t* __restrict__ key, const uint32_t* __restrict__ rank,
                           const uint32_t* __restrict__ cell_start, const uint32_t* __restrict__ orig,
                           unsigned long long* pairs) {
@@ -280,20 +304,98 @@ __global__ void k_cell_sort(int nbins, const uint32_t* __restrict__ cell_start, 
   }
 }
 
-// Stable order inside every bin: the scatter above placed a bin's pairs in
-// atomic (arbitrary) order; each pair's final position is the bin start plus
-// the number of the bin's pairs with a smaller reference index (pairs are
-// unique, so this is a permutation of the bin's slots).
-__global__ void k_rank_in_bin(int n, const unsigned long long* __restrict__ pairs, const uint32_t* __restrict__ key,
-                              const uint32_t* __restrict__ cell_start, unsigned long long* sorted) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n) return;
-  const unsigned long long pr = pairs[j];
-  const uint32_t c = key[(uint32_t)(pr & 0xffffffffull)];
-  const uint32_t b0 = cell_start[c], b1 = cell_start[c + 1];
-  uint32_t rank = 0;
-  for (uint32_t i = b0; i < b1; ++i) rank += pairs[i] < pr;
-  sorted[b0 + rank] = pr;
+// ---- stable LSD radix sort of (bin key, pair) ----
+// The hash kernels write every particle's key and pair (reference index << 32
+// | home slot) at its reference index, so the input is in reference-index
+// order and a stable sort by key orders every bin by reference index: the
+// permutation of the reference's stable sort_by_key (neighbors.h:130-132).
+// kRadixBits-bit digits, least significant first; each pass is a per-tile
+// digit histogram (digit-major: hist[d * tiles + tile]), an exclusive scan of
+// it (the scan kernels above) and a stable scatter.  The work is O(n) per pass
+// however the particles crowd into bins.
+constexpr int kRadixBits = 11;
+constexpr int kRadixDigits = 1 << kRadixBits;
+constexpr int kRadixThreads = 256;
+constexpr int kRadixWarps = kRadixThreads / 32;
+constexpr int kRadixItems = 16;
+constexpr int kRadixTile = kRadixThreads * kRadixItems;  // elements per tile (block)
+static_assert(kRadixBits == kRadixBitsHost && kRadixTile == kRadixTileHost, "radix buffer sizing");
+
+__device__ __forceinline__ uint32_t radix_digit(uint32_t key, int shift) {
+  return (key >> shift) & (uint32_t)(kRadixDigits - 1);
+}
+
+__global__ void __launch_bounds__(kRadixThreads) k_radix_hist(const uint32_t* __restrict__ keys, int n, int shift,
+                                                             int tiles, uint32_t* hist) {
+  __shared__ uint32_t cnt[kRadixDigits];
+  for (int d = threadIdx.x; d < kRadixDigits; d += kRadixThreads) cnt[d] = 0u;
+  __syncthreads();
+  const size_t base = (size_t)blockIdx.x * kRadixTile;
+  const int lane = threadIdx.x & 31;
+  for (int i = threadIdx.x; i < kRadixTile; i += kRadixThreads) {  // warp-uniform trip count
+    const size_t j = base + i;
+    const bool live = j < (size_t)n;
+    const uint32_t d = live ? radix_digit(keys[j], shift) : (uint32_t)kRadixDigits;
+    const unsigned peers = __match_any_sync(0xffffffffu, d);  // one shared-memory add per distinct digit
+    if (live && (peers & ((1u << lane) - 1u)) == 0u) atomicAdd(&cnt[d], (uint32_t)__popc(peers));
+  }
+  __syncthreads();
+  for (int d = threadIdx.x; d < kRadixDigits; d += kRadixThreads) hist[(size_t)d * tiles + blockIdx.x] = cnt[d];
+}
+
+// Stable scatter of one tile.  Warp w owns elements [w*32*kRadixItems,
+// (w+1)*32*kRadixItems) of the tile, walked item by item (element = item*32 +
+// lane): equal digits in one item are ranked by lane (__match_any_sync) and a
+// per-warp running count per digit carries the rank across items; the warps'
+// counts then become exclusive prefixes over the warps, so ranks follow the
+// element order across the tile, and tiles follow each other through the
+// scanned histogram.  keys_out may be null (last pass).
+__global__ void __launch_bounds__(kRadixThreads) k_radix_scatter(const uint32_t* __restrict__ keys_in,
+                                                                const unsigned long long* __restrict__ vals_in,
+                                                                int n, int shift, int tiles,
+                                                                const uint32_t* __restrict__ offsets,
+                                                                uint32_t* keys_out, unsigned long long* vals_out) {
+  __shared__ uint16_t wcnt[kRadixWarps * kRadixDigits];  // counts <= 32*kRadixItems, prefixes <= kRadixTile
+  for (int d = threadIdx.x; d < kRadixWarps * kRadixDigits; d += kRadixThreads) wcnt[d] = 0;
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  uint16_t* mine = wcnt + warp * kRadixDigits;
+  const size_t wbase = (size_t)blockIdx.x * kRadixTile + (size_t)warp * 32 * kRadixItems;
+  uint32_t dig[kRadixItems], rk[kRadixItems];
+#pragma unroll
+  for (int it = 0; it < kRadixItems; ++it) {
+    const size_t j = wbase + (size_t)it * 32 + lane;
+    const bool live = j < (size_t)n;
+    const uint32_t d = live ? radix_digit(keys_in[j], shift) : (uint32_t)kRadixDigits;
+    const unsigned peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t base = live ? (uint32_t)mine[d] : 0u;
+    __syncwarp();
+    if (live && (peers & lt) == 0u) mine[d] = (uint16_t)(base + (uint32_t)__popc(peers));
+    __syncwarp();
+    dig[it] = d;
+    rk[it] = base + (uint32_t)__popc(peers & lt);
+  }
+  __syncthreads();
+  for (int d = threadIdx.x; d < kRadixDigits; d += kRadixThreads) {
+    uint32_t run = 0;
+#pragma unroll
+    for (int w = 0; w < kRadixWarps; ++w) {
+      const uint32_t c = wcnt[w * kRadixDigits + d];
+      wcnt[w * kRadixDigits + d] = (uint16_t)run;
+      run += c;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int it = 0; it < kRadixItems; ++it) {
+    const size_t j = wbase + (size_t)it * 32 + lane;
+    if (j >= (size_t)n) continue;
+    const uint32_t d = dig[it];
+    const uint32_t pos = offsets[(size_t)d * tiles + blockIdx.x] + (uint32_t)mine[d] + rk[it];
+    vals_out[pos] = vals_in[j];
+    if (keys_out) keys_out[pos] = keys_in[j];
+  }
 }
 
 // Gather the state into sorted order.  FULL = also scratch and lambda (the
@@ -1228,7 +1330,14 @@ struct pbf_ctx {
   float4 *posH = nullptr, *pstH = nullptr, *velH = nullptr, *scrH = nullptr;
   float4 *posS = nullptr, *pstS = nullptr, *velS = nullptr, *scrS = nullptr, *xl = nullptr, *velT = nullptr;
   float *lamH = nullptr, *lamS = nullptr;
-  uint32_t *origH = nullptr, *origS = nullptr, *key = nullptr, *rank = nullptr, *keyH = nullptr;
+  uint32_t *origH = nullptr, *origS = nullptr, *key = nullptr, *keyH = nullptr;
+  // radix sort: keys at the reference index and their ping-pong twin, digit
+  // histograms, their scan, scan partials; `sorted` = the pair buffer holding
+  // the sorted pairs after the last pass
+  uint32_t *key_ref = nullptr, *key_alt = nullptr, *radix_hist = nullptr, *radix_off = nullptr,
+           *radix_parts = nullptr;
+  int radix_passes = 0;
+  unsigned long long* sorted = nullptr;
   uint32_t *cell_count = nullptr, *cell_start = nullptr, *scan_part = nullptr, *err = nullptr, *nudge = nullptr;
   unsigned long long *pairs = nullptr, *pairs_sorted = nullptr;
   int32_t *nbr = nullptr, *cnt = nullptr;
@@ -1571,29 +1680,55 @@ int harvest_times(pbf_ctx* ctx) {
 void launch_sort_to_pairs(pbf_ctx* ctx) {
   const int n = (int)ctx->n;
   const int m = ctx->nbins;  // scan m entries -> m+1 outputs
+  cudaStream_t s = ctx->stream;
   {
     Launch L(ctx, "scan_reduce");
-    k_scan_reduce<<<ctx->nscan_parts, kScanThreads, 0, ctx->stream>>>(ctx->cell_count, m, ctx->scan_part);
+    k_scan_reduce<<<ctx->nscan_parts, kScanThreads, 0, s>>>(ctx->cell_count, m, ctx->scan_part);
   }
   {
     Launch L(ctx, "scan_partials");
-    k_scan_partials<<<1, kScanThreads, 0, ctx->stream>>>(ctx->scan_part, ctx->nscan_parts);
+    k_scan_partials<<<1, kScanThreads, 0, s>>>(ctx->scan_part, ctx->nscan_parts);
   }
   {
     Launch L(ctx, "scan_apply");
-    k_scan_apply<<<ctx->nscan_parts, kScanThreads, 0, ctx->stream>>>(ctx->cell_count, m, ctx->scan_part,
-                                                                     ctx->cell_start);
+    k_scan_apply<<<ctx->nscan_parts, kScanThreads, 0, s>>>(ctx->cell_count, m, ctx->scan_part, ctx->cell_start);
   }
-  {
-    Launch L(ctx, "scatter");
-    k_scatter<<<blocks_for(n), kBlock, 0, ctx->stream>>>(n, ctx->key, ctx->rank, ctx->cell_start, ctx->origH,
-                                                         ctx->pairs);
+  // stable LSD radix sort of (key, pair), input in reference-index order
+  const int tiles = (int)(((size_t)n + kRadixTile - 1) / kRadixTile);
+  const int hm = kRadixDigits * tiles;
+  const int hp = (int)(((size_t)hm + 1 + kScanTile - 1) / kScanTile);
+  uint32_t* kin = ctx->key_ref;
+  uint32_t* kout = ctx->key_alt;
+  unsigned long long* vin = ctx->pairs;
+  unsigned long long* vout = ctx->pairs_sorted;
+  for (int p = 0; p < ctx->radix_passes; ++p) {
+    const int shift = p * kRadixBits;
+    const bool last = p == ctx->radix_passes - 1;
+    {
+      Launch L(ctx, "radix_hist");
+      k_radix_hist<<<tiles, kRadixThreads, 0, s>>>(kin, n, shift, tiles, ctx->radix_hist);
+    }
+    {
+      Launch L(ctx, "radix_scan");
+      k_scan_reduce<<<hp, kScanThreads, 0, s>>>(ctx->radix_hist, hm, ctx->radix_parts);
+    }
+    {
+      Launch L(ctx, "radix_scan");
+      k_scan_partials<<<1, kScanThreads, 0, s>>>(ctx->radix_parts, hp);
+    }
+    {
+      Launch L(ctx, "radix_scan");
+      k_scan_apply<<<hp, kScanThreads, 0, s>>>(ctx->radix_hist, hm, ctx->radix_parts, ctx->radix_off);
+    }
+    {
+      Launch L(ctx, "radix_scatter");
+      k_radix_scatter<<<tiles, kRadixThreads, 0, s>>>(kin, vin, n, shift, tiles, ctx->radix_off,
+                                                     last ? nullptr : kout, vout);
+    }
+    std::swap(kin, kout);
+    std::swap(vin, vout);
   }
-  {
-    Launch L(ctx, "rank_in_bin");
-    k_rank_in_bin<<<blocks_for(n), kBlock, 0, ctx->stream>>>(n, ctx->pairs, ctx->key, ctx->cell_start,
-                                                             ctx->pairs_sorted);
-  }
+  ctx->sorted = vin;  // the last pass's output (the input itself when no pass is needed)
 }
 
 void launch_fill(pbf_ctx* ctx, const float4* pst) {
@@ -1688,14 +1823,14 @@ void launch_step_t(pbf_ctx* ctx) {
   cudaMemsetAsync(ctx->cell_count, 0, sizeof(uint32_t) * (size_t)ctx->nbins, s);
   {
     Launch L(ctx, "ext_predict_hash");
-    k_ext_predict_hash<<<g, kBlock, 0, s>>>(P, n, ctx->posH, ctx->velH, ctx->pstH, ctx->key, ctx->rank,
-                                            ctx->cell_count, ctx->err);
+    k_ext_predict_hash<<<g, kBlock, 0, s>>>(P, n, ctx->posH, ctx->velH, ctx->pstH, ctx->origH, ctx->key,
+                                            ctx->cell_count, ctx->key_ref, ctx->pairs, ctx->err);
   }
   launch_sort_to_pairs(ctx);
   {
     Launch L(ctx, "reorder");
     const bool keep = !X && (ctx->recording || ctx->params.solver == 1);
-    k_reorder<false><<<g, kBlock, 0, s>>>(n, ctx->pairs_sorted, ctx->key, ctx->posH, ctx->pstH, ctx->velH, nullptr,
+    k_reorder<false><<<g, kBlock, 0, s>>>(n, ctx->sorted, ctx->key, ctx->posH, ctx->pstH, ctx->velH, nullptr,
                                           keep ? ctx->lamsumH : nullptr, ctx->posS, ctx->pstS, ctx->velS, nullptr,
                                           keep ? ctx->lamprevS : nullptr, ctx->origS, ctx->keyH);
   }
@@ -1823,20 +1958,21 @@ void launch_step(pbf_ctx* ctx) {
 }
 
 int launches_per_step(const pbf_ctx* ctx) {
-  // kernels only (the memsets are not): ext/predict/hash + 3 scan + scatter
-  // + rank in bin + reorder + fill + K x (density/lambda, [exact: lambda
-  // fix-up], delta-p) + (K==0: velocity)
+  // kernels only (the memsets are not): ext/predict/hash + 3 scan + radix
+  // passes x (histogram, 3 scan, scatter) + reorder + fill + K x
+  // (density/lambda, [exact: lambda fix-up], delta-p) + (K==0: velocity)
   // + 2 if gamma + 4 (visc, vort, apply, visc)
+  const int sort = 5 * ctx->radix_passes;
   const int K = ctx->params.solve_steps;
   const int tail = (ctx->params.gamma != 0.0f ? 2 : 0) + 4;
   if (ctx->params.solver == 1 && !ctx->params.exact_math) {
     // learned: warm iteration (features, network, delta-p) + (iters-1) x (check, decide, delta-p)
     // + final check, decide + velocity
     const int it = ctx->params.max_iterations > 0 ? ctx->params.max_iterations : 1;
-    return 1 + 3 + 1 + 1 + 1 + 1 + 3 + 3 * (it - 1) + 2 + 1 + tail;
+    return 1 + 3 + sort + 1 + 1 + 3 + 3 * (it - 1) + 2 + 1 + tail;
   }
   const int per_iter = ctx->params.exact_math ? 3 : 2;
-  return 1 + 3 + 1 + 1 + 1 + 1 + per_iter * K + (K == 0 ? 1 : 0) + tail;
+  return 1 + 3 + sort + 1 + 1 + per_iter * K + (K == 0 ? 1 : 0) + tail;
 }
 
 }  // namespace
@@ -1869,6 +2005,7 @@ static int create_ctx(const pbf_params* p, size_t capacity, const pbf_scene* sce
   ctx->capacity = capacity;
   ctx->nbins = ctx->dev.nbins;
   ctx->nbins_cap = ctx->nbins;
+  ctx->radix_passes = radix_passes_for(ctx->nbins);
   ctx->nscan_parts = (int)(((size_t)ctx->nbins + 1 + kScanTile - 1) / kScanTile);
   auto bail = [&](int code) {
     g_create_error = ctx->error;
@@ -1902,7 +2039,11 @@ static int create_ctx(const pbf_params* p, size_t capacity, const pbf_scene* sce
       (rc = dalloc(ctx, &ctx->velS, C)) || (rc = dalloc(ctx, &ctx->scrS, C)) || (rc = dalloc(ctx, &ctx->xl, C)) ||
       (rc = dalloc(ctx, &ctx->velT, C)) || (rc = dalloc(ctx, &ctx->lamH, C)) || (rc = dalloc(ctx, &ctx->lamS, C)) ||
       (rc = dalloc(ctx, &ctx->origH, C)) || (rc = dalloc(ctx, &ctx->origS, C)) || (rc = dalloc(ctx, &ctx->key, C)) ||
-      (rc = dalloc(ctx, &ctx->rank, C)) || (rc = dalloc(ctx, &ctx->keyH, C)) ||
+      (rc = dalloc(ctx, &ctx->key_ref, C)) || (rc = dalloc(ctx, &ctx->key_alt, C)) ||
+      (rc = dalloc(ctx, &ctx->keyH, C)) ||
+      (rc = dalloc(ctx, &ctx->radix_hist, radix_entries(C))) ||
+      (rc = dalloc(ctx, &ctx->radix_off, radix_entries(C) + 1)) ||
+      (rc = dalloc(ctx, &ctx->radix_parts, (radix_entries(C) + 1 + kScanTile - 1) / kScanTile)) ||
       (rc = dalloc(ctx, &ctx->cell_count, (size_t)ctx->nbins)) ||
       (rc = dalloc(ctx, &ctx->cell_start, (size_t)ctx->nbins + 1)) ||
       (rc = dalloc(ctx, &ctx->scan_part, (size_t)ctx->nscan_parts)) || (rc = dalloc(ctx, &ctx->err, 1)) ||
@@ -1983,6 +2124,7 @@ int pbf_set_params(pbf_ctx* ctx, const pbf_params* p) {
   ctx->lstride = lstride;
   std::memcpy(ctx->dims, dims, sizeof(dims));
   ctx->nbins = d.nbins;
+  ctx->radix_passes = radix_passes_for(ctx->nbins);
   ctx->nscan_parts = (int)(((size_t)ctx->nbins + 1 + kScanTile - 1) / kScanTile);
   if (batch) {
     ctx->regions = regions;
@@ -2139,9 +2281,10 @@ int pbf_find_neighbors(pbf_ctx* ctx, size_t bin_b, size_t bin_e, size_t fill_b, 
   const int n = (int)ctx->n, g = blocks_for(ctx->n);
   cudaStream_t s = ctx->stream;
   CK(cudaMemsetAsync(ctx->cell_count, 0, sizeof(uint32_t) * (size_t)ctx->nbins, s));
-  k_hash<<<g, kBlock, 0, s>>>(ctx->dev, n, ctx->pstH, ctx->key, ctx->rank, ctx->cell_count, ctx->err);
+  k_hash<<<g, kBlock, 0, s>>>(ctx->dev, n, ctx->pstH, ctx->origH, ctx->key, ctx->cell_count, ctx->key_ref,
+                              ctx->pairs, ctx->err);
   launch_sort_to_pairs(ctx);
-  k_reorder<true><<<g, kBlock, 0, s>>>(n, ctx->pairs_sorted, ctx->key, ctx->posH, ctx->pstH, ctx->velH, ctx->scrH,
+  k_reorder<true><<<g, kBlock, 0, s>>>(n, ctx->sorted, ctx->key, ctx->posH, ctx->pstH, ctx->velH, ctx->scrH,
                                        ctx->lamH, ctx->posS, ctx->pstS, ctx->velS, ctx->scrS, ctx->lamS, ctx->origS,
                                        ctx->keyH);
   const size_t f4 = sizeof(float4) * ctx->n;

@@ -9,8 +9,9 @@
 //  - branch-free: clamping (h^2 - d^2) and (h - r) at 0 zeroes the pairs with
 //    h < r < s, which stay in the lists because x* moves during the iterations;
 //  - kernel constants (norms, 1/rho0, mass) folded on the host;
-//  - kGL = 8 lanes per particle walk its row-major list together (see Group)
-//    and combine their partial sums with shuffles.
+//  - GL = 4 or 8 lanes per particle (the launch shape the autotuner picks)
+//    walk its row-major list together (see Group) and combine their partial
+//    sums with shuffles.
 // A particle sitting exactly on a neighbour (d^2 < 1e-16, the reference's
 // nudge condition |r| < 1e-8, particles.h:303-305) falls back to the
 // reference-ordered path for that particle.
@@ -133,7 +134,8 @@ __device__ __forceinline__ void gwalk1(const int32_t* __restrict__ row, int c, i
 }
 
 // Two records per neighbour: batches of kB2 keep the register count (and so
-// the occupancy) of the one-record walk.
+// the occupancy) of the one-record walk (batches of 4 at 4 lanes measured
+// slower: 64 registers).
 constexpr int kB2 = 2;
 
 template <int GL = kGL, class Body>
