@@ -62,6 +62,13 @@ constexpr int kRadixBitsHost = 11, kRadixTileHost = 4096;
 inline size_t radix_entries(size_t capacity) {
   return ((capacity + kRadixTileHost - 1) / kRadixTileHost) * ((size_t)1 << kRadixBitsHost);
 }
+// Neighbor list rows are kListAlign-entry multiples long, so the fast gathers
+// read whole vectors of indices (the entries past a particle's count are
+// replaced by a dummy slot, one past the last particle, whose every kernel
+// term is exactly zero).
+constexpr int kListAlign = 32;
+inline size_t list_stride(int cap) { return ((size_t)cap + kListAlign - 1) / kListAlign * kListAlign; }
+
 // Passes to sort keys < nbins.
 inline int radix_passes_for(int nbins) {
   int bits = 0;
@@ -74,10 +81,21 @@ inline int radix_passes_for(int nbins) {
 // ============================================================================
 
 // Upload: AoS float3 host layout -> float4 home buffers, identity order.
+// The dummy slot n the list padding points at: far from every particle (all
+// kernel terms vanish: Poly6 and Spiky are 0 beyond h, lambda and |w| are 0),
+// unit density (XSPH divides by it).  Kernels only write slots < n.
+constexpr float kFar = 1e15f;
+
 __global__ void k_upload(int n, const float* __restrict__ x, const float* __restrict__ v,
                          float4* posH, float4* pstH, float4* velH, float4* scrH, float* lamH,
-                         uint32_t* origH) {
+                         uint32_t* origH, float4* pstS, float4* xl, float4* velS, float4* velT) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) {
+    pstS[n] = make_float4(kFar, kFar, kFar, 0.0f);
+    xl[n] = make_float4(kFar, kFar, kFar, 0.0f);
+    velS[n] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+    velT[n] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+  }
   if (i >= n) return;
   const float4 p = make_float4(x[3 * i], x[3 * i + 1], x[3 * i + 2], 0.0f);
   posH[i] = p;
@@ -652,9 +670,9 @@ struct DensitySums {
 
 template <int GL, bool NH>
 __device__ __forceinline__ DensitySums density_sums(const Fast& F, const pbf::Group& G, const int32_t* row, int c,
-                                                    const float4* __restrict__ pst, float4 xp) {
+                                                    int n, const float4* __restrict__ pst, float4 xp) {
   DensitySums S{0.f, 0.f, 0.f, 0.f, 0.f, FLT_MAX, 0.f};
-  pbf::gwalk1<GL>(row, c, G.lane, pst, [&](int, float4 xq) {
+  pbf::gwalk1<GL>(row, c, n, G.lane, pst, [&](int, float4 xq) {
     const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
     const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
     S.dmin = fminf(S.dmin, d2);
@@ -686,7 +704,7 @@ __device__ __forceinline__ void density_lambda_tile(int tile, const Dev& P, cons
   const int b = G.b;
   const float4 xp = pst[b];
   const int c = G.live ? cnt[b] : 0;
-  const DensitySums S = density_sums<GL, MODE == kDlRecord>(F, G, nbr + (size_t)b * stride, c, pst, xp);
+  const DensitySums S = density_sums<GL, MODE == kDlRecord>(F, G, nbr + (size_t)b * stride, c, n, pst, xp);
   const float rho = fmaf(F.m_poly, S.sw, F.m_w0);
   if (MODE == kDlCheck && G.live && G.lane == 0) err += fmaxf(fmaf(rho, F.inv_rho0, -1.0f), 0.0f);
   if (!G.live || G.lane != 0) return;
@@ -756,7 +774,7 @@ __global__ void __launch_bounds__(kBlock) kl_features(Dev P, Fast F, pbf::MlpDev
   const int b = G.b;
   const float4 xp = pst[b];
   const int c = G.live ? cnt[b] : 0;
-  const DensitySums S = density_sums<pbf::kGL, true>(F, G, nbr + (size_t)b * stride, c, pst, xp);
+  const DensitySums S = density_sums<pbf::kGL, true>(F, G, nbr + (size_t)b * stride, c, n, pst, xp);
   if (!G.live || G.lane != 0) return;
   const float rho = fmaf(F.m_poly, S.sw, F.m_w0);
   const float L2 = F.lam_grad * F.lam_grad;
@@ -1118,7 +1136,7 @@ __device__ __forceinline__ void dp_update_tile(int tile, const Dev& P, const Fas
   const int c = G.live ? cnt[b] : 0;
   float ax = 0.f, ay = 0.f, az = 0.f;
   const float lp = xp.w;
-  pbf::gwalk1<GL>(nbr + (size_t)b * stride, c, G.lane, xl, [&](int, float4 xq) {
+  pbf::gwalk1<GL>(nbr + (size_t)b * stride, c, n, G.lane, xl, [&](int, float4 xq) {
     const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
     const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
     float l = lp + xq.w;
@@ -1169,7 +1187,7 @@ __global__ void __launch_bounds__(kBlock) kf_viscosity(Dev P, Fast F, int n, siz
   const float4 xp = pst[b], vp = vin[b];
   const int c = G.live ? cnt[b] : 0;
   float ax = 0.f, ay = 0.f, az = 0.f;
-  pbf::gwalk2<GL>(nbr + (size_t)b * stride, c, G.lane, pst, vin, [&](int, float4 xq, float4 vq) {
+  pbf::gwalk2<GL>(nbr + (size_t)b * stride, c, n, G.lane, pst, vin, [&](int, float4 xq, float4 vq) {
     const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
     const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
     const float wr = __fdividef(pbf::poly_cube(F, d2), vq.w);
@@ -1200,7 +1218,7 @@ __global__ void __launch_bounds__(kBlock) kf_vorticity(Dev P, Fast F, int n, siz
   const float4 xp = pst[b], vp = vel[b];
   const int c = G.live ? cnt[b] : 0;
   float wx = 0.f, wy = 0.f, wz = 0.f;
-  pbf::gwalk2<GL>(nbr + (size_t)b * stride, c, G.lane, pst, vel, [&](int, float4 xq, float4 vq) {
+  pbf::gwalk2<GL>(nbr + (size_t)b * stride, c, n, G.lane, pst, vel, [&](int, float4 xq, float4 vq) {
     const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
     const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
     const float t = pbf::spikey_over_r(F, d2);
@@ -1230,7 +1248,7 @@ __global__ void __launch_bounds__(kBlock) kf_apply_vorticity(Dev P, Fast F, int 
   const float4 xp = xl[b];
   const int c = G.live ? cnt[b] : 0;
   float ex = 0.f, ey = 0.f, ez = 0.f;
-  pbf::gwalk1<GL>(nbr + (size_t)b * stride, c, G.lane, xl, [&](int, float4 xq) {
+  pbf::gwalk1<GL>(nbr + (size_t)b * stride, c, n, G.lane, xl, [&](int, float4 xq) {
     const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
     const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
     const float t = xq.w * pbf::spikey_over_r(F, d2);
@@ -1321,8 +1339,8 @@ struct pbf_ctx {
   int64_t dims[3] = {0, 0, 0};
   int nbins = 0, nscan_parts = 0;
   int nbins_cap = 0;   // bins the cell arrays were allocated for
-  size_t lstride = 0;
-  size_t lstride_cap = 0;  // list row stride the list buffer was allocated for  // list row stride: neighbor_cap rounded up to 8 (whole 32-byte sectors)
+  size_t lstride = 0;      // list row stride: neighbor_cap rounded up to kListAlign entries
+  size_t lstride_cap = 0;  // list row stride the list buffer was allocated for
   int device = 0;
   cudaStream_t stream = nullptr;
   bool lists_valid = false;
@@ -2031,13 +2049,13 @@ static int create_ctx(const pbf_params* p, size_t capacity, const pbf_scene* sce
     return bail(PBF_ERR_CUDA);
   }
   const size_t C = capacity;
-  ctx->lstride = ((size_t)p->neighbor_cap + 7) / 8 * 8;
+  ctx->lstride = list_stride(p->neighbor_cap);
   ctx->lstride_cap = ctx->lstride;
   const size_t cap = ctx->lstride;
   if ((rc = dalloc(ctx, &ctx->posH, C)) || (rc = dalloc(ctx, &ctx->pstH, C)) || (rc = dalloc(ctx, &ctx->velH, C)) ||
-      (rc = dalloc(ctx, &ctx->scrH, C)) || (rc = dalloc(ctx, &ctx->posS, C)) || (rc = dalloc(ctx, &ctx->pstS, C)) ||
-      (rc = dalloc(ctx, &ctx->velS, C)) || (rc = dalloc(ctx, &ctx->scrS, C)) || (rc = dalloc(ctx, &ctx->xl, C)) ||
-      (rc = dalloc(ctx, &ctx->velT, C)) || (rc = dalloc(ctx, &ctx->lamH, C)) || (rc = dalloc(ctx, &ctx->lamS, C)) ||
+      (rc = dalloc(ctx, &ctx->scrH, C)) || (rc = dalloc(ctx, &ctx->posS, C)) || (rc = dalloc(ctx, &ctx->pstS, C + 1)) ||
+      (rc = dalloc(ctx, &ctx->velS, C + 1)) || (rc = dalloc(ctx, &ctx->scrS, C)) || (rc = dalloc(ctx, &ctx->xl, C + 1)) ||
+      (rc = dalloc(ctx, &ctx->velT, C + 1)) || (rc = dalloc(ctx, &ctx->lamH, C)) || (rc = dalloc(ctx, &ctx->lamS, C)) ||
       (rc = dalloc(ctx, &ctx->origH, C)) || (rc = dalloc(ctx, &ctx->origS, C)) || (rc = dalloc(ctx, &ctx->key, C)) ||
       (rc = dalloc(ctx, &ctx->key_ref, C)) || (rc = dalloc(ctx, &ctx->key_alt, C)) ||
       (rc = dalloc(ctx, &ctx->keyH, C)) ||
@@ -2113,7 +2131,7 @@ int pbf_set_params(pbf_ctx* ctx, const pbf_params* p) {
   const bool batch = !ctx->scenes.empty();
   int rc = batch ? make_dev_batch(ctx, *p, ctx->scenes, d, regions, first) : make_dev(ctx, *p, d, dims);
   if (rc) return rc;
-  const size_t lstride = ((size_t)p->neighbor_cap + 7) / 8 * 8;
+  const size_t lstride = list_stride(p->neighbor_cap);
   if (d.nbins > ctx->nbins_cap || lstride > ctx->lstride_cap)
     return fail(ctx, PBF_ERR_PARAMS, "new parameters need a larger grid or neighbor cap than allocated");
   if (d.nbins != ctx->nbins || p->neighbor_cap != ctx->params.neighbor_cap || d.s != ctx->dev.s)
@@ -2161,7 +2179,8 @@ int pbf_upload(pbf_ctx* ctx, const float* x, const float* v, size_t n) {
   if (v) CK(cudaMemcpyAsync(dv, v, n * 3 * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemsetAsync(ctx->lamsumH, 0, n * sizeof(float), ctx->stream));  // no lambda history yet
   k_upload<<<blocks_for(n), kBlock, 0, ctx->stream>>>((int)n, dx, v ? dv : nullptr, ctx->posH, ctx->pstH,
-                                                      ctx->velH, ctx->scrH, ctx->lamH, ctx->origH);
+                                                      ctx->velH, ctx->scrH, ctx->lamH, ctx->origH, ctx->pstS,
+                                                      ctx->xl, ctx->velS, ctx->velT);
   return check_launch(ctx, "upload");
 }
 

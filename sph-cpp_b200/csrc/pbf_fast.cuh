@@ -10,8 +10,8 @@
 //    h < r < s, which stay in the lists because x* moves during the iterations;
 //  - kernel constants (norms, 1/rho0, mass) folded on the host;
 //  - GL = 4 or 8 lanes per particle (the launch shape the autotuner picks)
-//    walk its row-major list together (see Group) and combine their partial
-//    sums with shuffles.
+//    walk its row-major, padded list together (see Group, gwalk1) and
+//    combine their partial sums with shuffles.
 // A particle sitting exactly on a neighbour (d^2 < 1e-16, the reference's
 // nudge condition |r| < 1e-8, particles.h:303-305) falls back to the
 // reference-ordered path for that particle.
@@ -108,58 +108,65 @@ __device__ __forceinline__ float gmin(float v) {
   return v;
 }
 
-// Walk entries lane, lane + GL, ... of a list row, kB entries per batch:
-// the batch's indices are loaded first, then its neighbour records, then the
-// bodies run (predicated past the count), keeping 2*kB loads in flight.
-constexpr int kB = 4;
-
+// Walk a list row: lane l of the group takes entries 4l..4l+3 of every
+// 4*GL-entry batch, one 16-byte index load, then its four neighbour records
+// (four independent loads in flight), then the four bodies.  Rows are padded
+// to a multiple of 32 entries, so the last, partial batch reads whole vectors
+// too; its entries past the count are replaced by `dummy`, a slot whose every
+// term is zero.
 template <int GL = kGL, class Body>
-__device__ __forceinline__ void gwalk1(const int32_t* __restrict__ row, int c, int lane,
+__device__ __forceinline__ void gwalk1(const int32_t* __restrict__ row, int c, int dummy, int lane,
                                        const float4* __restrict__ a, Body&& body) {
-  for (int k0 = lane; k0 < c; k0 += kB * GL) {
-    int q[kB];
-    float4 v[kB];
-#pragma unroll
-    for (int u = 0; u < kB; ++u) {
-      const int k = k0 + u * GL;
-      q[u] = k < c ? __ldg(row + k) : -1;
-    }
-#pragma unroll
-    for (int u = 0; u < kB; ++u)
-      if (q[u] >= 0) v[u] = __ldg(a + q[u]);
-#pragma unroll
-    for (int u = 0; u < kB; ++u)
-      if (q[u] >= 0) body(q[u], v[u]);
+  const int4* r4 = reinterpret_cast<const int4*>(row);
+  const int full = c / (4 * GL);
+  int t = 0;
+  for (; t < full; ++t) {
+    const int4 q = __ldg(r4 + t * GL + lane);
+    const float4 v0 = __ldg(a + q.x), v1 = __ldg(a + q.y), v2 = __ldg(a + q.z), v3 = __ldg(a + q.w);
+    body(q.x, v0);
+    body(q.y, v1);
+    body(q.z, v2);
+    body(q.w, v3);
+  }
+  if (t * 4 * GL < c) {
+    int4 q = __ldg(r4 + t * GL + lane);
+    const int e = t * 4 * GL + 4 * lane;
+    q.x = e < c ? q.x : dummy;
+    q.y = e + 1 < c ? q.y : dummy;
+    q.z = e + 2 < c ? q.z : dummy;
+    q.w = e + 3 < c ? q.w : dummy;
+    const float4 v0 = __ldg(a + q.x), v1 = __ldg(a + q.y), v2 = __ldg(a + q.z), v3 = __ldg(a + q.w);
+    body(q.x, v0);
+    body(q.y, v1);
+    body(q.z, v2);
+    body(q.w, v3);
   }
 }
 
-// Two records per neighbour: batches of kB2 keep the register count (and so
-// the occupancy) of the one-record walk (batches of 4 at 4 lanes measured
-// slower: 64 registers).
-constexpr int kB2 = 2;
-
+// Two records per neighbour: entries 2l, 2l+1 of every 2*GL-entry batch (an
+// 8-byte index load), so that four records are in flight per lane, as in the
+// one-record walk.
 template <int GL = kGL, class Body>
-__device__ __forceinline__ void gwalk2(const int32_t* __restrict__ row, int c, int lane,
+__device__ __forceinline__ void gwalk2(const int32_t* __restrict__ row, int c, int dummy, int lane,
                                        const float4* __restrict__ a, const float4* __restrict__ bsrc,
                                        Body&& body) {
-  constexpr int kB = kB2;
-  for (int k0 = lane; k0 < c; k0 += kB * GL) {
-    int q[kB];
-    float4 va[kB], vb[kB];
-#pragma unroll
-    for (int u = 0; u < kB; ++u) {
-      const int k = k0 + u * GL;
-      q[u] = k < c ? __ldg(row + k) : -1;
-    }
-#pragma unroll
-    for (int u = 0; u < kB; ++u)
-      if (q[u] >= 0) {
-        va[u] = __ldg(a + q[u]);
-        vb[u] = __ldg(bsrc + q[u]);
-      }
-#pragma unroll
-    for (int u = 0; u < kB; ++u)
-      if (q[u] >= 0) body(q[u], va[u], vb[u]);
+  const int2* r2 = reinterpret_cast<const int2*>(row);
+  const int full = c / (2 * GL);
+  int t = 0;
+  for (; t < full; ++t) {
+    const int2 q = __ldg(r2 + t * GL + lane);
+    const float4 a0 = __ldg(a + q.x), b0 = __ldg(bsrc + q.x), a1 = __ldg(a + q.y), b1 = __ldg(bsrc + q.y);
+    body(q.x, a0, b0);
+    body(q.y, a1, b1);
+  }
+  if (t * 2 * GL < c) {
+    int2 q = __ldg(r2 + t * GL + lane);
+    const int e = t * 2 * GL + 2 * lane;
+    q.x = e < c ? q.x : dummy;
+    q.y = e + 1 < c ? q.y : dummy;
+    const float4 a0 = __ldg(a + q.x), b0 = __ldg(bsrc + q.x), a1 = __ldg(a + q.y), b1 = __ldg(bsrc + q.y);
+    body(q.x, a0, b0);
+    body(q.y, a1, b1);
   }
 }
 
