@@ -43,7 +43,7 @@ extern "C" {
 #define PBF_ERR_PARAMS -5     /* parameters outside what the reference grid supports */
 #define PBF_ERR_STATE -6      /* call out of order (e.g. no neighbor lists yet) */
 #define PBF_ERR_DEVICE -7     /* device-side check tripped (see pbf_stats_t.error_flags) */
-#define PBF_ERR_IO -8         /* INI file unreadable */
+#define PBF_ERR_IO -8         /* INI or state file unreadable, or a short write */
 
 /* Device-side error flag bits (pbf_stats_t.error_flags). */
 #define PBF_FLAG_KEY_RANGE 1u     /* a bin id fell outside the grid; clamped */
@@ -232,6 +232,40 @@ int pbf_kernel_times(pbf_ctx* ctx, int max_kinds, const char** names, int64_t* l
 int pbf_reset_timing(pbf_ctx* ctx);
 /* Number of kernel launches one pbf_step(ctx, 1) issues. */
 int pbf_launches_per_step(pbf_ctx* ctx, int64_t* out);
+
+/* ---- growing the particle set (the emitter) ----
+ * pbf_add_particles replaces Particles::add (particles.h:184-199) for k host
+ * particles (AoS xyz; v may be NULL for zero velocity): they get the next
+ * reference indices n .. n+k-1, x* = x.  PBF_ERR_CAPACITY past the capacity
+ * (the reference throws), PBF_ERR_STATE on a batch of scenes.
+ * pbf_construct_fluid replaces Particles::construct_fluid (particles.h:231-250):
+ * the lattice of the box at particle_rest_spacing, z outer / x inner, point =
+ * index*spacing + min + spacing/2, all with `velocity` (NULL: zero); *added =
+ * the count.  The reference's emitter (distributor.h:357-369) is this call on
+ * the box of extent 1.1*spacing centred at the emitter, once per step while
+ * it is active.  A changed count drops the captured step graphs. */
+int pbf_add_particles(pbf_ctx* ctx, const float* x, const float* v, size_t k);
+int pbf_construct_fluid(pbf_ctx* ctx, const float fluid_min[3], const float fluid_max[3],
+                        const float velocity[3], size_t* added);
+/* Steps advanced by pbf_step on this context (restored by pbf_load_state). */
+uint64_t pbf_step_count(const pbf_ctx* ctx);
+
+/* ---- state files: output frames and checkpoints ----
+ * No counterpart in the reference (its output path is the renderer sync and
+ * ADIOS, distributor.h:742-750, adios_writer.h; it has no checkpoint).  One
+ * little-endian file: an 80-byte header
+ *   char magic[8] = "PBFSTATE"; uint32 version = 1; uint32 sizeof(pbf_params);
+ *   uint64 n; uint64 steps; uint32 flags (bit 0: network present); uint32 0;
+ *   pbf_tuning (5 + 5 int32)
+ * then the pbf_params block, then in the reference's particle order
+ *   float x[n][3], v[n][3], density[n], lambda[n], lambda_history[n]
+ * (lambda_history: the lambda the learned solver applied in the last step),
+ * then, with flag bit 0, float network[PBF_MLP_PARAMS], norm[PBF_MLP_NORM].
+ * pbf_load_state restores parameters, launch shapes, particles and network
+ * into a context with room for them; the steps that follow are bit-identical
+ * to those the saved context would have taken. */
+int pbf_save_state(pbf_ctx* ctx, const char* path);
+int pbf_load_state(pbf_ctx* ctx, const char* path);
 
 /* ---- batched scenes ----
  * No counterpart in the reference (one scene per process there).  One context

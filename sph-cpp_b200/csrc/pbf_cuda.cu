@@ -106,6 +106,32 @@ __global__ void k_upload(int n, const float* __restrict__ x, const float* __rest
   origH[i] = (uint32_t)i;
 }
 
+// Particles::add (particles.h:184-199) for k particles at the end: slots and
+// reference indices n0 .. n0+k-1, x* = x, v given or zero; the dummy slot
+// moves to the new end.
+__global__ void k_append(int n0, int k, const float* __restrict__ x, const float* __restrict__ v, float4* posH,
+                         float4* pstH, float4* velH, float4* scrH, float* lamH, float* lamsumH, uint32_t* origH,
+                         float4* pstS, float4* xl, float4* velS, float4* velT) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = n0 + k;
+  if (i == 0) {
+    pstS[n] = make_float4(kFar, kFar, kFar, 0.0f);
+    xl[n] = make_float4(kFar, kFar, kFar, 0.0f);
+    velS[n] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+    velT[n] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+  }
+  if (i >= k) return;
+  const int a = n0 + i;
+  const float4 p = make_float4(x[3 * i], x[3 * i + 1], x[3 * i + 2], 0.0f);
+  posH[a] = p;
+  pstH[a] = p;
+  velH[a] = v ? make_float4(v[3 * i], v[3 * i + 1], v[3 * i + 2], 0.0f) : make_float4(0.f, 0.f, 0.f, 0.f);
+  scrH[a] = make_float4(0.f, 0.f, 0.f, 0.f);
+  lamH[a] = 0.0f;
+  lamsumH[a] = 0.0f;
+  origH[a] = (uint32_t)a;
+}
+
 // Home slot order -> reference order, AoS float3.
 __global__ void k_unpermute_vec(int n, const float4* __restrict__ src, const uint32_t* __restrict__ orig,
                                 float* dst) {
@@ -1376,6 +1402,7 @@ struct pbf_ctx {
   float label_scale = 1.0f;
   int adam_t = 0;
   bool mlp_ready = false;
+  uint64_t steps_done = 0;  // steps advanced by pbf_step (saved with the state)
   // launch shapes of the fast gather families, and the persistent grids of
   // the learned solver's skippable launches (SMs x resident blocks)
   pbf_tuning tune{{8, 8, 8, 8, 8}, {kBlock, kBlock, kBlock, kBlock, kBlock}};
@@ -2232,6 +2259,169 @@ int pbf_set_array(pbf_ctx* ctx, int which, const float* host_in) {
   return PBF_OK;
 }
 
+// ---- growing the particle set ----
+int pbf_add_particles(pbf_ctx* ctx, const float* x, const float* v, size_t k) {
+  if (!ctx || (!x && k)) return ctx ? fail(ctx, PBF_ERR_ARG, "null positions") : PBF_ERR_ARG;
+  if (!ctx->scenes.empty()) return fail(ctx, PBF_ERR_STATE, "the scenes of a batch have fixed particle counts");
+  if (k == 0) return PBF_OK;
+  if (ctx->n + k > ctx->capacity)
+    return fail(ctx, PBF_ERR_CAPACITY, "Not enough capacity: %zu particles > capacity %zu", ctx->n + k,
+                ctx->capacity);
+  float* dx = ctx->stage;
+  float* dv = ctx->stage + 3 * ctx->capacity;
+  CK(cudaMemcpyAsync(dx, x, k * 3 * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  if (v) CK(cudaMemcpyAsync(dv, v, k * 3 * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  k_append<<<blocks_for(k), kBlock, 0, ctx->stream>>>((int)ctx->n, (int)k, dx, v ? dv : nullptr, ctx->posH,
+                                                      ctx->pstH, ctx->velH, ctx->scrH, ctx->lamH, ctx->lamsumH,
+                                                      ctx->origH, ctx->pstS, ctx->xl, ctx->velS, ctx->velT);
+  if (int rc = check_launch(ctx, "add_particles")) return rc;
+  CK(cudaStreamSynchronize(ctx->stream));  // the host buffers may go once this returns
+  ctx->n += k;
+  ctx->lists_valid = false;
+  drop_graphs(ctx);
+  return PBF_OK;
+}
+
+int pbf_construct_fluid(pbf_ctx* ctx, const float fluid_min[3], const float fluid_max[3], const float velocity[3],
+                        size_t* added) {
+  if (added) *added = 0;
+  if (!ctx || !fluid_min || !fluid_max) return PBF_ERR_ARG;
+  int64_t d[3];
+  if (int rc = pbf_lattice_dims(fluid_min, fluid_max, ctx->params.particle_rest_spacing, d))
+    return fail(ctx, rc, "particle_rest_spacing must be > 0");
+  const size_t k = (size_t)(d[0] * d[1] * d[2]);
+  if (k == 0) return PBF_OK;
+  if (ctx->n + k > ctx->capacity)
+    return fail(ctx, PBF_ERR_CAPACITY, "Not enough capacity: %zu particles > capacity %zu", ctx->n + k,
+                ctx->capacity);
+  std::vector<float> x(3 * k), v(3 * k, 0.0f);
+  if (int rc = pbf_build_lattice(fluid_min, d, ctx->params.particle_rest_spacing, 0.0f, 0, x.data()))
+    return fail(ctx, rc, "lattice construction failed");
+  if (velocity)
+    for (size_t i = 0; i < k; ++i)
+      for (int a = 0; a < 3; ++a) v[3 * i + a] = velocity[a];
+  if (int rc = pbf_add_particles(ctx, x.data(), v.data(), k)) return rc;
+  if (added) *added = k;
+  return PBF_OK;
+}
+
+uint64_t pbf_step_count(const pbf_ctx* ctx) { return ctx ? ctx->steps_done : 0; }
+
+// ---- the state file (output frames, checkpoints) ----
+namespace {
+constexpr char kStateMagic[8] = {'P', 'B', 'F', 'S', 'T', 'A', 'T', 'E'};
+constexpr uint32_t kStateVersion = 1;
+struct StateHeader {
+  char magic[8];
+  uint32_t version;
+  uint32_t params_bytes;
+  uint64_t n;
+  uint64_t steps;
+  uint32_t flags;  // bit 0: the learned warm start's network follows the arrays
+  uint32_t reserved;
+  pbf_tuning tuning;
+};
+struct FileCloser {
+  FILE* f;
+  ~FileCloser() {
+    if (f) std::fclose(f);
+  }
+};
+}  // namespace
+
+int pbf_save_state(pbf_ctx* ctx, const char* path) {
+  if (!ctx || !path) return PBF_ERR_ARG;
+  const size_t n = ctx->n;
+  std::vector<float> x(3 * n), v(3 * n), rho(n), lam(n), hist(n);
+  if (n) {
+    if (int rc = pbf_download(ctx, x.data(), v.data(), rho.data(), lam.data())) return rc;
+    k_unpermute_w<<<blocks_for(n), kBlock, 0, ctx->stream>>>((int)n, nullptr, ctx->lamsumH, ctx->origH, ctx->stage);
+    if (int rc = check_launch(ctx, "save_state")) return rc;
+    CK(cudaMemcpyAsync(hist.data(), ctx->stage, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  std::vector<float> net, norm;
+  if (ctx->mlp_ready) {
+    net.resize(pbf::kMlpParams);
+    norm.resize(PBF_MLP_NORM);
+    if (int rc = pbf_mlp_get(ctx, net.data(), norm.data())) return rc;
+  }
+  StateHeader h{};
+  std::memcpy(h.magic, kStateMagic, 8);
+  h.version = kStateVersion;
+  h.params_bytes = (uint32_t)sizeof(pbf_params);
+  h.n = n;
+  h.steps = ctx->steps_done;
+  h.flags = ctx->mlp_ready ? 1u : 0u;
+  h.tuning = ctx->tune;
+  FileCloser fc{std::fopen(path, "wb")};
+  if (!fc.f) return fail(ctx, PBF_ERR_IO, "cannot open %s for writing", path);
+  bool ok = std::fwrite(&h, sizeof(h), 1, fc.f) == 1 && std::fwrite(&ctx->params, sizeof(pbf_params), 1, fc.f) == 1;
+  auto put = [&](const std::vector<float>& a) {
+    if (ok && !a.empty()) ok = std::fwrite(a.data(), sizeof(float), a.size(), fc.f) == a.size();
+  };
+  put(x);
+  put(v);
+  put(rho);
+  put(lam);
+  put(hist);
+  put(net);
+  put(norm);
+  if (!ok || std::fflush(fc.f) != 0) return fail(ctx, PBF_ERR_IO, "short write to %s", path);
+  return PBF_OK;
+}
+
+int pbf_load_state(pbf_ctx* ctx, const char* path) {
+  if (!ctx || !path) return PBF_ERR_ARG;
+  FileCloser fc{std::fopen(path, "rb")};
+  if (!fc.f) return fail(ctx, PBF_ERR_IO, "cannot open %s", path);
+  StateHeader h{};
+  pbf_params p{};
+  if (std::fread(&h, sizeof(h), 1, fc.f) != 1 || std::memcmp(h.magic, kStateMagic, 8) != 0)
+    return fail(ctx, PBF_ERR_IO, "%s is not a PBF state file", path);
+  if (h.version != kStateVersion || h.params_bytes != sizeof(pbf_params))
+    return fail(ctx, PBF_ERR_IO, "%s: state version %u / parameter block %u bytes, this library reads %u / %zu", path,
+                h.version, h.params_bytes, kStateVersion, sizeof(pbf_params));
+  if (std::fread(&p, sizeof(p), 1, fc.f) != 1) return fail(ctx, PBF_ERR_IO, "%s: truncated", path);
+  if (h.n > ctx->capacity)
+    return fail(ctx, PBF_ERR_CAPACITY, "Not enough capacity: %llu particles > capacity %zu",
+                (unsigned long long)h.n, ctx->capacity);
+  const size_t n = (size_t)h.n;
+  std::vector<float> x(3 * n), v(3 * n), rho(n), lam(n), hist(n);
+  bool ok = true;
+  auto get = [&](std::vector<float>& a) {
+    if (ok && !a.empty()) ok = std::fread(a.data(), sizeof(float), a.size(), fc.f) == a.size();
+  };
+  get(x);
+  get(v);
+  get(rho);
+  get(lam);
+  get(hist);
+  std::vector<float> net, norm;
+  if (h.flags & 1u) {
+    net.resize(pbf::kMlpParams);
+    norm.resize(PBF_MLP_NORM);
+    get(net);
+    get(norm);
+  }
+  if (!ok) return fail(ctx, PBF_ERR_IO, "%s: truncated", path);
+  int rc;
+  if ((rc = pbf_set_params(ctx, &p)) || (rc = pbf_set_tuning(ctx, &h.tuning)) ||
+      (rc = pbf_upload(ctx, x.data(), v.data(), n)))
+    return rc;
+  if (n) {
+    if ((rc = pbf_set_array(ctx, PBF_ARRAY_DENSITIES, rho.data())) ||
+        (rc = pbf_set_array(ctx, PBF_ARRAY_LAMBDAS, lam.data())))
+      return rc;
+    // after an upload the slots are in reference order
+    CK(cudaMemcpyAsync(ctx->lamsumH, hist.data(), n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  if ((h.flags & 1u) && (rc = pbf_mlp_set(ctx, net.data(), norm.data()))) return rc;
+  ctx->steps_done = h.steps;
+  return PBF_OK;
+}
+
 int pbf_download(pbf_ctx* ctx, float* x, float* v, float* rho, float* lambda) {
   if (!ctx) return PBF_ERR_ARG;
   if (ctx->n == 0) return PBF_OK;
@@ -2413,6 +2603,7 @@ int pbf_step(pbf_ctx* ctx, int nsteps) {
     ctx->lists_valid = true;  // an empty set has (empty) lists
     return PBF_OK;
   }
+  ctx->steps_done += (uint64_t)nsteps;
   if (ctx->timing) {
     for (int i = 0; i < nsteps; ++i) launch_step(ctx);
     int rc = check_launch(ctx, "step");

@@ -59,6 +59,38 @@ class Particles:
     def batch(cls, batch) -> "Particles":
         return cls(batch.params(), 0, scenes=batch.scene_structs())
 
+    # -- growing the set, state files --
+    def add_particles(self, x: np.ndarray, v: np.ndarray | None = None) -> None:
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, 3)
+        if v is not None:
+            v = np.ascontiguousarray(v, dtype=np.float32).reshape(-1, 3)
+        self._check(self._lib.pbf_add_particles(self._ctx, _ptr(x), _ptr(v), x.shape[0]), "add_particles")
+
+    def construct_fluid(self, fluid_min, fluid_max, velocity=(0.0, 0.0, 0.0)) -> int:
+        """Particles::construct_fluid: append the lattice of the box; returns the count added."""
+        mn, mx, vel = (C.c_float * 3)(*fluid_min), (C.c_float * 3)(*fluid_max), (C.c_float * 3)(*velocity)
+        added = C.c_size_t()
+        self._check(self._lib.pbf_construct_fluid(self._ctx, mn, mx, vel, C.byref(added)), "construct_fluid")
+        return int(added.value)
+
+    def emit(self, center, velocity=(0.0, 0.0, 0.0)) -> int:
+        """The reference's emitter (distributor.h:357-369): construct_fluid on the
+        box of extent 1.1 * spacing centred at `center`; call before each step."""
+        sp = np.float32(self.params().particle_rest_spacing)
+        ext = np.float32(1.1) * sp
+        mn = [np.float32(c) - np.float32(0.5) * ext for c in center]
+        mx = [m + ext for m in mn]
+        return self.construct_fluid(mn, mx, velocity)
+
+    def step_count(self) -> int:
+        return int(self._lib.pbf_step_count(self._ctx))
+
+    def save_state(self, path) -> None:
+        self._check(self._lib.pbf_save_state(self._ctx, str(path).encode()), "save_state")
+
+    def load_state(self, path) -> None:
+        self._check(self._lib.pbf_load_state(self._ctx, str(path).encode()), "load_state")
+
     def scene_count(self) -> int:
         return int(self._lib.pbf_scene_count(self._ctx))
 

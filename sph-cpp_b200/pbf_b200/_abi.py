@@ -167,6 +167,11 @@ SIGNATURES = {
     "pbf_kernel_times": (_i, [_vp, _i, _P(C.c_char_p), _P(C.c_int64), _P(C.c_double), _P(C.c_int)]),
     "pbf_reset_timing": (_i, [_vp]),
     "pbf_launches_per_step": (_i, [_vp, _P(C.c_int64)]),
+    "pbf_add_particles": (_i, [_vp, _vp, _vp, _sz]),
+    "pbf_construct_fluid": (_i, [_vp, _P(C.c_float), _P(C.c_float), _P(C.c_float), _P(_sz)]),
+    "pbf_step_count": (C.c_uint64, [_vp]),
+    "pbf_save_state": (_i, [_vp, C.c_char_p]),
+    "pbf_load_state": (_i, [_vp, C.c_char_p]),
     "pbf_create_batch": (_i, [_P(PbfParams), _P(PbfScene), _i, _P(_vp)]),
     "pbf_scene_count": (_i, [_vp]),
     "pbf_scene_stats": (_i, [_vp, _i, _P(PbfStats)]),
