@@ -64,6 +64,20 @@ class Particles {
     return out;
   }
 
+  // particles.h:184-199 (add) and 231-250 (construct_fluid): append particles;
+  // throws past the capacity, as the reference does.
+  void add(const float* x_aos, const float* v_aos, std::size_t k) { check(pbf_add_particles(ctx_, x_aos, v_aos, k)); }
+  std::size_t construct_fluid(const float fluid_min[3], const float fluid_max[3],
+                              const float velocity[3] = nullptr) {
+    std::size_t added = 0;
+    check(pbf_construct_fluid(ctx_, fluid_min, fluid_max, velocity, &added));
+    return added;
+  }
+
+  // Output frames and checkpoints (pbf.h: state files).
+  void save(const char* path) { check(pbf_save_state(ctx_, path)); }
+  void load(const char* path) { check(pbf_load_state(ctx_, path)); }
+
   // The stages.
   template <class S> void apply_external_forces(const S& s) { check(pbf_apply_external_forces(ctx_, s.begin, s.end)); }
   template <class S> void predict_positions(const S& s) { check(pbf_predict_positions(ctx_, s.begin, s.end)); }

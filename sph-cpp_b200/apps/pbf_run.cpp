@@ -7,10 +7,14 @@
 // (--fused) through the graph-captured step — and prints statistics.
 //
 //   pbf_run params.ini [steps] [--fused] [--jitter AMP] [--seed S] [--dump out.bin]
+//           [--save state.pbf] [--resume state.pbf] [--frames K PREFIX]
 //
 // --dump writes the final positions and velocities as raw float32 AoS
-// (N x 3 each, after a uint64 N): the headless stand-in for the reference's
-// renderer gather / ADIOS position output (distributor.h:742-750).
+// (N x 3 each, after a uint64 N); --frames writes a state file (pbf.h) every
+// K steps as PREFIX_<step>.pbf: the headless stand-ins for the reference's
+// renderer gather / ADIOS position output (distributor.h:742-750).  --save
+// writes the final state, --resume starts from a state file instead of the
+// INI's initial fluid (the parameters then come from the file).
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -31,11 +35,21 @@ int main(int argc, char* argv[]) {
     float jitter = 0.0f;
     uint64_t seed = 0;
     const char* dump = nullptr;
+    const char* save = nullptr;
+    const char* resume = nullptr;
+    const char* frame_prefix = nullptr;
+    int frame_every = 0;
     for (int i = 2; i < argc; ++i) {
       if (!std::strcmp(argv[i], "--fused")) fused = true;
       else if (!std::strcmp(argv[i], "--jitter") && i + 1 < argc) jitter = (float)std::atof(argv[++i]);
       else if (!std::strcmp(argv[i], "--seed") && i + 1 < argc) seed = std::strtoull(argv[++i], nullptr, 10);
       else if (!std::strcmp(argv[i], "--dump") && i + 1 < argc) dump = argv[++i];
+      else if (!std::strcmp(argv[i], "--save") && i + 1 < argc) save = argv[++i];
+      else if (!std::strcmp(argv[i], "--resume") && i + 1 < argc) resume = argv[++i];
+      else if (!std::strcmp(argv[i], "--frames") && i + 2 < argc) {
+        frame_every = std::atoi(argv[++i]);
+        frame_prefix = argv[++i];
+      }
     }
     pbf_params raw;
     float fmin[3], fmax[3];
@@ -46,16 +60,41 @@ int main(int argc, char* argv[]) {
     float rho0 = 0.0f;
     if (pbf_lattice_rest_density(&raw, raw.particle_rest_spacing, &rho0) == PBF_OK) raw.rest_density = rho0;
     auto* parameters = new sim::gpu::Parameters(raw);
-    int64_t dims[3];
-    pbf_lattice_dims(fmin, fmax, raw.particle_rest_spacing, dims);
-    const size_t n = (size_t)(dims[0] * dims[1] * dims[2]);
-    std::vector<float> x(3 * n), v(3 * n, 0.0f);
-    pbf_build_lattice(fmin, dims, raw.particle_rest_spacing, jitter * raw.smoothing_radius, seed, x.data());
-    auto* particles = new sim::gpu::Particles(parameters->raw(), n);
-    particles->upload(x.data(), v.data(), n);
+    size_t n = 0;
+    std::vector<float> x, v;
+    sim::gpu::Particles* particles = nullptr;
+    if (resume) {
+      // the particle count is the uint64 at byte 16 of the state file's header
+      FILE* f = std::fopen(resume, "rb");
+      uint64_t nn = 0;
+      const bool ok = f && std::fseek(f, 16, SEEK_SET) == 0 && std::fread(&nn, sizeof(nn), 1, f) == 1;
+      if (f) std::fclose(f);
+      if (!ok) throw std::runtime_error(std::string("cannot read ") + resume);
+      n = (size_t)nn;
+      particles = new sim::gpu::Particles(parameters->raw(), n > 0 ? n : 1);
+      particles->load(resume);
+      x.resize(3 * n);
+      v.resize(3 * n);
+    } else {
+      int64_t dims[3];
+      pbf_lattice_dims(fmin, fmax, raw.particle_rest_spacing, dims);
+      n = (size_t)(dims[0] * dims[1] * dims[2]);
+      x.assign(3 * n, 0.0f);
+      v.assign(3 * n, 0.0f);
+      pbf_build_lattice(fmin, dims, raw.particle_rest_spacing, jitter * raw.smoothing_radius, seed, x.data());
+      particles = new sim::gpu::Particles(parameters->raw(), n);
+      particles->upload(x.data(), v.data(), n);
+    }
 
     const sim::gpu::IndexSpan resident_span{0, n}, local_span{0, n};
+    const uint64_t first_step = pbf_step_count(particles->handle());  // > 0 after --resume of a fused run
     for (int frame = 0; frame < steps; ++frame) {
+      if (frame_every > 0 && frame % frame_every == 0) {
+        char name[4096];
+        std::snprintf(name, sizeof(name), "%s_%06llu.pbf", frame_prefix,
+                      (unsigned long long)(first_step + (uint64_t)frame));
+        particles->save(name);
+      }
       if (fused) {
         particles->step(1);
         continue;
@@ -83,6 +122,7 @@ int main(int argc, char* argv[]) {
                 "com %.7g %.7g %.7g mean_neighbors %.4f flags %u\n",
                 n, steps, st.mean_density_error, st.max_density_error, st.kinetic_energy, st.center_of_mass[0],
                 st.center_of_mass[1], st.center_of_mass[2], st.mean_neighbors, st.error_flags);
+    if (save) particles->save(save);
     if (dump) {
       particles->download(x.data(), v.data());
       FILE* f = std::fopen(dump, "wb");

@@ -82,3 +82,27 @@ def test_stage_loop_equals_fused_step(tmp_path):
     assert np.array_equal(x1, x2)
     assert np.array_equal(v1, v2)
     assert "flags 0" in out1 and "flags 0" in out2
+
+
+@pytest.mark.gpu
+def test_driver_save_resume_and_frames(tmp_path):
+    """--save / --resume through state files: 4 + 3 resumed steps equal 7
+    straight steps bit for bit; --frames writes one state file per K steps."""
+    ini = tmp_path / "dam.ini"
+    ini.write_text(INI)
+
+    def run(*args):
+        r = subprocess.run([str(APP), str(ini), *map(str, args)], capture_output=True, text=True, timeout=120)
+        assert r.returncode == 0, r.stdout + r.stderr
+        return r.stdout
+
+    run(7, "--fused", "--jitter", "0.005", "--seed", "7", "--dump", tmp_path / "straight.bin")
+    run(4, "--fused", "--jitter", "0.005", "--seed", "7", "--save", tmp_path / "mid.pbf",
+        "--frames", 2, tmp_path / "frame")
+    run(3, "--fused", "--resume", tmp_path / "mid.pbf", "--dump", tmp_path / "resumed.bin")
+    a = (tmp_path / "straight.bin").read_bytes()
+    b = (tmp_path / "resumed.bin").read_bytes()
+    assert a == b
+    frames = sorted(p.name for p in tmp_path.glob("frame_*.pbf"))
+    assert frames == ["frame_000000.pbf", "frame_000002.pbf"]
+    assert (tmp_path / "frame_000002.pbf").read_bytes()[:8] == b"PBFSTATE"
