@@ -49,6 +49,10 @@ using pbf::Fast;
 namespace {
 
 constexpr int kBlock = 256;
+// density/lambda and delta-p are held to 42 registers (6 blocks of kBlock, or
+// 12 of the autotuned 128, per SM): measured faster than at their natural
+// 44-48; the other gathers are faster as the compiler leaves them.
+constexpr int kGatherMinBlocks = 6;
 constexpr int kScanThreads = 1024;
 constexpr int kScanItems = 4;
 constexpr int kScanTile = kScanThreads * kScanItems;
@@ -764,7 +768,7 @@ __device__ __forceinline__ void density_lambda_tile(int tile, const Dev& P, cons
 // The residual check runs on a persistent grid walking the tiles, so that
 // once the step has converged the launch costs a few hundred empty blocks.
 template <int MODE, int GL>
-__global__ void __launch_bounds__(kBlock) kf_density_lambda(Dev P, Fast F, int n, size_t stride,
+__global__ void __launch_bounds__(kBlock, kGatherMinBlocks) kf_density_lambda(Dev P, Fast F, int n, size_t stride,
                                                             const int32_t* __restrict__ nbr,
                                                             const int32_t* __restrict__ cnt,
                                                             const float4* __restrict__ pst, float4* xl, float4* vel,
@@ -1191,7 +1195,7 @@ __device__ __forceinline__ void dp_update_tile(int tile, const Dev& P, const Fas
 // COND launches (the learned solver's extra iterations) use a persistent grid
 // and skip the whole launch once the step has converged.
 template <bool SCORR, bool LAST, bool COND, int GL>
-__global__ void __launch_bounds__(kBlock) kf_dp_update(Dev P, Fast F, int n, size_t stride,
+__global__ void __launch_bounds__(kBlock, kGatherMinBlocks) kf_dp_update(Dev P, Fast F, int n, size_t stride,
                                                        const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
                                                        const float4* __restrict__ xl, float4* pst,
                                                        const float4* __restrict__ pos, float4* vel,
