@@ -536,7 +536,7 @@ def main():
                          "step_gbs": step_bytes / (t_dev / K) / 1e9},
             "kernels": kernels,
             "autotune_ms_per_step": None if tune_table is None else
-            {f"{l}x{b}": v for (l, b), v in tune_table.items()},
+            {f"{l}x{b}{'staged' if st else ''}": v for (l, b, st), v in tune_table.items()},
             "physics": {"mean_neighbors": nbar, "cap_hits": st["cap_hits"],
                         "mean_density_error": st["mean_density_error"], "error_flags": st["error_flags"],
                         "finite": ok},

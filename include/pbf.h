@@ -108,6 +108,8 @@ typedef struct pbf_stats_t {
   uint32_t error_flags;       /* PBF_FLAG_* bits raised since the last pbf_stats */
   uint32_t solver_iterations; /* Jacobi iterations the last step ran */
   double solver_residual;     /* learned solver: mean clamped density error at its last check */
+  uint32_t tiles;             /* 32-particle tiles of the last list fill that wrote staging (0: none) */
+  uint32_t tiles_staged;      /* of those, the tiles the staged gathers read from shared memory */
 } pbf_stats_t;
 
 typedef struct pbf_ctx pbf_ctx;
@@ -253,10 +255,10 @@ uint64_t pbf_step_count(const pbf_ctx* ctx);
 /* ---- state files: output frames and checkpoints ----
  * No counterpart in the reference (its output path is the renderer sync and
  * ADIOS, distributor.h:742-750, adios_writer.h; it has no checkpoint).  One
- * little-endian file: an 80-byte header
+ * little-endian file: a 104-byte header
  *   char magic[8] = "PBFSTATE"; uint32 version = 1; uint32 sizeof(pbf_params);
  *   uint64 n; uint64 steps; uint32 flags (bit 0: network present); uint32 0;
- *   pbf_tuning (5 + 5 int32)
+ *   pbf_tuning (3 x 5 int32); uint32 0
  * then the pbf_params block, then in the reference's particle order
  *   float x[n][3], v[n][3], density[n], lambda[n], lambda_history[n]
  * (lambda_history: the lambda the learned solver applied in the last step),
@@ -297,9 +299,13 @@ int pbf_scene_stats(pbf_ctx* ctx, int scene, pbf_stats_t* out);
  * No counterpart in the reference (its loops are OpenMP for_each_index).
  * Each family of gather kernels runs with `lanes` threads per particle
  * walking one neighbor list together (4 or 8) in blocks of `block` threads
- * (128 or 256).  The shape changes only the order of floating-point sums
- * inside a particle (fast math), never the lists; exact_math kernels run one
- * thread per particle and ignore it.  Default: 8 lanes, 256 threads. */
+ * (128 or 256), either reading the neighbours' records from global memory or,
+ * `staged` (4 lanes, 128 threads only), from shared memory: each block copies
+ * the neighbour bins of its 32-particle tile there first and walks 16-bit
+ * lists of staging indices the list fill writes beside the int32 lists.  The
+ * shape changes only the order of floating-point sums inside a particle (fast
+ * math), never the lists; exact_math kernels run one thread per particle and
+ * ignore it.  Default: 8 lanes, 256 threads, not staged. */
 enum {
   PBF_TUNE_DENSITY = 0,          /* density + lambda, and the learned solver's residual check */
   PBF_TUNE_DELTA_P = 1,          /* position delta + x* update */
@@ -308,10 +314,11 @@ enum {
   PBF_TUNE_APPLY_VORTICITY = 4,
   PBF_TUNE_FAMILIES = 5
 };
-#define PBF_TUNE_CANDIDATES 4  /* (lanes, block) = (4,128) (4,256) (8,128) (8,256) */
+#define PBF_TUNE_CANDIDATES 5  /* (lanes, block, staged) = (4,128,0) (4,256,0) (8,128,0) (8,256,0) (4,128,1) */
 typedef struct {
   int lanes[PBF_TUNE_FAMILIES];
   int block[PBF_TUNE_FAMILIES];
+  int staged[PBF_TUNE_FAMILIES];
 } pbf_tuning;
 int pbf_get_tuning(const pbf_ctx* ctx, pbf_tuning* out);
 /* PBF_ERR_ARG for a shape outside the candidates; drops captured graphs. */

@@ -480,15 +480,34 @@ __global__ void k_reorder(int n, const unsigned long long* __restrict__ pairs, c
 // float re-hash still decides which bins are visited.
 constexpr int kFillBlock = 128;
 
+// Tiles of kTile consecutive sorted slots (one warp of the list fill, one
+// block of the staged gathers).  A tile's neighbour bins lie in the bounding
+// box of its own bins grown by one bin; every (y, z) row of that box is one
+// contiguous slot run (bins of a row have consecutive keys), so a staged
+// gather copies at most kTileRuns runs, kStageMax records, to shared memory.
+constexpr int kTile = 32, kTileRuns = 16, kStageMax = 1024;
+
+// Staging descriptors of the tiles (written by the list fill).
+struct TileIO {
+  int32_t* nruns;   // [tiles] runs of the tile; 0: not staged (the gathers walk the int32 lists)
+  int32_t* total;   // [tiles] staged records
+  int4* runs;       // [tiles][kTileRuns] (first slot, records, staging base, 0)
+  uint16_t* nbr16;  // [slot][stride] staging index of every list entry
+};
+
+template <bool STAGE>
 __global__ void __launch_bounds__(kFillBlock) k_fill2(Dev P, int n, size_t stride, const float4* __restrict__ pst,
                                                       const uint32_t* __restrict__ cell_start, int32_t* nbr,
-                                                      int32_t* cnt, uint32_t* err) {
+                                                      int32_t* cnt, uint32_t* err, TileIO T) {
   const int b = blockIdx.x * kFillBlock + threadIdx.x;
-  if (b >= n) return;
-  const float4 xp = pst[b];
+  if (!STAGE && b >= n) return;
+  if (STAGE && (b & ~(kTile - 1)) >= n) return;  // a whole warp past the end: no tile (warp-uniform)
+  const bool live = b < n;
+  const int bb = live ? b : n - 1;  // the lanes past the end of the last tile mirror the last particle
+  const float4 xp = pst[bb];
   const int cap = P.cap;
   const float s = P.s;
-  const pbf::Region R = pbf::region_of(P, b);
+  const pbf::Region R = pbf::region_of(P, bb);
   int32_t* row = nbr + (size_t)b * stride;
   // calculate_neighbor_indices (neighbors.h:172-185): the bin of coord + i*s
   // per axis for i = -1, 0, 1, in the reference's float operations.  The 27
@@ -501,6 +520,55 @@ __global__ void __launch_bounds__(kFillBlock) k_fill2(Dev P, int n, size_t strid
     by[i] = pbf::dev_axis_bin(pbf::xadd(xp.y, o), s);
     bz[i] = pbf::dev_axis_bin(pbf::xadd(xp.z, o), s);
   }
+  const bool finite = isfinite(xp.x) && isfinite(xp.y) && isfinite(xp.z);
+  // The tile's staging runs (STAGE): warp-wide box of the own bins, one run
+  // per (y, z) row of the grown box, the runs' staging bases by a prefix sum.
+  __shared__ int soff[STAGE ? kFillBlock : 1];  // per lane: staging base - first slot of run `lane`
+  const int lane = threadIdx.x & 31, tile = b / kTile;
+  int xmn = 0, xmx = 0, ymn = 0, zmn = 0, ny = 0, nz = 0;
+  bool staged = false, stray = false;
+  uint16_t* row16 = STAGE ? T.nbr16 + (size_t)b * stride : nullptr;
+  if (STAGE) {
+    const unsigned full = 0xffffffffu;
+    const uint32_t key0 = __shfl_sync(full, R.key0, 0);  // every lane shuffles
+    const bool same = __all_sync(full, finite && R.key0 == key0);
+    xmn = __reduce_min_sync(full, (unsigned)bx[1] ^ 0x80000000u) ^ 0x80000000u;
+    xmx = __reduce_max_sync(full, (unsigned)bx[1] ^ 0x80000000u) ^ 0x80000000u;
+    ymn = __reduce_min_sync(full, (unsigned)by[1] ^ 0x80000000u) ^ 0x80000000u;
+    const int ymx = __reduce_max_sync(full, (unsigned)by[1] ^ 0x80000000u) ^ 0x80000000u;
+    zmn = __reduce_min_sync(full, (unsigned)bz[1] ^ 0x80000000u) ^ 0x80000000u;
+    const int zmx = __reduce_max_sync(full, (unsigned)bz[1] ^ 0x80000000u) ^ 0x80000000u;
+    ny = ymx - ymn + 3;
+    nz = zmx - zmn + 3;
+    staged = same && ny * nz <= kTileRuns;
+    int slot0 = 0, len = 0;
+    if (staged && lane < ny * nz) {
+      const int yr = ymn - 1 + lane % ny, zr = zmn - 1 + lane / ny;
+      const int x0 = max(xmn - 1, 0), x1 = min(xmx + 1, R.dimx - 1);
+      if (yr >= 0 && yr < R.dimy && zr >= 0 && zr < R.dimz && x0 <= x1) {
+        const uint32_t rk = R.key0 + (uint32_t)(R.dimx * R.dimy) * (uint32_t)zr + (uint32_t)yr * (uint32_t)R.dimx;
+        slot0 = (int)cell_start[rk + (uint32_t)x0];
+        len = (int)cell_start[rk + (uint32_t)x1 + 1u] - slot0;
+      }
+    }
+    int incl = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(full, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const int total = __shfl_sync(full, incl, 31);
+    const int base = incl - len;
+    staged = staged && total <= kStageMax;
+    soff[threadIdx.x] = base - slot0;
+    if (lane == 0) {
+      T.nruns[tile] = staged ? ny * nz : 0;
+      T.total[tile] = total;
+    }
+    if (staged && lane < ny * nz) T.runs[(size_t)tile * kTileRuns + lane] = make_int4(slot0, len, base, 0);
+    __syncwarp();
+    if (!live) return;
+  }
   // Per-axis distance from the particle to its own bin's faces, less the margin.
   const float lo[3] = {fmaxf(xp.x - ((float)bx[1] * s - s) - P.skip_eps, 0.f),
                        fmaxf(xp.y - ((float)by[1] * s - s) - P.skip_eps, 0.f),
@@ -508,7 +576,6 @@ __global__ void __launch_bounds__(kFillBlock) k_fill2(Dev P, int n, size_t strid
   const float hi[3] = {fmaxf(((float)(bx[1] + 1) * s - s) - xp.x - P.skip_eps, 0.f),
                        fmaxf(((float)(by[1] + 1) * s - s) - xp.y - P.skip_eps, 0.f),
                        fmaxf(((float)(bz[1] + 1) * s - s) - xp.z - P.skip_eps, 0.f)};
-  const bool finite = isfinite(xp.x) && isfinite(xp.y) && isfinite(xp.z);
   int count = 0;
 
   for (int i = 0; i < 3; i++) {
@@ -528,11 +595,20 @@ __global__ void __launch_bounds__(kFillBlock) k_fill2(Dev P, int n, size_t strid
           continue;
         const uint32_t nb =
             R.key0 + (uint32_t)(R.dimx * R.dimy) * (uint32_t)cz + ((uint32_t)cy * (uint32_t)R.dimx + (uint32_t)cx);
+        int off = 0;
+        if (STAGE && staged) {
+          const int ry = cy - (ymn - 1), rz = cz - (zmn - 1);
+          if (cx < xmn - 1 || cx > xmx + 1 || ry < 0 || ry >= ny || rz < 0 || rz >= nz) stray = true;
+          else off = soff[(threadIdx.x & ~31) + rz * ny + ry];
+        }
         const uint32_t q1 = cell_start[nb + 1];
         for (uint32_t q = cell_start[nb]; q < q1; ++q) {
           const float4 xq = pst[q];
           const float d2 = pbf::mag2<true>(pbf::xsub(xp.x, xq.x), pbf::xsub(xp.y, xq.y), pbf::xsub(xp.z, xq.z));
-          if (d2 < P.s2 && q != (uint32_t)b && count < cap) row[count++] = (int32_t)q;
+          if (d2 < P.s2 && q != (uint32_t)b && count < cap) {
+            if (STAGE && staged) row16[count] = (uint16_t)((int)q + off);
+            row[count++] = (int32_t)q;
+          }
         }
         if (count >= cap) goto done;
       }
@@ -540,6 +616,8 @@ __global__ void __launch_bounds__(kFillBlock) k_fill2(Dev P, int n, size_t strid
   }
 done:
   cnt[b] = count;
+  // a bin outside the tile's box (float re-hash at a bin face): the tile walks the int32 lists
+  if (STAGE && stray) T.nruns[tile] = 0;
 }
 
 // ---- density (particles.h:292-313) ----
@@ -698,11 +776,15 @@ struct DensitySums {
   float sw, s1x, s1y, s1z, s2, dmin, nh;
 };
 
-template <int GL, bool NH>
-__device__ __forceinline__ DensitySums density_sums(const Fast& F, const pbf::Group& G, const int32_t* row, int c,
-                                                    int n, const float4* __restrict__ pst, float4 xp) {
+// STAGED: the neighbour records come from the tile's staging area `src` in
+// shared memory through the 16-bit list row16; else from `src` in global
+// memory through the int32 list row.  `dummy` names the zero record.
+template <int GL, bool NH, bool STAGED = false>
+__device__ __forceinline__ DensitySums density_sums(const Fast& F, const pbf::Group& G, const int32_t* row,
+                                                    const uint16_t* row16, int c, int dummy, const float4* src,
+                                                    float4 xp) {
   DensitySums S{0.f, 0.f, 0.f, 0.f, 0.f, FLT_MAX, 0.f};
-  pbf::gwalk1<GL>(row, c, n, G.lane, pst, [&](int, float4 xq) {
+  auto body = [&](int, float4 xq) {
     const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
     const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
     S.dmin = fminf(S.dmin, d2);
@@ -714,7 +796,11 @@ __device__ __forceinline__ DensitySums density_sums(const Fast& F, const pbf::Gr
     S.s1y = fmaf(t, dy, S.s1y);
     S.s1z = fmaf(t, dz, S.s1z);
     S.s2 = fmaf(t * t, d2, S.s2);
-  });
+  };
+  if (STAGED)
+    pbf::swalk1<GL>(row16, c, dummy, G.lane, src, body);
+  else
+    pbf::gwalk1<GL>(row, c, dummy, G.lane, src, body);
   S.sw = pbf::gsum<GL>(S.sw);
   S.s1x = pbf::gsum<GL>(S.s1x);
   S.s1y = pbf::gsum<GL>(S.s1y);
@@ -725,16 +811,20 @@ __device__ __forceinline__ DensitySums density_sums(const Fast& F, const pbf::Gr
   return S;
 }
 
-template <int MODE, int GL>
+template <int MODE, int GL, bool STAGED = false>
 __device__ __forceinline__ void density_lambda_tile(int tile, const Dev& P, const Fast& F, int n, size_t stride,
                                                     const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
                                                     const float4* __restrict__ pst, float4* xl, float4* vel,
-                                                    float* lam, uint32_t* nudge, const LearnIO& io, float& err) {
+                                                    float* lam, uint32_t* nudge, const LearnIO& io, float& err,
+                                                    const uint16_t* nbr16 = nullptr, const float4* stage = nullptr,
+                                                    int staged = 0) {
   const pbf::Group G = pbf::group_at<GL>(n, tile);
   const int b = G.b;
   const float4 xp = pst[b];
   const int c = G.live ? cnt[b] : 0;
-  const DensitySums S = density_sums<GL, MODE == kDlRecord>(F, G, nbr + (size_t)b * stride, c, n, pst, xp);
+  const DensitySums S = density_sums<GL, MODE == kDlRecord, STAGED>(
+      F, G, nbr + (size_t)b * stride, STAGED ? nbr16 + (size_t)b * stride : nullptr, c, STAGED ? staged : n,
+      STAGED ? stage : pst, xp);
   const float rho = fmaf(F.m_poly, S.sw, F.m_w0);
   if (MODE == kDlCheck && G.live && G.lane == 0) err += fmaxf(fmaf(rho, F.inv_rho0, -1.0f), 0.0f);
   if (!G.live || G.lane != 0) return;
@@ -781,6 +871,65 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) kf_density_lambda(De
   if (MODE == kDlCheck) pbf::block_partial<kBlock>(err, io.partials + blockIdx.x);
 }
 
+// ---- staged gathers: one 32-particle tile per block of kStageThreads ----
+constexpr int kStageThreads = kTile * 4;  // 4 lanes per particle
+
+// Copy the tile's neighbour records (the runs of its descriptor) from a (and
+// b2 when B2) to shared memory, the zero record after them; every thread of
+// the block calls it.  Returns the staged count, or -1 for a tile the list
+// fill did not stage (its gathers then walk the int32 lists).
+template <bool B2>
+__device__ __forceinline__ int stage_tile(const TileIO& T, int tile, const float4* __restrict__ a, float4* sa,
+                                          const float4* __restrict__ b2, float4* sb) {
+  __shared__ int4 runs[kTileRuns];
+  __shared__ int hdr[2];
+  if (threadIdx.x < kTileRuns) runs[threadIdx.x] = T.runs[(size_t)tile * kTileRuns + threadIdx.x];
+  if (threadIdx.x == 0) {
+    hdr[0] = T.nruns[tile];
+    hdr[1] = T.total[tile];
+  }
+  __syncthreads();
+  const int nr = hdr[0], total = hdr[1];
+  if (nr > 0) {
+    for (int r = 0; r < nr; ++r) {
+      const int4 ru = runs[r];
+      for (int i = threadIdx.x; i < ru.y; i += blockDim.x) {
+        sa[ru.z + i] = a[ru.x + i];
+        if (B2) sb[ru.z + i] = b2[ru.x + i];
+      }
+    }
+    if (threadIdx.x == 0) {
+      sa[total] = make_float4(kFar, kFar, kFar, 0.0f);
+      if (B2) sb[total] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+    }
+  }
+  __syncthreads();
+  return nr > 0 ? total : -1;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kStageThreads) ks_density_lambda(Dev P, Fast F, int n, size_t stride,
+                                                                  const int32_t* __restrict__ nbr,
+                                                                  const int32_t* __restrict__ cnt,
+                                                                  const float4* __restrict__ pst, float4* xl,
+                                                                  float4* vel, float* lam, uint32_t* nudge, LearnIO io,
+                                                                  TileIO T) {
+  __shared__ float4 stage[kStageMax + 1];
+  if (MODE == kDlCheck && io.state->done) return;
+  const int tiles = (n + kTile - 1) / kTile;
+  float err = 0.0f;
+  for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const int staged = stage_tile<false>(T, tile, pst, stage, nullptr, nullptr);
+    if (staged >= 0)
+      density_lambda_tile<MODE, 4, true>(tile, P, F, n, stride, nbr, cnt, pst, xl, vel, lam, nudge, io, err, T.nbr16,
+                                         stage, staged);
+    else
+      density_lambda_tile<MODE, 4>(tile, P, F, n, stride, nbr, cnt, pst, xl, vel, lam, nudge, io, err);
+    __syncthreads();  // the next tile's staging overwrites the area
+  }
+  if (MODE == kDlCheck) pbf::block_partial<kStageThreads>(err, io.partials + blockIdx.x);
+}
+
 // Learned warm start, first Jacobi iteration, in two launches:
 // kl_features: the gather of kf_density_lambda, then per particle the 12
 // normalised features as a BF16 row of 16 (columns 12..15 are padding the
@@ -804,7 +953,7 @@ __global__ void __launch_bounds__(kBlock) kl_features(Dev P, Fast F, pbf::MlpDev
   const int b = G.b;
   const float4 xp = pst[b];
   const int c = G.live ? cnt[b] : 0;
-  const DensitySums S = density_sums<pbf::kGL, true>(F, G, nbr + (size_t)b * stride, c, n, pst, xp);
+  const DensitySums S = density_sums<pbf::kGL, true>(F, G, nbr + (size_t)b * stride, nullptr, c, n, pst, xp);
   if (!G.live || G.lane != 0) return;
   const float rho = fmaf(F.m_poly, S.sw, F.m_w0);
   const float L2 = F.lam_grad * F.lam_grad;
@@ -1155,18 +1304,29 @@ __global__ void __launch_bounds__(kBlock) k_apply_vorticity(Dev P, int n, size_t
 // ---- fast gathers (exact_math = 0), kGL lanes per particle, see pbf_fast.cuh ----
 // COND: the learned solver's extra iterations, skipped once the step has
 // converged; lamsum (when given) accumulates the applied lambda.
-template <bool SCORR, bool LAST, int GL>
+// Where a gather's neighbour records come from: the tile's staging area
+// (STAGED: shared memory through the 16-bit list) or global memory.
+struct Src {
+  const uint16_t* nbr16;  // STAGED: the 16-bit lists
+  const float4* a;        // first record array (staged copy or global)
+  const float4* b;        // second record array (two-record gathers)
+  int dummy;              // index of the zero record
+};
+
+template <bool SCORR, bool LAST, int GL, bool STAGED = false>
 __device__ __forceinline__ void dp_update_tile(int tile, const Dev& P, const Fast& F, int n, size_t stride,
                                                const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
                                                const float4* __restrict__ xl, float4* pst,
-                                               const float4* __restrict__ pos, float4* vel, float* lamsum) {
+                                               const float4* __restrict__ pos, float4* vel, float* lamsum,
+                                               Src src = Src{nullptr, nullptr, nullptr, 0}) {
   const pbf::Group G = pbf::group_at<GL>(n, tile);
   const int b = G.b;
   const float4 xp = xl[b];
   const int c = G.live ? cnt[b] : 0;
   float ax = 0.f, ay = 0.f, az = 0.f;
   const float lp = xp.w;
-  pbf::gwalk1<GL>(nbr + (size_t)b * stride, c, n, G.lane, xl, [&](int, float4 xq) {
+  pbf::walk1<GL, STAGED>(nbr + (size_t)b * stride, STAGED ? src.nbr16 + (size_t)b * stride : nullptr, c,
+                         STAGED ? src.dummy : n, G.lane, STAGED ? src.a : xl, [&](int, float4 xq) {
     const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
     const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
     float l = lp + xq.w;
@@ -1206,18 +1366,43 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) kf_dp_update(Dev P, 
     dp_update_tile<SCORR, LAST, GL>(tile, P, F, n, stride, nbr, cnt, xl, pst, pos, vel, lamsum);
 }
 
-template <bool FINAL, int GL>
-__global__ void __launch_bounds__(kBlock) kf_viscosity(Dev P, Fast F, int n, size_t stride,
-                                                       const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
-                                                       const float4* __restrict__ pst, const float4* __restrict__ vin,
-                                                       float4* vout, float4* posH, float4* pstH,
-                                                       const uint32_t* __restrict__ origS, uint32_t* origH) {
-  const pbf::Group G = pbf::group_of<GL>(n);
+template <bool SCORR, bool LAST, bool COND>
+__global__ void __launch_bounds__(kStageThreads) ks_dp_update(Dev P, Fast F, int n, size_t stride,
+                                                             const int32_t* __restrict__ nbr,
+                                                             const int32_t* __restrict__ cnt,
+                                                             const float4* __restrict__ xl, float4* pst,
+                                                             const float4* __restrict__ pos, float4* vel,
+                                                             const pbf::SolveState* __restrict__ state,
+                                                             float* lamsum, TileIO T) {
+  __shared__ float4 stage[kStageMax + 1];
+  if (COND && state->done) return;
+  const int tiles = (n + kTile - 1) / kTile;
+  for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const int staged = stage_tile<false>(T, tile, xl, stage, nullptr, nullptr);
+    if (staged >= 0)
+      dp_update_tile<SCORR, LAST, 4, true>(tile, P, F, n, stride, nbr, cnt, xl, pst, pos, vel, lamsum,
+                                           Src{T.nbr16, stage, nullptr, staged});
+    else
+      dp_update_tile<SCORR, LAST, 4>(tile, P, F, n, stride, nbr, cnt, xl, pst, pos, vel, lamsum);
+    __syncthreads();
+  }
+}
+
+template <bool FINAL, int GL, bool STAGED = false>
+__device__ __forceinline__ void viscosity_tile(int tile, const Fast& F, int n, size_t stride,
+                                               const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
+                                               const float4* __restrict__ pst, const float4* __restrict__ vin,
+                                               float4* vout, float4* posH, float4* pstH,
+                                               const uint32_t* __restrict__ origS, uint32_t* origH,
+                                               Src src = Src{nullptr, nullptr, nullptr, 0}) {
+  const pbf::Group G = pbf::group_at<GL>(n, tile);
   const int b = G.b;
   const float4 xp = pst[b], vp = vin[b];
   const int c = G.live ? cnt[b] : 0;
   float ax = 0.f, ay = 0.f, az = 0.f;
-  pbf::gwalk2<GL>(nbr + (size_t)b * stride, c, n, G.lane, pst, vin, [&](int, float4 xq, float4 vq) {
+  pbf::walk2<GL, STAGED>(nbr + (size_t)b * stride, STAGED ? src.nbr16 + (size_t)b * stride : nullptr, c,
+                         STAGED ? src.dummy : n, G.lane, STAGED ? src.a : pst, STAGED ? src.b : vin,
+                         [&](int, float4 xq, float4 vq) {
     const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
     const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
     const float wr = __fdividef(pbf::poly_cube(F, d2), vq.w);
@@ -1238,17 +1423,47 @@ __global__ void __launch_bounds__(kBlock) kf_viscosity(Dev P, Fast F, int n, siz
   }
 }
 
-template <int GL>
-__global__ void __launch_bounds__(kBlock) kf_vorticity(Dev P, Fast F, int n, size_t stride,
+template <bool FINAL, int GL>
+__global__ void __launch_bounds__(kBlock) kf_viscosity(Dev P, Fast F, int n, size_t stride,
                                                        const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
-                                                       const float4* __restrict__ pst, const float4* __restrict__ vel,
-                                                       float4* scr, float4* xl) {
-  const pbf::Group G = pbf::group_of<GL>(n);
+                                                       const float4* __restrict__ pst, const float4* __restrict__ vin,
+                                                       float4* vout, float4* posH, float4* pstH,
+                                                       const uint32_t* __restrict__ origS, uint32_t* origH) {
+  viscosity_tile<FINAL, GL>(blockIdx.x, F, n, stride, nbr, cnt, pst, vin, vout, posH, pstH, origS, origH);
+}
+
+template <bool FINAL>
+__global__ void __launch_bounds__(kStageThreads) ks_viscosity(Dev P, Fast F, int n, size_t stride,
+                                                             const int32_t* __restrict__ nbr,
+                                                             const int32_t* __restrict__ cnt,
+                                                             const float4* __restrict__ pst,
+                                                             const float4* __restrict__ vin, float4* vout,
+                                                             float4* posH, float4* pstH,
+                                                             const uint32_t* __restrict__ origS, uint32_t* origH,
+                                                             TileIO T) {
+  __shared__ float4 sa[kStageMax + 1], sb[kStageMax + 1];
+  const int tile = blockIdx.x;
+  const int staged = stage_tile<true>(T, tile, pst, sa, vin, sb);
+  if (staged >= 0)
+    viscosity_tile<FINAL, 4, true>(tile, F, n, stride, nbr, cnt, pst, vin, vout, posH, pstH, origS, origH,
+                                   Src{T.nbr16, sa, sb, staged});
+  else
+    viscosity_tile<FINAL, 4>(tile, F, n, stride, nbr, cnt, pst, vin, vout, posH, pstH, origS, origH);
+}
+
+template <int GL, bool STAGED = false>
+__device__ __forceinline__ void vorticity_tile(int tile, const Fast& F, int n, size_t stride,
+                                               const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
+                                               const float4* __restrict__ pst, const float4* __restrict__ vel,
+                                               float4* scr, float4* xl, Src src = Src{nullptr, nullptr, nullptr, 0}) {
+  const pbf::Group G = pbf::group_at<GL>(n, tile);
   const int b = G.b;
   const float4 xp = pst[b], vp = vel[b];
   const int c = G.live ? cnt[b] : 0;
   float wx = 0.f, wy = 0.f, wz = 0.f;
-  pbf::gwalk2<GL>(nbr + (size_t)b * stride, c, n, G.lane, pst, vel, [&](int, float4 xq, float4 vq) {
+  pbf::walk2<GL, STAGED>(nbr + (size_t)b * stride, STAGED ? src.nbr16 + (size_t)b * stride : nullptr, c,
+                         STAGED ? src.dummy : n, G.lane, STAGED ? src.a : pst, STAGED ? src.b : vel,
+                         [&](int, float4 xq, float4 vq) {
     const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
     const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
     const float t = pbf::spikey_over_r(F, d2);
@@ -1268,17 +1483,41 @@ __global__ void __launch_bounds__(kBlock) kf_vorticity(Dev P, Fast F, int n, siz
 }
 
 template <int GL>
-__global__ void __launch_bounds__(kBlock) kf_apply_vorticity(Dev P, Fast F, int n, size_t stride,
+__global__ void __launch_bounds__(kBlock) kf_vorticity(Dev P, Fast F, int n, size_t stride,
+                                                       const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
+                                                       const float4* __restrict__ pst, const float4* __restrict__ vel,
+                                                       float4* scr, float4* xl) {
+  vorticity_tile<GL>(blockIdx.x, F, n, stride, nbr, cnt, pst, vel, scr, xl);
+}
+
+__global__ void __launch_bounds__(kStageThreads) ks_vorticity(Dev P, Fast F, int n, size_t stride,
                                                              const int32_t* __restrict__ nbr,
                                                              const int32_t* __restrict__ cnt,
-                                                             const float4* __restrict__ xl,
-                                                             const float4* __restrict__ scr, float4* vel) {
-  const pbf::Group G = pbf::group_of<GL>(n);
+                                                             const float4* __restrict__ pst,
+                                                             const float4* __restrict__ vel, float4* scr, float4* xl,
+                                                             TileIO T) {
+  __shared__ float4 sa[kStageMax + 1], sb[kStageMax + 1];
+  const int tile = blockIdx.x;
+  const int staged = stage_tile<true>(T, tile, pst, sa, vel, sb);
+  if (staged >= 0)
+    vorticity_tile<4, true>(tile, F, n, stride, nbr, cnt, pst, vel, scr, xl, Src{T.nbr16, sa, sb, staged});
+  else
+    vorticity_tile<4>(tile, F, n, stride, nbr, cnt, pst, vel, scr, xl);
+}
+
+template <int GL, bool STAGED = false>
+__device__ __forceinline__ void apply_vorticity_tile(int tile, const Fast& F, int n, size_t stride,
+                                                     const int32_t* __restrict__ nbr,
+                                                     const int32_t* __restrict__ cnt,
+                                                     const float4* __restrict__ xl, const float4* __restrict__ scr,
+                                                     float4* vel, Src src = Src{nullptr, nullptr, nullptr, 0}) {
+  const pbf::Group G = pbf::group_at<GL>(n, tile);
   const int b = G.b;
   const float4 xp = xl[b];
   const int c = G.live ? cnt[b] : 0;
   float ex = 0.f, ey = 0.f, ez = 0.f;
-  pbf::gwalk1<GL>(nbr + (size_t)b * stride, c, n, G.lane, xl, [&](int, float4 xq) {
+  pbf::walk1<GL, STAGED>(nbr + (size_t)b * stride, STAGED ? src.nbr16 + (size_t)b * stride : nullptr, c,
+                         STAGED ? src.dummy : n, G.lane, STAGED ? src.a : xl, [&](int, float4 xq) {
     const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
     const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
     const float t = xq.w * pbf::spikey_over_r(F, d2);
@@ -1298,6 +1537,30 @@ __global__ void __launch_bounds__(kBlock) kf_apply_vorticity(Dev P, Fast F, int 
   v.y = fmaf(fmaf(Nz, wp.x, -Nx * wp.z), F.vort_dt, v.y);
   v.z = fmaf(fmaf(Nx, wp.y, -Ny * wp.x), F.vort_dt, v.z);
   vel[b] = v;
+}
+
+template <int GL>
+__global__ void __launch_bounds__(kBlock) kf_apply_vorticity(Dev P, Fast F, int n, size_t stride,
+                                                             const int32_t* __restrict__ nbr,
+                                                             const int32_t* __restrict__ cnt,
+                                                             const float4* __restrict__ xl,
+                                                             const float4* __restrict__ scr, float4* vel) {
+  apply_vorticity_tile<GL>(blockIdx.x, F, n, stride, nbr, cnt, xl, scr, vel);
+}
+
+__global__ void __launch_bounds__(kStageThreads) ks_apply_vorticity(Dev P, Fast F, int n, size_t stride,
+                                                                   const int32_t* __restrict__ nbr,
+                                                                   const int32_t* __restrict__ cnt,
+                                                                   const float4* __restrict__ xl,
+                                                                   const float4* __restrict__ scr, float4* vel,
+                                                                   TileIO T) {
+  __shared__ float4 stage[kStageMax + 1];
+  const int tile = blockIdx.x;
+  const int staged = stage_tile<false>(T, tile, xl, stage, nullptr, nullptr);
+  if (staged >= 0)
+    apply_vorticity_tile<4, true>(tile, F, n, stride, nbr, cnt, xl, scr, vel, Src{T.nbr16, stage, nullptr, staged});
+  else
+    apply_vorticity_tile<4>(tile, F, n, stride, nbr, cnt, xl, scr, vel);
 }
 
 // Residual statistics (no state change): density over the current lists,
@@ -1409,9 +1672,13 @@ struct pbf_ctx {
   uint64_t steps_done = 0;  // steps advanced by pbf_step (saved with the state)
   // launch shapes of the fast gather families, and the persistent grids of
   // the learned solver's skippable launches (SMs x resident blocks)
-  pbf_tuning tune{{8, 8, 8, 8, 8}, {kBlock, kBlock, kBlock, kBlock, kBlock}};
+  pbf_tuning tune{{8, 8, 8, 8, 8}, {kBlock, kBlock, kBlock, kBlock, kBlock}, {0, 0, 0, 0, 0}};
   int sms = 148;
   int pgrid_check = 148, pgrid_dp = 148;
+  // staged gathers: tile descriptors and the 16-bit lists the list fill writes
+  int32_t *tile_nruns = nullptr, *tile_total = nullptr;
+  int4* tile_runs = nullptr;
+  uint16_t* nbr16 = nullptr;
   int partials_cap = 0;
 
   // batch of scenes (empty: one scene, the parameter block's box); the device
@@ -1655,9 +1922,23 @@ void with_lanes(int lanes, Fn&& fn) {
     fn(std::integral_constant<int, 8>{});
 }
 
-bool shape_ok(int lanes, int block) { return (lanes == 4 || lanes == 8) && (block == 128 || block == 256); }
+bool shape_ok(int lanes, int block, int staged) {
+  if (staged) return staged == 1 && lanes == 4 && block == kStageThreads;
+  return (lanes == 4 || lanes == 8) && (block == 128 || block == 256);
+}
+
+bool any_staged(const pbf_ctx* ctx) {
+  if (ctx->params.exact_math) return false;
+  for (int f = 0; f < PBF_TUNE_FAMILIES; ++f)
+    if (ctx->tune.staged[f]) return true;
+  return false;
+}
+
+TileIO tile_io(const pbf_ctx* ctx) { return TileIO{ctx->tile_nruns, ctx->tile_total, ctx->tile_runs, ctx->nbr16}; }
+
 
 int grid_of(const pbf_ctx* ctx, int family) {
+  if (ctx->tune.staged[family]) return (int)((ctx->n + kTile - 1) / kTile);
   return blocks_for(ctx->n * (size_t)ctx->tune.lanes[family], ctx->tune.block[family]);
 }
 
@@ -1671,14 +1952,20 @@ int update_shapes(pbf_ctx* ctx) {
     return std::min(ctx->sms * per_sm, ctx->partials_cap);
   };
   const pbf_tuning& t = ctx->tune;
-  with_lanes(t.lanes[PBF_TUNE_DENSITY], [&](auto gl) {
-    ctx->pgrid_check = resident((const void*)kf_density_lambda<kDlCheck, decltype(gl)::value>,
-                                t.block[PBF_TUNE_DENSITY]);
-  });
-  with_lanes(t.lanes[PBF_TUNE_DELTA_P], [&](auto gl) {
-    ctx->pgrid_dp = resident((const void*)kf_dp_update<false, false, true, decltype(gl)::value>,
-                             t.block[PBF_TUNE_DELTA_P]);
-  });
+  if (t.staged[PBF_TUNE_DENSITY])
+    ctx->pgrid_check = resident((const void*)ks_density_lambda<kDlCheck>, kStageThreads);
+  else
+    with_lanes(t.lanes[PBF_TUNE_DENSITY], [&](auto gl) {
+      ctx->pgrid_check = resident((const void*)kf_density_lambda<kDlCheck, decltype(gl)::value>,
+                                  t.block[PBF_TUNE_DENSITY]);
+    });
+  if (t.staged[PBF_TUNE_DELTA_P])
+    ctx->pgrid_dp = resident((const void*)ks_dp_update<false, false, true>, kStageThreads);
+  else
+    with_lanes(t.lanes[PBF_TUNE_DELTA_P], [&](auto gl) {
+      ctx->pgrid_dp = resident((const void*)kf_dp_update<false, false, true, decltype(gl)::value>,
+                               t.block[PBF_TUNE_DELTA_P]);
+    });
   cudaGetLastError();  // occupancy queries leave no error behind
   return PBF_OK;
 }
@@ -1782,8 +2069,12 @@ void launch_sort_to_pairs(pbf_ctx* ctx) {
 
 void launch_fill(pbf_ctx* ctx, const float4* pst) {
   Launch L(ctx, "fill_neighbors");
-  k_fill2<<<blocks_for(ctx->n, kFillBlock), kFillBlock, 0, ctx->stream>>>(ctx->dev, (int)ctx->n, ctx->lstride, pst,
-                                                                         ctx->cell_start, ctx->nbr, ctx->cnt, ctx->err);
+  if (any_staged(ctx))
+    k_fill2<true><<<blocks_for(ctx->n, kFillBlock), kFillBlock, 0, ctx->stream>>>(
+        ctx->dev, (int)ctx->n, ctx->lstride, pst, ctx->cell_start, ctx->nbr, ctx->cnt, ctx->err, tile_io(ctx));
+  else
+    k_fill2<false><<<blocks_for(ctx->n, kFillBlock), kFillBlock, 0, ctx->stream>>>(
+        ctx->dev, (int)ctx->n, ctx->lstride, pst, ctx->cell_start, ctx->nbr, ctx->cnt, ctx->err, tile_io(ctx));
 }
 
 // ---- the fused step (graph-capturable: fixed pointers, no host sync) ----
@@ -1835,28 +2126,47 @@ void launch_learned_solve(pbf_ctx* ctx) {
     const int warps = (n + 15) / 16;
     kl_mlp<<<(warps + 3) / 4, 128, 0, s>>>(M, n, ctx->featb, ctx->xl, ctx->lamH, ctx->lamsumH);
   }
-  with_lanes(T.lanes[PBF_TUNE_DELTA_P], [&](auto gl) {
+  const TileIO tio = tile_io(ctx);
+  if (T.staged[PBF_TUNE_DELTA_P]) {
     Launch L(ctx, "dp_update");
-    kf_dp_update<SCORR, false, false, decltype(gl)::value><<<grid_of(ctx, PBF_TUNE_DELTA_P), bp, 0, s>>>(
-        P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS, ctx->posS, ctx->velS, ctx->state, nullptr);
-  });
+    ks_dp_update<SCORR, false, false><<<grid_of(ctx, PBF_TUNE_DELTA_P), kStageThreads, 0, s>>>(
+        P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS, ctx->posS, ctx->velS, ctx->state, nullptr, tio);
+  } else {
+    with_lanes(T.lanes[PBF_TUNE_DELTA_P], [&](auto gl) {
+      Launch L(ctx, "dp_update");
+      kf_dp_update<SCORR, false, false, decltype(gl)::value><<<grid_of(ctx, PBF_TUNE_DELTA_P), bp, 0, s>>>(
+          P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS, ctx->posS, ctx->velS, ctx->state, nullptr);
+    });
+  }
   for (int r = 1; r <= iters; ++r) {
     const bool final_check = r == iters;
-    with_lanes(T.lanes[PBF_TUNE_DENSITY], [&](auto gl) {
+    if (T.staged[PBF_TUNE_DENSITY]) {
       Launch L(ctx, "residual_check");
-      kf_density_lambda<kDlCheck, decltype(gl)::value><<<gpc, bd, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS,
-                                                                         ctx->xl, ctx->velS, ctx->lamH, ctx->nudge, io);
-    });
+      ks_density_lambda<kDlCheck><<<gpc, kStageThreads, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl,
+                                                                ctx->velS, ctx->lamH, ctx->nudge, io, tio);
+    } else {
+      with_lanes(T.lanes[PBF_TUNE_DENSITY], [&](auto gl) {
+        Launch L(ctx, "residual_check");
+        kf_density_lambda<kDlCheck, decltype(gl)::value><<<gpc, bd, 0, s>>>(
+            P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl, ctx->velS, ctx->lamH, ctx->nudge, io);
+      });
+    }
     {
       Launch L(ctx, "decide");
       pbf::k_decide<<<1, pbf::kDecideThreads, 0, s>>>(n, tol, final_check ? 1 : 0, ctx->partials, gpc, ctx->state);
     }
     if (final_check) break;
-    with_lanes(T.lanes[PBF_TUNE_DELTA_P], [&](auto gl) {
+    if (T.staged[PBF_TUNE_DELTA_P]) {
       Launch L(ctx, "dp_update");
-      kf_dp_update<SCORR, false, true, decltype(gl)::value><<<gpd, bp, 0, s>>>(
-          P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS, ctx->posS, ctx->velS, ctx->state, ctx->lamsumH);
-    });
+      ks_dp_update<SCORR, false, true><<<gpd, kStageThreads, 0, s>>>(
+          P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS, ctx->posS, ctx->velS, ctx->state, ctx->lamsumH, tio);
+    } else {
+      with_lanes(T.lanes[PBF_TUNE_DELTA_P], [&](auto gl) {
+        Launch L(ctx, "dp_update");
+        kf_dp_update<SCORR, false, true, decltype(gl)::value><<<gpd, bp, 0, s>>>(
+            P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS, ctx->posS, ctx->velS, ctx->state, ctx->lamsumH);
+      });
+    }
   }
   Launch L(ctx, "update_velocities");
   k_update_v<<<g, kBlock, 0, s>>>(P, n, ctx->pstS, ctx->posS, ctx->velS);
@@ -1899,7 +2209,17 @@ void launch_step_t(pbf_ctx* ctx) {
       if (X)
         k_density_lambda<X><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl, ctx->velS,
                                                  ctx->lamH, ctx->nudge);
-      else
+      else if (T.staged[PBF_TUNE_DENSITY]) {
+        const int gd = grid_of(ctx, PBF_TUNE_DENSITY);
+        if (ctx->recording)
+          ks_density_lambda<kDlRecord><<<gd, kStageThreads, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS,
+                                                                    ctx->xl, ctx->velS, ctx->lamH, ctx->nudge, io,
+                                                                    tile_io(ctx));
+        else
+          ks_density_lambda<kDlPlain><<<gd, kStageThreads, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS,
+                                                                   ctx->xl, ctx->velS, ctx->lamH, ctx->nudge, io,
+                                                                   tile_io(ctx));
+      } else
         with_lanes(T.lanes[PBF_TUNE_DENSITY], [&](auto gl) {
           constexpr int GL = decltype(gl)::value;
           const int gd = grid_of(ctx, PBF_TUNE_DENSITY), bd = T.block[PBF_TUNE_DENSITY];
@@ -1925,6 +2245,16 @@ void launch_step_t(pbf_ctx* ctx) {
       else
         k_dp_update<X, SCORR, false><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS,
                                                           ctx->posS, ctx->velS, ctx->lamH, ctx->nudge);
+    } else if (T.staged[PBF_TUNE_DELTA_P]) {
+      const int gd = grid_of(ctx, PBF_TUNE_DELTA_P);
+      if (last)
+        ks_dp_update<SCORR, true, false><<<gd, kStageThreads, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl,
+                                                                      ctx->pstS, ctx->posS, ctx->velS, ctx->state,
+                                                                      nullptr, tile_io(ctx));
+      else
+        ks_dp_update<SCORR, false, false><<<gd, kStageThreads, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl,
+                                                                       ctx->pstS, ctx->posS, ctx->velS, ctx->state,
+                                                                       nullptr, tile_io(ctx));
     } else {
       with_lanes(T.lanes[PBF_TUNE_DELTA_P], [&](auto gl) {
         constexpr int GL = decltype(gl)::value;
@@ -1970,30 +2300,56 @@ void launch_step_t(pbf_ctx* ctx) {
     k_viscosity<X, true><<<g, kBlock, 0, s>>>(P, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->velT, ctx->velH,
                                               ctx->posH, ctx->pstH, ctx->origS, ctx->origH);
   } else {
+    const TileIO tio = tile_io(ctx);
     const int gv = grid_of(ctx, PBF_TUNE_VISCOSITY), bv = T.block[PBF_TUNE_VISCOSITY];
-    with_lanes(T.lanes[PBF_TUNE_VISCOSITY], [&](auto gl) {
+    if (T.staged[PBF_TUNE_VISCOSITY]) {
       Launch L(ctx, "viscosity");
-      kf_viscosity<false, decltype(gl)::value><<<gv, bv, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS,
-                                                                 ctx->velS, ctx->velT, nullptr, nullptr, nullptr,
-                                                                 nullptr);
-    });
-    with_lanes(T.lanes[PBF_TUNE_VORTICITY], [&](auto gl) {
+      ks_viscosity<false><<<gv, kStageThreads, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->velS,
+                                                       ctx->velT, nullptr, nullptr, nullptr, nullptr, tio);
+    } else {
+      with_lanes(T.lanes[PBF_TUNE_VISCOSITY], [&](auto gl) {
+        Launch L(ctx, "viscosity");
+        kf_viscosity<false, decltype(gl)::value><<<gv, bv, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS,
+                                                                   ctx->velS, ctx->velT, nullptr, nullptr, nullptr,
+                                                                   nullptr);
+      });
+    }
+    if (T.staged[PBF_TUNE_VORTICITY]) {
       Launch L(ctx, "vorticity");
-      kf_vorticity<decltype(gl)::value><<<grid_of(ctx, PBF_TUNE_VORTICITY), T.block[PBF_TUNE_VORTICITY], 0, s>>>(
-          P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->velT, ctx->scrH, ctx->xl);
-    });
-    with_lanes(T.lanes[PBF_TUNE_APPLY_VORTICITY], [&](auto gl) {
+      ks_vorticity<<<grid_of(ctx, PBF_TUNE_VORTICITY), kStageThreads, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt,
+                                                                               ctx->pstS, ctx->velT, ctx->scrH,
+                                                                               ctx->xl, tio);
+    } else {
+      with_lanes(T.lanes[PBF_TUNE_VORTICITY], [&](auto gl) {
+        Launch L(ctx, "vorticity");
+        kf_vorticity<decltype(gl)::value><<<grid_of(ctx, PBF_TUNE_VORTICITY), T.block[PBF_TUNE_VORTICITY], 0, s>>>(
+            P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->velT, ctx->scrH, ctx->xl);
+      });
+    }
+    if (T.staged[PBF_TUNE_APPLY_VORTICITY]) {
       Launch L(ctx, "apply_vorticity");
-      kf_apply_vorticity<decltype(gl)::value>
-          <<<grid_of(ctx, PBF_TUNE_APPLY_VORTICITY), T.block[PBF_TUNE_APPLY_VORTICITY], 0, s>>>(
-              P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->scrH, ctx->velT);
-    });
-    with_lanes(T.lanes[PBF_TUNE_VISCOSITY], [&](auto gl) {
+      ks_apply_vorticity<<<grid_of(ctx, PBF_TUNE_APPLY_VORTICITY), kStageThreads, 0, s>>>(
+          P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->scrH, ctx->velT, tio);
+    } else {
+      with_lanes(T.lanes[PBF_TUNE_APPLY_VORTICITY], [&](auto gl) {
+        Launch L(ctx, "apply_vorticity");
+        kf_apply_vorticity<decltype(gl)::value>
+            <<<grid_of(ctx, PBF_TUNE_APPLY_VORTICITY), T.block[PBF_TUNE_APPLY_VORTICITY], 0, s>>>(
+                P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->scrH, ctx->velT);
+      });
+    }
+    if (T.staged[PBF_TUNE_VISCOSITY]) {
       Launch L(ctx, "viscosity_final");
-      kf_viscosity<true, decltype(gl)::value><<<gv, bv, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->velT,
-                                                                ctx->velH, ctx->posH, ctx->pstH, ctx->origS,
-                                                                ctx->origH);
-    });
+      ks_viscosity<true><<<gv, kStageThreads, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->velT,
+                                                      ctx->velH, ctx->posH, ctx->pstH, ctx->origS, ctx->origH, tio);
+    } else {
+      with_lanes(T.lanes[PBF_TUNE_VISCOSITY], [&](auto gl) {
+        Launch L(ctx, "viscosity_final");
+        kf_viscosity<true, decltype(gl)::value><<<gv, bv, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS,
+                                                                  ctx->velT, ctx->velH, ctx->posH, ctx->pstH,
+                                                                  ctx->origS, ctx->origH);
+      });
+    }
   }
 }
 
@@ -2103,6 +2459,10 @@ static int create_ctx(const pbf_params* p, size_t capacity, const pbf_scene* sce
       (rc = dalloc(ctx, &ctx->maxerr, 1)) || (rc = dalloc(ctx, &ctx->hits, 1)) ||
       (rc = dalloc(ctx, &ctx->lamsumH, C)) || (rc = dalloc(ctx, &ctx->lamprevS, C)) ||
       (rc = dalloc(ctx, &ctx->featb, C * pbf::kMlpInPad)) ||
+      (rc = dalloc(ctx, &ctx->tile_nruns, (C + kTile - 1) / kTile)) ||
+      (rc = dalloc(ctx, &ctx->tile_total, (C + kTile - 1) / kTile)) ||
+      (rc = dalloc(ctx, &ctx->tile_runs, (C + kTile - 1) / kTile * kTileRuns)) ||
+      (rc = dalloc(ctx, &ctx->nbr16, C * cap)) ||
       (rc = dalloc(ctx, &ctx->state, 1)) || (rc = dalloc(ctx, &ctx->partials, (size_t)ctx->partials_cap)) ||
       (rc = dalloc(ctx, &ctx->mlp_params, pbf::kMlpParams)) ||
       (rc = dalloc(ctx, &ctx->mlp_grad, pbf::kMlpParams)) || (rc = dalloc(ctx, &ctx->mlp_m, pbf::kMlpParams)) ||
@@ -2324,7 +2684,9 @@ struct StateHeader {
   uint32_t flags;  // bit 0: the learned warm start's network follows the arrays
   uint32_t reserved;
   pbf_tuning tuning;
+  uint32_t reserved2;  // the header is 104 bytes, a multiple of 8
 };
+static_assert(sizeof(StateHeader) == 104, "state file header layout");
 struct FileCloser {
   FILE* f;
   ~FileCloser() {
@@ -2725,6 +3087,13 @@ static int stats_range(pbf_ctx* ctx, size_t b0, size_t b1, bool clear_flags, pbf
     out->solver_iterations = (uint32_t)ctx->params.solve_steps;
     out->solver_residual = -1.0;
   }
+  if (any_staged(ctx) && ctx->n) {  // the tiles of the last list fill
+    const size_t tiles = (ctx->n + kTile - 1) / kTile;
+    std::vector<int32_t> nr(tiles);
+    CK(cudaMemcpy(nr.data(), ctx->tile_nruns, tiles * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    out->tiles = (uint32_t)tiles;
+    for (int32_t v : nr) out->tiles_staged += v > 0 ? 1u : 0u;
+  }
   return PBF_OK;
 }
 
@@ -2935,17 +3304,19 @@ int pbf_get_tuning(const pbf_ctx* ctx, pbf_tuning* out) {
 int pbf_set_tuning(pbf_ctx* ctx, const pbf_tuning* t) {
   if (!ctx || !t) return PBF_ERR_ARG;
   for (int f = 0; f < PBF_TUNE_FAMILIES; ++f)
-    if (!shape_ok(t->lanes[f], t->block[f]))
-      return fail(ctx, PBF_ERR_ARG, "gather family %d: %d lanes x %d threads is not a supported shape "
-                  "(lanes 4 or 8, block 128 or 256)", f, t->lanes[f], t->block[f]);
+    if (!shape_ok(t->lanes[f], t->block[f], t->staged[f]))
+      return fail(ctx, PBF_ERR_ARG, "gather family %d: %d lanes x %d threads%s is not a supported shape "
+                  "(lanes 4 or 8, block 128 or 256; staged: 4 x 128)", f, t->lanes[f], t->block[f],
+                  t->staged[f] ? " staged" : "");
   ctx->tune = *t;
   drop_graphs(ctx);
   return update_shapes(ctx);
 }
 
 namespace {
-constexpr int kCandLanes[PBF_TUNE_CANDIDATES] = {4, 4, 8, 8};
-constexpr int kCandBlock[PBF_TUNE_CANDIDATES] = {128, 256, 128, 256};
+constexpr int kCandLanes[PBF_TUNE_CANDIDATES] = {4, 4, 8, 8, 4};
+constexpr int kCandBlock[PBF_TUNE_CANDIDATES] = {128, 256, 128, 256, kStageThreads};
+constexpr int kCandStaged[PBF_TUNE_CANDIDATES] = {0, 0, 0, 0, 1};
 
 int family_of(const char* name) {
   if (!std::strcmp(name, "density_lambda") || !std::strcmp(name, "residual_check")) return PBF_TUNE_DENSITY;
@@ -3001,6 +3372,7 @@ int pbf_autotune(pbf_ctx* ctx, int steps, pbf_tuning* chosen, double* ms) {
   const bool timing = ctx->timing;
   const pbf_tuning before = ctx->tune;
   double t[PBF_TUNE_CANDIDATES][PBF_TUNE_FAMILIES] = {};
+  double fill_ms[PBF_TUNE_CANDIDATES] = {};
   ctx->timing = true;
   auto finish = [&](int code) {
     ctx->timing = timing;
@@ -3015,6 +3387,7 @@ int pbf_autotune(pbf_ctx* ctx, int steps, pbf_tuning* chosen, double* ms) {
     for (int f = 0; f < PBF_TUNE_FAMILIES; ++f) {
       ctx->tune.lanes[f] = kCandLanes[c];
       ctx->tune.block[f] = kCandBlock[c];
+      ctx->tune.staged[f] = kCandStaged[c];
     }
     if ((rc = update_shapes(ctx)) || (rc = snap.restore(ctx))) return finish(rc);
     launch_step(ctx);  // untimed: first touch of this shape
@@ -3026,16 +3399,41 @@ int pbf_autotune(pbf_ctx* ctx, int steps, pbf_tuning* chosen, double* ms) {
     for (const auto& kv : ctx->times) {
       const int f = family_of(kv.first.c_str());
       if (f >= 0) t[c][f] += kv.second.second / steps;
+      if (kv.first == "fill_neighbors") fill_ms[c] = kv.second.second / steps;
     }
   }
+  // The fastest direct shape per family; then staging, for the families it
+  // speeds up, only when those savings exceed what staging adds to the list
+  // fill (the 16-bit lists and tile descriptors it then writes).
   pbf_tuning best = before;
+  int pick[PBF_TUNE_FAMILIES];
+  double direct_fill = 0.0;
+  int ndirect = 0;
+  for (int c = 0; c < PBF_TUNE_CANDIDATES; ++c)
+    if (!kCandStaged[c]) {
+      direct_fill += fill_ms[c];
+      ++ndirect;
+    }
+  direct_fill /= ndirect > 0 ? ndirect : 1;
+  double saved = 0.0;
+  int staged_c = -1;
+  for (int c = 0; c < PBF_TUNE_CANDIDATES; ++c)
+    if (kCandStaged[c]) staged_c = c;
   for (int f = 0; f < PBF_TUNE_FAMILIES; ++f) {
-    int bc = 0;
-    for (int c = 1; c < PBF_TUNE_CANDIDATES; ++c)
-      if (t[c][f] < t[bc][f]) bc = c;
+    int bc = -1;
+    for (int c = 0; c < PBF_TUNE_CANDIDATES; ++c)
+      if (!kCandStaged[c] && (bc < 0 || t[c][f] < t[bc][f])) bc = c;
+    pick[f] = bc;
+    if (staged_c >= 0 && t[staged_c][f] > 0.0 && t[staged_c][f] < t[bc][f]) saved += t[bc][f] - t[staged_c][f];
+  }
+  const bool use_staged = staged_c >= 0 && saved > fill_ms[staged_c] - direct_fill;
+  for (int f = 0; f < PBF_TUNE_FAMILIES; ++f) {
+    int bc = pick[f];
+    if (use_staged && t[staged_c][f] > 0.0 && t[staged_c][f] < t[bc][f]) bc = staged_c;
     if (t[bc][f] > 0.0) {  // a family the step never launches keeps its shape
       best.lanes[f] = kCandLanes[bc];
       best.block[f] = kCandBlock[bc];
+      best.staged[f] = kCandStaged[bc];
     }
   }
   if (ms)

@@ -170,6 +170,90 @@ __device__ __forceinline__ void gwalk2(const int32_t* __restrict__ row, int c, i
   }
 }
 
+// ---- staged walks: the tile's neighbour records in shared memory ----
+// The list fill writes, beside each int32 list, a 16-bit list of indices into
+// the tile's staging area (the neighbour bins of a 32-particle tile, copied to
+// shared memory by the gather kernel; index `dummy` = the zero-contribution
+// record past the staged ones).  Lane l of the group takes entries 8l..8l+7 of
+// every 8*GL-entry batch (one 16-byte load), in two halves of four records.
+__device__ __forceinline__ uint32_t lo16(uint32_t w) { return w & 0xffffu; }
+__device__ __forceinline__ uint32_t hi16(uint32_t w) { return w >> 16; }
+
+template <class Body>
+__device__ __forceinline__ void stage_quad(const float4* stage, uint32_t w0, uint32_t w1, Body&& body) {
+  const int i0 = (int)lo16(w0), i1 = (int)hi16(w0), i2 = (int)lo16(w1), i3 = (int)hi16(w1);
+  const float4 v0 = stage[i0], v1 = stage[i1], v2 = stage[i2], v3 = stage[i3];
+  body(i0, v0);
+  body(i1, v1);
+  body(i2, v2);
+  body(i3, v3);
+}
+
+// Entries e and e+1 (the two halves of `word`): those at or past c name the dummy.
+__device__ __forceinline__ uint32_t stage_fix(uint32_t word, int e, int c, uint32_t dummy) {
+  const uint32_t lo = e < c ? lo16(word) : dummy;
+  const uint32_t hi = e + 1 < c ? hi16(word) : dummy;
+  return lo | (hi << 16);
+}
+
+// Entries e..e+7 of a 16-byte load (little-endian: w.x holds e, e+1).
+__device__ __forceinline__ uint4 stage_tail(uint4 w, int e, int c, uint32_t dummy) {
+  return make_uint4(stage_fix(w.x, e, c, dummy), stage_fix(w.y, e + 2, c, dummy), stage_fix(w.z, e + 4, c, dummy),
+                    stage_fix(w.w, e + 6, c, dummy));
+}
+
+template <int GL = kGL, class Body>
+__device__ __forceinline__ void swalk1(const uint16_t* __restrict__ row16, int c, int dummy, int lane,
+                                       const float4* stage, Body&& body) {
+  const uint4* r4 = reinterpret_cast<const uint4*>(row16);
+  const int batches = (c + 8 * GL - 1) / (8 * GL);
+  for (int t = 0; t < batches; ++t) {
+    uint4 w = __ldg(r4 + t * GL + lane);
+    if (t == batches - 1) w = stage_tail(w, t * 8 * GL + 8 * lane, c, (uint32_t)dummy);
+    stage_quad(stage, w.x, w.y, body);
+    stage_quad(stage, w.z, w.w, body);
+  }
+}
+
+// Two staged records per neighbour (a, b staged at the same index).
+template <int GL = kGL, class Body>
+__device__ __forceinline__ void swalk2(const uint16_t* __restrict__ row16, int c, int dummy, int lane,
+                                       const float4* sa, const float4* sb, Body&& body) {
+  const uint4* r4 = reinterpret_cast<const uint4*>(row16);
+  const int batches = (c + 8 * GL - 1) / (8 * GL);
+  for (int t = 0; t < batches; ++t) {
+    uint4 w = __ldg(r4 + t * GL + lane);
+    if (t == batches - 1) w = stage_tail(w, t * 8 * GL + 8 * lane, c, (uint32_t)dummy);
+    const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int i0 = (int)lo16(ws[k]), i1 = (int)hi16(ws[k]);
+      const float4 a0 = sa[i0], b0 = sb[i0], a1 = sa[i1], b1 = sb[i1];
+      body(i0, a0, b0);
+      body(i1, a1, b1);
+    }
+  }
+}
+
+// One walk for both sources: staged (shared memory, 16-bit list) or direct.
+template <int GL, bool STAGED, class Body>
+__device__ __forceinline__ void walk1(const int32_t* row, const uint16_t* row16, int c, int dummy, int lane,
+                                      const float4* src, Body&& body) {
+  if (STAGED)
+    swalk1<GL>(row16, c, dummy, lane, src, body);
+  else
+    gwalk1<GL>(row, c, dummy, lane, src, body);
+}
+
+template <int GL, bool STAGED, class Body>
+__device__ __forceinline__ void walk2(const int32_t* row, const uint16_t* row16, int c, int dummy, int lane,
+                                      const float4* sa, const float4* sb, Body&& body) {
+  if (STAGED)
+    swalk2<GL>(row16, c, dummy, lane, sa, sb, body);
+  else
+    gwalk2<GL>(row, c, dummy, lane, sa, sb, body);
+}
+
 // (h - r)^2 / r for r < h, else 0 (the Del_Spikey magnitude over r, no norm).
 __device__ __forceinline__ float spikey_over_r(const Fast& F, float d2) {
   const float rinv = rsqrtf(fmaxf(d2, 1e-30f));

@@ -345,17 +345,18 @@ class Particles:
         return t.as_dict()
 
     def set_tuning(self, shapes: dict) -> None:
+        """{family: (lanes, block) or (lanes, block, staged)}; unnamed families keep theirs."""
         t = _abi.PbfTuning()
         cur = self.tuning()
-        cur.update(shapes)
+        cur.update({f: tuple(v) + (0,) * (3 - len(v)) for f, v in shapes.items()})
         for i, f in enumerate(_abi.TUNE_FAMILIES):
-            t.lanes[i], t.block[i] = cur[f]
+            t.lanes[i], t.block[i], t.staged[i] = cur[f]
         self._check(self._lib.pbf_set_tuning(self._ctx, C.byref(t)), "set_tuning")
 
     def autotune(self, steps: int = 3) -> tuple[dict, dict]:
         """Time every candidate shape on `steps` steps of the current state
         (restored afterwards), apply the fastest per family; returns (chosen,
-        {(lanes, block): {family: ms per step}})."""
+        {(lanes, block, staged): {family: ms per step}})."""
         t = _abi.PbfTuning()
         nc, nf = len(_abi.TUNE_CANDIDATES), len(_abi.TUNE_FAMILIES)
         ms = (C.c_double * (nc * nf))()

@@ -32,7 +32,8 @@ MLP_PARAMS = 5057
 MLP_NORM = 25
 
 TUNE_FAMILIES = ("density", "delta_p", "viscosity", "vorticity", "apply_vorticity")
-TUNE_CANDIDATES = ((4, 128), (4, 256), (8, 128), (8, 256))  # (lanes per particle, threads per block)
+# (lanes per particle, threads per block, staged in shared memory)
+TUNE_CANDIDATES = ((4, 128, 0), (4, 256, 0), (8, 128, 0), (8, 256, 0), (4, 128, 1))
 
 NOALLOC_MAX_PARTICLES = 65536
 NOALLOC_MAX_BINS = 262144
@@ -89,6 +90,8 @@ class PbfStats(C.Structure):
         ("error_flags", C.c_uint32),
         ("solver_iterations", C.c_uint32),
         ("solver_residual", C.c_double),
+        ("tiles", C.c_uint32),
+        ("tiles_staged", C.c_uint32),
     ]
 
     def as_dict(self) -> dict:
@@ -103,6 +106,8 @@ class PbfStats(C.Structure):
             "error_flags": int(self.error_flags),
             "solver_iterations": int(self.solver_iterations),
             "solver_residual": self.solver_residual,
+            "tiles": int(self.tiles),
+            "tiles_staged": int(self.tiles_staged),
         }
 
 
@@ -111,10 +116,10 @@ class PbfScene(C.Structure):
 
 
 class PbfTuning(C.Structure):
-    _fields_ = [("lanes", C.c_int * 5), ("block", C.c_int * 5)]
+    _fields_ = [("lanes", C.c_int * 5), ("block", C.c_int * 5), ("staged", C.c_int * 5)]
 
     def as_dict(self) -> dict:
-        return {f: (int(self.lanes[i]), int(self.block[i])) for i, f in enumerate(TUNE_FAMILIES)}
+        return {f: (int(self.lanes[i]), int(self.block[i]), int(self.staged[i])) for i, f in enumerate(TUNE_FAMILIES)}
 
 
 _P = C.POINTER

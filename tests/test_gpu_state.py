@@ -92,7 +92,7 @@ def test_state_file_errors(tmp_path):
     assert raw[:8] == b"PBFSTATE"
     version, pbytes, n, steps = np.frombuffer(raw[8:32], dtype="<u4,<u4,<u8,<u8")[0]
     assert version == 1 and pbytes == C_PARAMS_BYTES and n == sc.n and steps == 0
-    x = np.frombuffer(raw, "<f4", count=3 * sc.n, offset=80 + pbytes).reshape(-1, 3)
+    x = np.frombuffer(raw, "<f4", count=3 * sc.n, offset=104 + pbytes).reshape(-1, 3)
     assert np.array_equal(x, a.positions())
 
 

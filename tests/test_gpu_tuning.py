@@ -25,7 +25,7 @@ BARS = {"mean_density_error": 0.014, "max_density_error": 0.044, "kinetic_energy
 
 
 def _all_families(shape):
-    return {f: shape for f in _abi.TUNE_FAMILIES}
+    return {f: tuple(shape) + (0,) * (3 - len(shape)) for f in _abi.TUNE_FAMILIES}
 
 
 @pytest.mark.parametrize("shape", _abi.TUNE_CANDIDATES)
@@ -58,13 +58,13 @@ def test_shapes_agree_on_100_step_statistics():
     sc = make_scene("dam_65k")
     x = sc.positions()
     out = {}
-    for shape in ((4, 128), (8, 256)):
+    for shape in ((4, 128, 1), (8, 256, 0)):
         g = Particles(sc.params(), sc.n)
         g.set_tuning(_all_families(shape))
         g.upload(x)
         out[shape] = _averaged(g)
         assert g.stats()["error_flags"] == 0
-    a, b = out[(4, 128)], out[(8, 256)]
+    a, b = out[(4, 128, 1)], out[(8, 256, 0)]
     for k in BARS:
         assert a[k] == pytest.approx(b[k], rel=BARS[k]), (k, a[k], b[k])
 
@@ -75,7 +75,9 @@ def test_set_tuning_rejects_unsupported_shapes():
     for bad in ((16, 256), (8, 512), (3, 128), (8, 96)):
         with pytest.raises(RuntimeError, match="not a supported shape"):
             g.set_tuning({"viscosity": bad})
-    assert g.tuning() == _all_families((8, 256))  # unchanged
+    assert g.tuning() == _all_families((8, 256, 0))  # unchanged
+    with pytest.raises(RuntimeError, match="not a supported shape"):
+        g.set_tuning({"density": (8, 256, 1)})  # staged is 4 lanes x 128 threads only
 
 
 def test_autotune_restores_state_and_applies_its_choice():
@@ -94,8 +96,13 @@ def test_autotune_restores_state_and_applies_its_choice():
     for cand, per_family in table.items():
         for f, ms in per_family.items():
             assert ms > 0.0, (cand, f)
-    for f, shape in chosen.items():  # the choice is the fastest candidate of each family
-        assert table[shape][f] == min(table[c][f] for c in table)
+    direct = [c for c in table if not c[2]]
+    for f, shape in chosen.items():  # the fastest direct shape, or staging where it is faster still
+        best_direct = min(table[c][f] for c in direct)
+        if shape[2]:
+            assert table[shape][f] < best_direct
+        else:
+            assert table[shape][f] == best_direct
     # the next step is the step a fresh context with the chosen shapes takes
     # from the same state (the slot order after the sort depends only on the
     # bins and the original indices)
@@ -123,5 +130,26 @@ def test_autotune_learned_solver_and_exact_math():
     ex.upload(make_scene("dam_2k").positions())
     ex.step(1)
     chosen, table = ex.autotune(1)
-    assert chosen == _all_families((8, 256))
+    assert chosen == _all_families((8, 256, 0))
     assert all(ms == 0.0 for c in table for ms in table[c].values())
+
+
+def test_staged_gathers_stage_most_tiles_and_match_direct():
+    """The staged shape reads most tiles from shared memory (the rest walk the
+    int32 lists) and agrees with the direct shape after a few fast steps."""
+    sc = make_scene("dam_65k")
+    x = sc.positions()
+    res = {}
+    for staged in (1, 0):
+        g = Particles(sc.params(), sc.n)
+        g.set_tuning(_all_families((4, 128, staged)))
+        g.upload(x)
+        g.step(5)
+        st = g.stats()
+        res[staged] = (g.positions(), g.velocities(), st)
+    st = res[1][2]
+    assert st["tiles"] == (sc.n + 31) // 32 and st["tiles_staged"] > 0.8 * st["tiles"], st
+    assert res[0][2]["tiles"] == 0
+    scale = max(sc.box_max)
+    np.testing.assert_allclose(res[1][0], res[0][0], rtol=0, atol=1e-4 * scale)
+    np.testing.assert_allclose(res[1][1], res[0][1], rtol=0, atol=1e-3)
