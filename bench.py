@@ -137,7 +137,6 @@ def kernel_bytes(name: str, n: int, nbar: float, K: int, nbins: int) -> float:
         "warm_features": 16 + L + 16 + 16 + 4 + 16 + 32,       # x*, list, v, last lambda in; (x*, l1), v, bf16 features out
         "warm_mlp": 32 + 16 + 16 + 4 + 4,                       # features, (x*, l1) in; (x*, lambda), lambda, sum out
         "residual_check": 16 + L + 16 + 4 + 4,                  # as density_lambda
-        "decide": 0.0,
         "reorder": 8 + 4 + 3 * 16 + 3 * 16 + 4 + 4,             # pair, key, (x, x*, v) in and out, orig, key
         "fill_neighbors": 16 + 4 * nbar + 4 + 8.0 * nbins / n,  # own x*, list + count out, bin starts
         "density_lambda": 16 + L + 16 + 4 + 4,                  # x* in; list; (x*, lambda), rho, lambda out

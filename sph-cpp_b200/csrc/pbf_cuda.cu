@@ -766,6 +766,8 @@ struct LearnIO {
   pbf::SolveState* state; // kDlCheck
   double* partials;       // kDlCheck: one sum per block of the (persistent) grid
   int first;              // first Jacobi iteration of the step
+  float tol;              // kDlCheck: residual tolerance
+  int final_check;        // kDlCheck: the step's last allowed check (records, never extends)
 };
 
 // The sums a density + lambda gather produces for one particle, combined
@@ -868,7 +870,10 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) kf_density_lambda(De
   float err = 0.0f;
   for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x)
     density_lambda_tile<MODE, GL>(tile, P, F, n, stride, nbr, cnt, pst, xl, vel, lam, nudge, io, err);
-  if (MODE == kDlCheck) pbf::block_partial<kBlock>(err, io.partials + blockIdx.x);
+  if (MODE == kDlCheck) {
+    pbf::block_partial<kBlock>(err, io.partials + blockIdx.x);
+    pbf::decide_if_last<kBlock>(io.state, io.partials, n, io.tol, io.final_check);
+  }
 }
 
 // ---- staged gathers: one 32-particle tile per block of kStageThreads ----
@@ -927,7 +932,10 @@ __global__ void __launch_bounds__(kStageThreads) ks_density_lambda(Dev P, Fast F
       density_lambda_tile<MODE, 4>(tile, P, F, n, stride, nbr, cnt, pst, xl, vel, lam, nudge, io, err);
     __syncthreads();  // the next tile's staging overwrites the area
   }
-  if (MODE == kDlCheck) pbf::block_partial<kStageThreads>(err, io.partials + blockIdx.x);
+  if (MODE == kDlCheck) {
+    pbf::block_partial<kStageThreads>(err, io.partials + blockIdx.x);
+    pbf::decide_if_last<kStageThreads>(io.state, io.partials, n, io.tol, io.final_check);
+  }
 }
 
 // Learned warm start, first Jacobi iteration, in two launches:
@@ -944,16 +952,18 @@ __global__ void __launch_bounds__(kStageThreads) ks_density_lambda(Dev P, Fast F
 // so the residual-checked plain iterations that follow are part of the method.
 constexpr float kWarmMaxGain = 3.0f;
 
-__global__ void __launch_bounds__(kBlock) kl_features(Dev P, Fast F, pbf::MlpDev M, int n, size_t stride,
+template <int GL>
+__global__ void __launch_bounds__(kBlock, kGatherMinBlocks) kl_features(Dev P, Fast F, pbf::MlpDev M, int n,
+                                                                        size_t stride,
                                                       const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
                                                       const float4* __restrict__ pst, float4* xl, float4* vel,
                                                       float* lam, uint32_t* nudge, const float* __restrict__ lamprev,
                                                       __nv_bfloat16* featb) {
-  const pbf::Group G = pbf::group_of(n);
+  const pbf::Group G = pbf::group_of<GL>(n);
   const int b = G.b;
   const float4 xp = pst[b];
   const int c = G.live ? cnt[b] : 0;
-  const DensitySums S = density_sums<pbf::kGL, true>(F, G, nbr + (size_t)b * stride, nullptr, c, n, pst, xp);
+  const DensitySums S = density_sums<GL, true>(F, G, nbr + (size_t)b * stride, nullptr, c, n, pst, xp);
   if (!G.live || G.lane != 0) return;
   const float rho = fmaf(F.m_poly, S.sw, F.m_w0);
   const float L2 = F.lam_grad * F.lam_grad;
@@ -2106,7 +2116,7 @@ void launch_learned_solve(pbf_ctx* ctx) {
   const Fast& F = ctx->fast;
   cudaStream_t s = ctx->stream;
   const pbf_tuning& T = ctx->tune;
-  const int g = blocks_for(n), gg = blocks_for((size_t)n * pbf::kGL);
+  const int g = blocks_for(n);
   // skippable launches: persistent grids
   const int gpc = std::min(grid_of(ctx, PBF_TUNE_DENSITY), ctx->pgrid_check);
   const int gpd = std::min(grid_of(ctx, PBF_TUNE_DELTA_P), ctx->pgrid_dp);
@@ -2114,12 +2124,18 @@ void launch_learned_solve(pbf_ctx* ctx) {
   const float tol = ctx->params.residual_tol;
   const int iters = ctx->params.max_iterations > 0 ? ctx->params.max_iterations : 1;
   cudaMemsetAsync(ctx->state, 0, sizeof(pbf::SolveState), s);
-  LearnIO io{nullptr, nullptr, nullptr, ctx->state, ctx->partials, 0};
+  LearnIO io{nullptr, nullptr, nullptr, ctx->state, ctx->partials, 0, tol, 0};
   const pbf::MlpDev M = mlp_dev(ctx);
   {
-    Launch L(ctx, "warm_features");
-    kl_features<<<gg, kBlock, 0, s>>>(P, F, M, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl, ctx->velS, ctx->lamH,
-                                      ctx->nudge, ctx->lamprevS, ctx->featb);
+    // the density family's shape (4 lanes x 128 threads when that family is staged)
+    const int fl = T.staged[PBF_TUNE_DENSITY] ? 4 : T.lanes[PBF_TUNE_DENSITY];
+    const int fb = T.staged[PBF_TUNE_DENSITY] ? kStageThreads : T.block[PBF_TUNE_DENSITY];
+    with_lanes(fl, [&](auto gl) {
+      Launch L(ctx, "warm_features");
+      kl_features<decltype(gl)::value><<<blocks_for((size_t)n * fl, fb), fb, 0, s>>>(
+          P, F, M, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl, ctx->velS, ctx->lamH, ctx->nudge, ctx->lamprevS,
+          ctx->featb);
+    });
   }
   {
     Launch L(ctx, "warm_mlp");
@@ -2140,6 +2156,7 @@ void launch_learned_solve(pbf_ctx* ctx) {
   }
   for (int r = 1; r <= iters; ++r) {
     const bool final_check = r == iters;
+    io.final_check = final_check ? 1 : 0;
     if (T.staged[PBF_TUNE_DENSITY]) {
       Launch L(ctx, "residual_check");
       ks_density_lambda<kDlCheck><<<gpc, kStageThreads, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl,
@@ -2150,10 +2167,6 @@ void launch_learned_solve(pbf_ctx* ctx) {
         kf_density_lambda<kDlCheck, decltype(gl)::value><<<gpc, bd, 0, s>>>(
             P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl, ctx->velS, ctx->lamH, ctx->nudge, io);
       });
-    }
-    {
-      Launch L(ctx, "decide");
-      pbf::k_decide<<<1, pbf::kDecideThreads, 0, s>>>(n, tol, final_check ? 1 : 0, ctx->partials, gpc, ctx->state);
     }
     if (final_check) break;
     if (T.staged[PBF_TUNE_DELTA_P]) {
@@ -2200,7 +2213,7 @@ void launch_step_t(pbf_ctx* ctx) {
   if (!X && ctx->params.solver == 1) {
     launch_learned_solve<SCORR>(ctx);
   } else {
-  LearnIO io{ctx->feats, ctx->lamsumH, ctx->lamprevS, ctx->state, nullptr, 0};
+  LearnIO io{ctx->feats, ctx->lamsumH, ctx->lamprevS, ctx->state, nullptr, 0, 0.0f, 0};
   for (int it = 0; it < K; ++it) {
     io.first = it == 0;
     if (X) cudaMemsetAsync(ctx->nudge, 0, sizeof(uint32_t), s);
@@ -2371,10 +2384,10 @@ int launches_per_step(const pbf_ctx* ctx) {
   const int K = ctx->params.solve_steps;
   const int tail = (ctx->params.gamma != 0.0f ? 2 : 0) + 4;
   if (ctx->params.solver == 1 && !ctx->params.exact_math) {
-    // learned: warm iteration (features, network, delta-p) + (iters-1) x (check, decide, delta-p)
-    // + final check, decide + velocity
+    // learned: warm iteration (features, network, delta-p) + (iters-1) x (check, delta-p)
+    // + final check + velocity
     const int it = ctx->params.max_iterations > 0 ? ctx->params.max_iterations : 1;
-    return 1 + 3 + sort + 1 + 1 + 3 + 3 * (it - 1) + 2 + 1 + tail;
+    return 1 + 3 + sort + 1 + 1 + 3 + 2 * (it - 1) + 1 + 1 + tail;
   }
   const int per_iter = ctx->params.exact_math ? 3 : 2;
   return 1 + 3 + sort + 1 + 1 + per_iter * K + (K == 0 ? 1 : 0) + tail;

@@ -301,6 +301,8 @@ struct SolveState {
   double residual;      // mean clamped density error at the last check
   uint32_t done;        // residual at or below the tolerance: the rest of the step's iterations skip
   uint32_t iterations;  // Jacobi iterations applied this step
+  uint32_t ticket;      // blocks of the running check that have written their partial sum
+  uint32_t pad;
 };
 
 // Sum of v over the block (every thread calls it; blockDim.x a multiple of 32,
@@ -322,28 +324,35 @@ __device__ __forceinline__ void block_partial(float v, double* out) {
   }
 }
 
-// After a check pass: the mean error from the check's per-block partial sums
-// (added in a fixed order, so the decision is the same on every run), then
-// either stop or allow one more iteration (the final check of a step only
-// records the residual).  One block of kDecideThreads.
-constexpr int kDecideThreads = 256;
-__global__ void __launch_bounds__(kDecideThreads) k_decide(int n, float tol, int final_check,
-                                                           const double* __restrict__ partials, int nparts,
-                                                           SolveState* st) {
-  if (st->done) return;  // uniform: read by every thread before thread 0 writes
-  __shared__ double red[kDecideThreads];
+// The end of a residual check (every thread of every block calls it, after
+// block_partial): the last block to finish adds the grid's partial sums in a
+// fixed order (so the decision is the same on every run) and either stops the
+// step's iterations (mean error at or below tol) or allows one more (the final
+// check of a step only records the residual).
+template <int THREADS>
+__device__ __forceinline__ void decide_if_last(SolveState* st, const double* partials, int n, float tol,
+                                               int final_check) {
+  __shared__ unsigned last;
+  __shared__ double red[THREADS];
+  if (threadIdx.x == 0) {
+    __threadfence();  // this block's partial before its ticket
+    last = atomicAdd(&st->ticket, 1u) == gridDim.x - 1u;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
   double s = 0.0;
-  for (int i = threadIdx.x; i < nparts; i += kDecideThreads) s += partials[i];
+  for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x) s += __ldcg(partials + i);
   red[threadIdx.x] = s;
   __syncthreads();
-#pragma unroll
-  for (int o = kDecideThreads / 2; o > 0; o >>= 1) {
+  for (unsigned o = blockDim.x / 2; o > 0; o >>= 1) {
     if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
     __syncthreads();
   }
   if (threadIdx.x != 0) return;
   const double mean = red[0] / (double)(n > 0 ? n : 1);
   st->residual = mean;
+  st->ticket = 0u;
   if (mean <= (double)tol) st->done = 1u;
   else if (!final_check) st->iterations += 1u;
 }
