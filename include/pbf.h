@@ -48,6 +48,7 @@ extern "C" {
 /* Device-side error flag bits (pbf_stats_t.error_flags). */
 #define PBF_FLAG_KEY_RANGE 1u     /* a bin id fell outside the grid; clamped */
 #define PBF_FLAG_NONFINITE 2u     /* a non-finite position was hashed */
+#define PBF_FLAG_WAIT_TIMEOUT 4u  /* a kernel gave up a bounded wait on the tensor cores; that launch's results are invalid */
 
 /*
  * Parameter block.  Field meaning follows the reference's public

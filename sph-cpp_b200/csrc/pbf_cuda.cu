@@ -42,6 +42,7 @@
 #include "pbf_kernels.cuh"
 #include "pbf_fast.cuh"
 #include "pbf_learn.cuh"
+#include "pbf_mlp_tc.cuh"
 
 using pbf::Dev;
 using pbf::Fast;
@@ -944,8 +945,8 @@ __global__ void __launch_bounds__(kStageThreads) ks_density_lambda(Dev P, Fast F
 // network's first layer multiplies by zero; column 15 flags a particle the
 // reference-ordered nudge path handled), and the plain first-iteration
 // lambda l1 in xl.w.
-// kl_mlp: the network on the tensor cores, one warp per 16 particles, every
-// warp busy; lambda = the output kept between l1 and kWarmMaxGain * l1.
+// kl_mlp_tc<true>: the network on the tensor cores (tcgen05, below);
+// lambda = the output kept between l1 and kWarmMaxGain * l1.
 // A single over-relaxed iteration on its own overshoots and the overshoot
 // feeds the velocity update (measured on the oracle: 1 iteration at 2.5x
 // lambda ends near 4% density error where 1 plain iteration ends near 1.5%),
@@ -995,30 +996,158 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) kl_features(Dev P, F
   lam[b] = l1;
 }
 
-__global__ void __launch_bounds__(128) kl_mlp(pbf::MlpDev M, int n, const __nv_bfloat16* __restrict__ featb,
-                                              float4* xl, float* lam, float* lamsum) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  const int g = lane >> 2, t = lane & 3;
-  const int r0 = warp * 16;
-  if (r0 >= n) return;  // whole warp
-  const int ra = min(r0 + g, n - 1), rb = min(r0 + g + 8, n - 1);
-  const uint32_t* fa = reinterpret_cast<const uint32_t*>(featb + (size_t)ra * pbf::kMlpInPad);
-  const uint32_t* fb = reinterpret_cast<const uint32_t*>(featb + (size_t)rb * pbf::kMlpInPad);
-  uint32_t a[4] = {__ldg(fa + t), __ldg(fb + t), __ldg(fa + t + 4), __ldg(fb + t + 4)};
-  float y_lo, y_hi;
-  pbf::mlp_forward16(M, a, lane, y_lo, y_hi);
-  if (t != 0) return;
+// The network on the 5th-generation tensor cores (see pbf_mlp_tc.cuh): a
+// persistent grid of 256-thread CTAs, each holding the weights in shared
+// memory and 64 TMEM columns, walking 128-row tiles.  Two threads per row
+// (warps w and w + 4 read the same TMEM lanes), each for 32 of the 64 hidden
+// columns.  Per tile: the rows' BF16 features -> one M128 N64 K16 MMA ->
+// layer-1 epilogue (bias, GELU, BF16 back to shared memory as layer 2's A
+// operand) -> four M128 N64 K16 MMAs into the same columns -> layer-2
+// epilogue (bias, GELU, the dot with w3, the two halves added).
+// WARM: features from featb (column 15 flags the reference-ordered nudge
+// path), lambda = the output kept between l1 and kWarmMaxGain * l1.  PREDICT: normalised float features, y = the output.  A wait that
+// gives up raises PBF_FLAG_WAIT_TIMEOUT; every CTA frees its TMEM.
+template <bool WARM>
+__global__ void __launch_bounds__(pbf::tc::kThreads, 6) kl_mlp_tc(pbf::MlpDev M, int n,
+                                                              const __nv_bfloat16* __restrict__ featb,
+                                                              const float* __restrict__ feats, float4* xl,
+                                                              float* lam, float* lamsum, float* y, uint32_t* err) {
+  namespace T = pbf::tc;
+  __shared__ __align__(1024) uint8_t sB1[pbf::kMlpH * pbf::kMlpInPad * 2];  // W1 [64 n][16 k]
+  __shared__ __align__(1024) uint8_t sB2[pbf::kMlpH * pbf::kMlpH * 2];      // W2 [64 n][64 k]
+  __shared__ __align__(1024) uint8_t sA1[T::kRows * pbf::kMlpInPad * 2];    // features [128][16]
+  __shared__ __align__(1024) uint8_t sA2[T::kRows * pbf::kMlpH * 2];        // hidden 1 [128][64]
+  __shared__ float sb1[pbf::kMlpH], sb2[pbf::kMlpH], sw3[pbf::kMlpH], half2[T::kRows];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tslot;
+  __shared__ int fail;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int row = tid & (T::kRows - 1), h = tid >> 7;  // row in the tile, column half
+  const int tiles = (n + T::kRows - 1) / T::kRows;
+  for (int i = tid; i < pbf::kMlpH * 2; i += T::kThreads) {  // W1: 64 rows x 2 chunks of 8 along k
+    const int r = i >> 1, kc = (i & 1) * 8;
+    *reinterpret_cast<uint4*>(sB1 + T::core_off(r, kc, pbf::kMlpInPad)) =
+        *reinterpret_cast<const uint4*>(M.w1 + r * pbf::kMlpInPad + kc);
+  }
+  for (int i = tid; i < pbf::kMlpH * 8; i += T::kThreads) {  // W2: 64 rows x 8 chunks
+    const int r = i >> 3, kc = (i & 7) * 8;
+    *reinterpret_cast<uint4*>(sB2 + T::core_off(r, kc, pbf::kMlpH)) =
+        *reinterpret_cast<const uint4*>(M.w2 + r * pbf::kMlpH + kc);
+  }
+  if (tid < pbf::kMlpH) {
+    sb1[tid] = M.b1[tid];
+    sb2[tid] = M.b2[tid];
+    sw3[tid] = M.w3[tid];
+  }
+  const uint32_t bar = T::smem_u32(&mbar);
+  if (tid == 0) {
+    T::bar_init(bar, 1);
+    fail = 0;
+  }
+  if (warp == 0) T::tmem_alloc(T::smem_u32(&tslot));
+  T::fence_before_sync();
+  __syncthreads();
+  T::fence_after_sync();
+  const uint32_t tmem = tslot;
+  const uint32_t lanes = tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(32 * h);  // this thread's half
+  const float b3 = M.b3[0];
+  const uint64_t dB1 = T::smem_desc(T::smem_u32(sB1), 128, 256);
+  const uint32_t a1 = T::smem_u32(sA1), a2 = T::smem_u32(sA2), b2 = T::smem_u32(sB2);
+  uint32_t phase = 0;
+  for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const int r = tile * T::kRows + row;
+    uint4 f = make_uint4(0u, 0u, 0u, 0u);  // half h of the row's 16 features
+    if (r < n) {
+      if (WARM) {
+        f = reinterpret_cast<const uint4*>(featb + (size_t)r * pbf::kMlpInPad)[h];
+      } else if (h == 0) {
+        const float* x = feats + (size_t)r * pbf::kMlpIn;
+        f = make_uint4(pbf::pack_bf16x2(x[0], x[1]), pbf::pack_bf16x2(x[2], x[3]), pbf::pack_bf16x2(x[4], x[5]),
+                       pbf::pack_bf16x2(x[6], x[7]));
+      } else {
+        const float* x = feats + (size_t)r * pbf::kMlpIn;
+        f = make_uint4(pbf::pack_bf16x2(x[8], x[9]), pbf::pack_bf16x2(x[10], x[11]), 0u, 0u);
+      }
+    }
+    const uint32_t flag = f.w >> 16;  // h = 1: column 15 (WARM: the nudge path handled the particle)
+    // columns 12..15 meet zero rows of W1; the flag column is cleared for the MMA
+    *reinterpret_cast<uint4*>(sA1 + T::core_off(row, 8 * h, pbf::kMlpInPad)) =
+        h ? make_uint4(f.x, f.y, 0u, 0u) : f;
+    T::fence_proxy_async();
+    T::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+      T::fence_after_sync();
+      T::mma_bf16(tmem, T::smem_desc(a1, 128, 256), dB1, T::kIdescM128N64, 0u);
+      T::mma_commit(bar);
+    }
+    if (!T::bar_wait(bar, phase)) fail = 1;
+    phase ^= 1u;
+    __syncthreads();
+    if (fail) break;
+    T::fence_after_sync();
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const int r = r0 + g + 8 * h;
-    if (r >= n) break;
-    const uint32_t flag = __ldg(reinterpret_cast<const uint32_t*>(featb + (size_t)r * pbf::kMlpInPad) + 7);
-    const float4 x = xl[r];
-    float l = x.w;  // l1, or the nudge path's lambda
-    if ((flag >> 16) == 0u) l = fminf(fmaxf((h ? y_hi : y_lo) * M.label_scale, kWarmMaxGain * x.w), x.w);
-    xl[r] = make_float4(x.x, x.y, x.z, l);
-    lam[r] = l;
-    lamsum[r] = l;
+    for (int c = 0; c < 32; c += 16) {
+      float v[16];
+      T::tmem_ld16(lanes + (uint32_t)c, v);
+      const int c0 = 32 * h + c;
+#pragma unroll
+      for (int j = 0; j < 16; j += 8) {
+        uint4 w;
+        w.x = pbf::pack_bf16x2(pbf::gelu(v[j] + sb1[c0 + j]), pbf::gelu(v[j + 1] + sb1[c0 + j + 1]));
+        w.y = pbf::pack_bf16x2(pbf::gelu(v[j + 2] + sb1[c0 + j + 2]), pbf::gelu(v[j + 3] + sb1[c0 + j + 3]));
+        w.z = pbf::pack_bf16x2(pbf::gelu(v[j + 4] + sb1[c0 + j + 4]), pbf::gelu(v[j + 5] + sb1[c0 + j + 5]));
+        w.w = pbf::pack_bf16x2(pbf::gelu(v[j + 6] + sb1[c0 + j + 6]), pbf::gelu(v[j + 7] + sb1[c0 + j + 7]));
+        *reinterpret_cast<uint4*>(sA2 + T::core_off(row, c0 + j, pbf::kMlpH)) = w;
+      }
+    }
+    T::fence_proxy_async();
+    T::fence_before_sync();
+    __syncthreads();  // every layer-1 accumulator read before layer 2 overwrites them
+    if (tid == 0) {
+      T::fence_after_sync();
+#pragma unroll
+      for (int ks = 0; ks < 4; ++ks)
+        T::mma_bf16(tmem, T::smem_desc(a2 + 256u * ks, 128, 1024), T::smem_desc(b2 + 256u * ks, 128, 1024),
+                    T::kIdescM128N64, ks > 0 ? 1u : 0u);
+      T::mma_commit(bar);
+    }
+    if (!T::bar_wait(bar, phase)) fail = 1;
+    phase ^= 1u;
+    __syncthreads();
+    if (fail) break;
+    T::fence_after_sync();
+    float acc = 0.0f;
+#pragma unroll
+    for (int c = 0; c < 32; c += 16) {
+      float v[16];
+      T::tmem_ld16(lanes + (uint32_t)c, v);
+      const int c0 = 32 * h + c;
+#pragma unroll
+      for (int q = 0; q < 16; ++q) acc = fmaf(pbf::gelu(v[q] + sb2[c0 + q]), sw3[c0 + q], acc);
+    }
+    if (h == 0) half2[row] = acc;
+    T::fence_before_sync();
+    __syncthreads();  // the first halves in shared memory; TMEM and operands free for the next tile
+    if (h == 1 && r < n) {
+      const float yv = half2[row] + acc + b3;
+      if (WARM) {
+        const float4 x = xl[r];
+        float l = x.w;  // l1, or the nudge path's lambda
+        if (flag == 0u) l = fminf(fmaxf(yv * M.label_scale, kWarmMaxGain * x.w), x.w);
+        xl[r] = make_float4(x.x, x.y, x.z, l);
+        lam[r] = l;
+        lamsum[r] = l;
+      } else {
+        y[r] = yv;
+      }
+    }
+  }
+  if (fail && tid == 0) atomicOr(err, PBF_FLAG_WAIT_TIMEOUT);
+  __syncthreads();
+  if (warp == 0) {
+    T::fence_after_sync();
+    T::tmem_free(tmem);
   }
 }
 
@@ -1947,6 +2076,14 @@ bool any_staged(const pbf_ctx* ctx) {
 TileIO tile_io(const pbf_ctx* ctx) { return TileIO{ctx->tile_nruns, ctx->tile_total, ctx->tile_runs, ctx->nbr16}; }
 
 
+// The tensor-core network: a persistent grid of at most 6 CTAs per SM (the
+// most that 33 KB of shared memory each lets reside; 6 x 64 of the SM's 512
+// TMEM columns), never more CTAs than tiles.
+int mlp_tc_grid(const pbf_ctx* ctx, int n) {
+  const int tiles = (n + pbf::tc::kRows - 1) / pbf::tc::kRows;
+  return std::max(1, std::min(tiles, 6 * ctx->sms));
+}
+
 int grid_of(const pbf_ctx* ctx, int family) {
   if (ctx->tune.staged[family]) return (int)((ctx->n + kTile - 1) / kTile);
   return blocks_for(ctx->n * (size_t)ctx->tune.lanes[family], ctx->tune.block[family]);
@@ -2139,8 +2276,8 @@ void launch_learned_solve(pbf_ctx* ctx) {
   }
   {
     Launch L(ctx, "warm_mlp");
-    const int warps = (n + 15) / 16;
-    kl_mlp<<<(warps + 3) / 4, 128, 0, s>>>(M, n, ctx->featb, ctx->xl, ctx->lamH, ctx->lamsumH);
+    kl_mlp_tc<true><<<mlp_tc_grid(ctx, n), pbf::tc::kThreads, 0, s>>>(M, n, ctx->featb, nullptr, ctx->xl, ctx->lamH,
+                                                                 ctx->lamsumH, nullptr, ctx->err);
   }
   const TileIO tio = tile_io(ctx);
   if (T.staged[PBF_TUNE_DELTA_P]) {
@@ -3263,11 +3400,16 @@ int pbf_mlp_predict(pbf_ctx* ctx, const float* features, size_t n, float* y) {
   float* df = ctx->stage;
   float* dy = ctx->stage + n * pbf::kMlpIn;
   CK(cudaMemcpyAsync(df, features, n * pbf::kMlpIn * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
-  const int warps = (int)((n + 15) / 16);
-  pbf::k_mlp_predict<false><<<(warps + 3) / 4, 128, 0, ctx->stream>>>(mlp_dev(ctx), df, (int)n, dy);
+  kl_mlp_tc<false><<<mlp_tc_grid(ctx, (int)n), pbf::tc::kThreads, 0, ctx->stream>>>(
+      mlp_dev(ctx), (int)n, nullptr, df, nullptr, nullptr, nullptr, dy, ctx->err);
   if (int rc = check_launch(ctx, "mlp_predict")) return rc;
+  uint32_t err = 0;
   CK(cudaMemcpyAsync(y, dy, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(&err, ctx->err, sizeof(err), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
+  // the context's error word (the step's flags are kept: a timeout raised by
+  // an earlier step fails this call too, the context's tensor-core path has failed)
+  if (err & PBF_FLAG_WAIT_TIMEOUT) return fail(ctx, PBF_ERR_DEVICE, "mlp_predict: a tensor-core wait timed out");
   return PBF_OK;
 }
 

@@ -244,31 +244,6 @@ __global__ void __launch_bounds__(128) k_mlp_grad(MlpDev M, const float* __restr
   }
 }
 
-// Network output for n rows of features (NORMALIZE: raw features).
-template <bool NORMALIZE>
-__global__ void __launch_bounds__(128) k_mlp_predict(MlpDev M, const float* __restrict__ feats, int n, float* y) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  const int g = lane >> 2, t = lane & 3;
-  const int r0 = warp * 16;
-  if (r0 >= n) return;  // whole warp exits together
-  auto f = [&](int r, int k) {
-    if (r >= n || k >= kMlpIn) return 0.0f;
-    const float x = feats[(size_t)r * kMlpIn + k];
-    return NORMALIZE ? (x - M.feat_mean[k]) * M.feat_inv_std[k] : x;
-  };
-  uint32_t a[4];
-  a[0] = pack_bf16x2(f(r0 + g, 2 * t), f(r0 + g, 2 * t + 1));
-  a[1] = pack_bf16x2(f(r0 + g + 8, 2 * t), f(r0 + g + 8, 2 * t + 1));
-  a[2] = pack_bf16x2(f(r0 + g, 2 * t + 8), f(r0 + g, 2 * t + 9));
-  a[3] = pack_bf16x2(f(r0 + g + 8, 2 * t + 8), f(r0 + g + 8, 2 * t + 9));
-  float y_lo, y_hi;
-  mlp_forward16(M, a, lane, y_lo, y_hi);
-  if (t == 0) {
-    if (r0 + g < n) y[r0 + g] = y_lo;
-    if (r0 + g + 8 < n) y[r0 + g + 8] = y_hi;
-  }
-}
-
 // ---- features and the residual-checked solve ----
 
 // Raw features of a particle at its first Jacobi iteration (order documented
