@@ -353,6 +353,65 @@ def test_all_particles_in_one_cell():
     assert gc.min() == 60
 
 
+def _bin_face_positions(sc, s, frac=0.25, seed=5):
+    """The jittered lattice with a share of its coordinates moved to values
+    just below a bin face where the float re-hash of c - s, c, c + s
+    (floor((v + s)/s) in float32, neighbors.h:109-114 and 172-185) does not
+    give three consecutive bins.  Returns the positions and how many
+    particles re-hash that way."""
+    f = np.float32
+    s = f(s)
+
+    def axis_bin(v):
+        return np.floor(f(f(v + s) / s))
+
+    def rehash(c):
+        return axis_bin(f(c - s)), axis_bin(c), axis_bin(f(c + s))
+
+    quirks = set()
+    for k in range(int(max(sc.box_max) / s) + 1):  # a few ulps either side of every face k*s
+        for direction in (-np.inf, np.inf):
+            v = f(f(k) * s)
+            for _ in range(8):
+                v = np.nextafter(v, f(direction), dtype=np.float32)
+                b0, b1, b2 = rehash(v)
+                if v > 0 and not (b0 + 1 == b1 and b1 + 1 == b2):
+                    quirks.add(float(v))
+    quirks = np.array(sorted(quirks), np.float32)
+    assert quirks.size > 0
+    x = sc.positions()
+    rng = np.random.default_rng(seed)
+    for a in range(3):
+        for i in np.flatnonzero(rng.random(x.shape[0]) < frac):
+            d = np.abs(quirks - x[i, a])
+            j = int(np.argmin(d))
+            if d[j] < 0.3 and quirks[j] < sc.box_max[a]:
+                x[i, a] = quirks[j]
+    b0, b1, b2 = rehash(x)
+    odd = ~((b0 + 1 == b1) & (b1 + 1 == b2)).all(axis=1)
+    return x, int(odd.sum())
+
+
+def test_lists_at_bin_faces_bit_exact():
+    """Particles whose float re-hash skips or repeats a bin walk their own 27
+    bins; the others of their bin share one sweep of the bin's neighbourhood.
+    Lists bit-exact against the oracle, in exact and in fast math."""
+    sc = make_scene("dam_8k", gravity=0.0)
+    x, odd = _bin_face_positions(sc, sc.params().neighbor_bin_spacing)
+    assert odd > 200, odd
+    for exact in (1, 0):
+        p = sc.with_(exact_math=exact).params()
+        g = Particles(p, sc.n)
+        o = OracleSim(p, sc.n)
+        g.upload(x)
+        o.set_state(x)
+        for i, fn in enumerate((g.apply_external_forces, g.predict_positions, g.find_neighbors)):
+            fn()
+            o.stage(i)
+        assert np.array_equal(g.get_array(ARRAY_POSITION_STARS), x)  # the lists are built on these very values
+        assert_lists_equal(g, o, p.neighbor_cap)
+
+
 def _coincident_scene():
     sc = make_scene("dam_2k")
     x = sc.positions()
