@@ -138,6 +138,7 @@ def kernel_bytes(name: str, n: int, nbar: float, K: int, nbins: int) -> float:
         "warm_mlp": 32 + 16 + 16 + 4 + 4,                       # features, (x*, l1) in; (x*, lambda), lambda, sum out
         "residual_check": 16 + L + 16 + 4 + 4,                  # as density_lambda
         "reorder": 8 + 4 + 3 * 16 + 3 * 16 + 4 + 4,             # pair, key, (x, x*, v) in and out, orig, key
+        "runs": 16 + 4,                                         # x* in (the previous slot's is a cache hit); run end out
         "fill_neighbors": 16 + 4 * nbar + 4 + 8.0 * nbins / n,  # own x*, list + count out, bin starts
         "density_lambda": 16 + L + 16 + 4 + 4,                  # x* in; list; (x*, lambda), rho, lambda out
         "dp_update": 16 + L + 16 + (32.0 / K),                  # (x*, lambda) in; list; x* out; last: x in, v out

@@ -469,6 +469,74 @@ __global__ void k_reorder(int n, const unsigned long long* __restrict__ pairs, c
   if (lamS) lamS[b] = lamH[a];  // FULL: lambda; fused step: last step's lambda sum, when kept
 }
 
+// Runs of bit-identical x* among consecutive sorted slots (particles piled
+// onto one point, e.g. clamped into a box corner by a collapsing scene):
+// run_end[i] = the first slot j > i whose x* differs from slot j - 1's, or the
+// end of i's block of kRunBlock slots, whichever comes first.  Equal x* gives
+// equal distance tests, so the list fill decides a whole run with one test.
+constexpr int kRunBlock = 1024;
+__global__ void __launch_bounds__(kRunBlock) k_runs(int n, const float4* __restrict__ pst, uint32_t* run_end) {
+  __shared__ uint32_t wfirst[kRunBlock / 32];  // first run start of every warp's 32 slots
+  const int i = blockIdx.x * kRunBlock + threadIdx.x;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint32_t base = (uint32_t)blockIdx.x * kRunBlock;
+  const uint32_t bend = min(base + (uint32_t)kRunBlock, (uint32_t)n);
+  bool start = false;
+  if (i < n) {
+    if (threadIdx.x == 0) {
+      start = true;
+    } else {
+      const float4 a = pst[i], b = pst[i - 1];
+      start = __float_as_uint(a.x) != __float_as_uint(b.x) || __float_as_uint(a.y) != __float_as_uint(b.y) ||
+              __float_as_uint(a.z) != __float_as_uint(b.z);
+    }
+  }
+  const unsigned m = __ballot_sync(0xffffffffu, start);
+  if (lane == 0) wfirst[w] = m ? base + (uint32_t)(w * 32 + __ffs(m) - 1) : 0xffffffffu;
+  __syncthreads();
+  if (i >= n) return;
+  const unsigned above = m & ~((2u << lane) - 1u);  // starts in this warp after slot i
+  uint32_t e = bend;
+  if (above) {
+    e = base + (uint32_t)(w * 32 + __ffs(above) - 1);
+  } else {
+    for (int v = w + 1; v < kRunBlock / 32; ++v)
+      if (wfirst[v] != 0xffffffffu) {
+        e = wfirst[v];
+        break;
+      }
+  }
+  run_end[i] = e;
+}
+
+// Bins holding more particles than this walk their candidates run by run.
+constexpr uint32_t kRunBin = 512;
+
+// One crowded bin [q0, q1) of the list fill, run by run: one distance test per
+// run of bit-identical x*; on a hit the run's slots are appended in order, the
+// particle's own slot left out, while the list has room.  Returns the new
+// length.  Out of line, so that the common per-candidate loop keeps its code.
+__device__ __noinline__ int fill_runs(float px, float py, float pz, float s2, int cap, uint32_t self, uint32_t q0,
+                                      uint32_t q1, const float4* __restrict__ pst,
+                                      const uint32_t* __restrict__ run_end, int32_t* row, uint16_t* row16, int off,
+                                      int count) {
+  for (uint32_t q = q0; q < q1;) {
+    const float4 xq = pst[q];
+    const uint32_t qe = min(run_end[q], q1);
+    const float d2 = pbf::mag2<true>(pbf::xsub(px, xq.x), pbf::xsub(py, xq.y), pbf::xsub(pz, xq.z));
+    if (d2 < s2) {
+      for (uint32_t r = q; r < qe && count < cap; ++r) {
+        if (r == self) continue;
+        if (row16) row16[count] = (uint16_t)((int)r + off);
+        row[count++] = (int32_t)r;
+      }
+      if (count >= cap) break;
+    }
+    q = qe;
+  }
+  return count;
+}
+
 // fill_neighbors (neighbors.h:197-230) over slots in sorted order: the 27
 // bins in the reference's order (x offset outer, z inner, float re-hash of
 // coord + i*s), candidates of a bin in ascending reference index, strict
@@ -478,7 +546,10 @@ __global__ void k_reorder(int n, const unsigned long long* __restrict__ pairs, c
 // particle to the bin's face, less a margin of many ulps of the coordinate
 // (P.skip_eps), squared and summed, exceeds s^2.  Only bins equal to the
 // integer offset of the particle's own bin are skipped, so the reference's
-// float re-hash still decides which bins are visited.
+// float re-hash still decides which bins are visited.  A bin of more than
+// kRunBin particles is walked run by run (k_runs): a run of bit-identical x*
+// is one distance test, and on a hit its slots are appended in order (the
+// particle's own slot left out), the list the one-by-one walk gives.
 constexpr int kFillBlock = 128;
 
 // Tiles of kTile consecutive sorted slots (one warp of the list fill, one
@@ -498,7 +569,8 @@ struct TileIO {
 
 template <bool STAGE>
 __global__ void __launch_bounds__(kFillBlock) k_fill2(Dev P, int n, size_t stride, const float4* __restrict__ pst,
-                                                      const uint32_t* __restrict__ cell_start, int32_t* nbr,
+                                                      const uint32_t* __restrict__ cell_start,
+                                                      const uint32_t* __restrict__ run_end, int32_t* nbr,
                                                       int32_t* cnt, uint32_t* err, TileIO T) {
   const int b = blockIdx.x * kFillBlock + threadIdx.x;
   if (!STAGE && b >= n) return;
@@ -602,13 +674,18 @@ __global__ void __launch_bounds__(kFillBlock) k_fill2(Dev P, int n, size_t strid
           if (cx < xmn - 1 || cx > xmx + 1 || ry < 0 || ry >= ny || rz < 0 || rz >= nz) stray = true;
           else off = soff[(threadIdx.x & ~31) + rz * ny + ry];
         }
-        const uint32_t q1 = cell_start[nb + 1];
-        for (uint32_t q = cell_start[nb]; q < q1; ++q) {
-          const float4 xq = pst[q];
-          const float d2 = pbf::mag2<true>(pbf::xsub(xp.x, xq.x), pbf::xsub(xp.y, xq.y), pbf::xsub(xp.z, xq.z));
-          if (d2 < P.s2 && q != (uint32_t)b && count < cap) {
-            if (STAGE && staged) row16[count] = (uint16_t)((int)q + off);
-            row[count++] = (int32_t)q;
+        const uint32_t q0 = cell_start[nb], q1 = cell_start[nb + 1];
+        if (q1 - q0 > kRunBin) {
+          count = fill_runs(xp.x, xp.y, xp.z, P.s2, cap, (uint32_t)b, q0, q1, pst, run_end, row,
+                            STAGE && staged ? row16 : nullptr, off, count);
+        } else {
+          for (uint32_t q = q0; q < q1; ++q) {
+            const float4 xq = pst[q];
+            const float d2 = pbf::mag2<true>(pbf::xsub(xp.x, xq.x), pbf::xsub(xp.y, xq.y), pbf::xsub(xp.z, xq.z));
+            if (d2 < P.s2 && q != (uint32_t)b && count < cap) {
+              if (STAGE && staged) row16[count] = (uint16_t)((int)q + off);
+              row[count++] = (int32_t)q;
+            }
           }
         }
         if (count >= cap) goto done;
@@ -1781,6 +1858,7 @@ struct pbf_ctx {
   float4 *posS = nullptr, *pstS = nullptr, *velS = nullptr, *scrS = nullptr, *xl = nullptr, *velT = nullptr;
   float *lamH = nullptr, *lamS = nullptr;
   uint32_t *origH = nullptr, *origS = nullptr, *key = nullptr, *keyH = nullptr;
+  uint32_t* run_end = nullptr;  // per sorted slot: end of its run of bit-identical x* (k_runs)
   // radix sort: keys at the reference index and their ping-pong twin, digit
   // histograms, their scan, scan partials; `sorted` = the pair buffer holding
   // the sorted pairs after the last pass
@@ -2215,13 +2293,19 @@ void launch_sort_to_pairs(pbf_ctx* ctx) {
 }
 
 void launch_fill(pbf_ctx* ctx, const float4* pst) {
+  {
+    Launch L(ctx, "runs");
+    k_runs<<<blocks_for(ctx->n, kRunBlock), kRunBlock, 0, ctx->stream>>>((int)ctx->n, pst, ctx->run_end);
+  }
   Launch L(ctx, "fill_neighbors");
   if (any_staged(ctx))
     k_fill2<true><<<blocks_for(ctx->n, kFillBlock), kFillBlock, 0, ctx->stream>>>(
-        ctx->dev, (int)ctx->n, ctx->lstride, pst, ctx->cell_start, ctx->nbr, ctx->cnt, ctx->err, tile_io(ctx));
+        ctx->dev, (int)ctx->n, ctx->lstride, pst, ctx->cell_start, ctx->run_end, ctx->nbr, ctx->cnt, ctx->err,
+        tile_io(ctx));
   else
     k_fill2<false><<<blocks_for(ctx->n, kFillBlock), kFillBlock, 0, ctx->stream>>>(
-        ctx->dev, (int)ctx->n, ctx->lstride, pst, ctx->cell_start, ctx->nbr, ctx->cnt, ctx->err, tile_io(ctx));
+        ctx->dev, (int)ctx->n, ctx->lstride, pst, ctx->cell_start, ctx->run_end, ctx->nbr, ctx->cnt, ctx->err,
+        tile_io(ctx));
 }
 
 // ---- the fused step (graph-capturable: fixed pointers, no host sync) ----
@@ -2514,7 +2598,7 @@ void launch_step(pbf_ctx* ctx) {
 
 int launches_per_step(const pbf_ctx* ctx) {
   // kernels only (the memsets are not): ext/predict/hash + 3 scan + radix
-  // passes x (histogram, 3 scan, scatter) + reorder + fill + K x
+  // passes x (histogram, 3 scan, scatter) + reorder + runs + fill + K x
   // (density/lambda, [exact: lambda fix-up], delta-p) + (K==0: velocity)
   // + 2 if gamma + 4 (visc, vort, apply, visc)
   const int sort = 5 * ctx->radix_passes;
@@ -2524,10 +2608,10 @@ int launches_per_step(const pbf_ctx* ctx) {
     // learned: warm iteration (features, network, delta-p) + (iters-1) x (check, delta-p)
     // + final check + velocity
     const int it = ctx->params.max_iterations > 0 ? ctx->params.max_iterations : 1;
-    return 1 + 3 + sort + 1 + 1 + 3 + 2 * (it - 1) + 1 + 1 + tail;
+    return 1 + 3 + sort + 1 + 2 + 3 + 2 * (it - 1) + 1 + 1 + tail;
   }
   const int per_iter = ctx->params.exact_math ? 3 : 2;
-  return 1 + 3 + sort + 1 + 1 + per_iter * K + (K == 0 ? 1 : 0) + tail;
+  return 1 + 3 + sort + 1 + 2 + per_iter * K + (K == 0 ? 1 : 0) + tail;
 }
 
 }  // namespace
@@ -2595,7 +2679,7 @@ static int create_ctx(const pbf_params* p, size_t capacity, const pbf_scene* sce
       (rc = dalloc(ctx, &ctx->velT, C + 1)) || (rc = dalloc(ctx, &ctx->lamH, C)) || (rc = dalloc(ctx, &ctx->lamS, C)) ||
       (rc = dalloc(ctx, &ctx->origH, C)) || (rc = dalloc(ctx, &ctx->origS, C)) || (rc = dalloc(ctx, &ctx->key, C)) ||
       (rc = dalloc(ctx, &ctx->key_ref, C)) || (rc = dalloc(ctx, &ctx->key_alt, C)) ||
-      (rc = dalloc(ctx, &ctx->keyH, C)) ||
+      (rc = dalloc(ctx, &ctx->keyH, C)) || (rc = dalloc(ctx, &ctx->run_end, C)) ||
       (rc = dalloc(ctx, &ctx->radix_hist, radix_entries(C))) ||
       (rc = dalloc(ctx, &ctx->radix_off, radix_entries(C) + 1)) ||
       (rc = dalloc(ctx, &ctx->radix_parts, (radix_entries(C) + 1 + kScanTile - 1) / kScanTile)) ||

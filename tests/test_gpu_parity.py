@@ -412,6 +412,48 @@ def test_lists_at_bin_faces_bit_exact():
         assert_lists_equal(g, o, p.neighbor_cap)
 
 
+def _crowded_corner_positions(sc, seed=9):
+    """The jittered lattice with a collapsed corner: every third particle of
+    the first 6,000 piled onto one point near the box corner, and every third
+    one after it (of the first 600) scattered inside the same bin, so the
+    corner bin holds about 2,200 particles whose bit-identical runs are broken
+    by distinct ones in index order."""
+    x = sc.positions()
+    rng = np.random.default_rng(seed)
+    x[0:6000:3] = (0.05, 0.05, 0.05)
+    k = len(range(1, 600, 3))
+    x[1:600:3] = rng.uniform(0.0, 0.6, (k, 3)).astype(np.float32)
+    return x
+
+
+def test_crowded_corner_runs_bit_exact():
+    """A bin of thousands of particles, most of them on one point: the fill
+    decides each run of identical positions with one distance test.  Lists
+    bit-exact against the oracle (stages, exact and fast math), and the fused
+    exact step stays bit-identical to the oracle."""
+    sc = make_scene("dam_8k")
+    x = _crowded_corner_positions(sc)
+    for exact in (1, 0):
+        p = sc.with_(exact_math=exact).params()
+        g = Particles(p, sc.n)
+        o = OracleSim(p, sc.n)
+        g.upload(x)
+        o.set_state(x)
+        for i, fn in enumerate((g.apply_external_forces, g.predict_positions, g.find_neighbors)):
+            fn()
+            o.stage(i)
+        b = g.bins()
+        assert (b["bin_end"].astype(np.int64) - b["bin_begin"]).max() > 2000  # the crowded bin is there
+        assert_lists_equal(g, o, p.neighbor_cap)
+    sc2, p, g, o = pair(sc)
+    g.upload(x)
+    o.set_state(x)
+    g.step(3)
+    o.step(3)
+    assert_arrays(g, o, which=(ARRAY_POSITIONS, ARRAY_VELOCITIES, ARRAY_DENSITIES))
+    assert_lists_equal(g, o, p.neighbor_cap)
+
+
 def _coincident_scene():
     sc = make_scene("dam_2k")
     x = sc.positions()
