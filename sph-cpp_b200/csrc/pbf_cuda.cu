@@ -1541,7 +1541,7 @@ __device__ __forceinline__ void dp_update_tile(int tile, const Dev& P, const Fas
   const int c = G.live ? cnt[b] : 0;
   float ax = 0.f, ay = 0.f, az = 0.f;
   const float lp = xp.w;
-  pbf::walk1<GL, STAGED>(nbr + (size_t)b * stride, STAGED ? src.nbr16 + (size_t)b * stride : nullptr, c,
+  pbf::walk1<GL, STAGED, true>(nbr + (size_t)b * stride, STAGED ? src.nbr16 + (size_t)b * stride : nullptr, c,
                          STAGED ? src.dummy : n, G.lane, STAGED ? src.a : xl, [&](int, float4 xq) {
     const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
     const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
@@ -1616,7 +1616,7 @@ __device__ __forceinline__ void viscosity_tile(int tile, const Fast& F, int n, s
   const float4 xp = pst[b], vp = vin[b];
   const int c = G.live ? cnt[b] : 0;
   float ax = 0.f, ay = 0.f, az = 0.f;
-  pbf::walk2<GL, STAGED>(nbr + (size_t)b * stride, STAGED ? src.nbr16 + (size_t)b * stride : nullptr, c,
+  pbf::walk2<GL, STAGED, FINAL>(nbr + (size_t)b * stride, STAGED ? src.nbr16 + (size_t)b * stride : nullptr, c,
                          STAGED ? src.dummy : n, G.lane, STAGED ? src.a : pst, STAGED ? src.b : vin,
                          [&](int, float4 xq, float4 vq) {
     const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;

@@ -111,62 +111,106 @@ __device__ __forceinline__ float gmin(float v) {
 // Walk a list row: lane l of the group takes entries 4l..4l+3 of every
 // 4*GL-entry batch, one 16-byte index load, then its four neighbour records
 // (four independent loads in flight), then the four bodies.  Rows are padded
-// to a multiple of 32 entries, so the last, partial batch reads whole vectors
-// too; its entries past the count are replaced by `dummy`, a slot whose every
-// term is zero.
-template <int GL = kGL, class Body>
+// to a multiple of 32 entries, so every batch reads whole vectors inside the
+// row; entries of the last batch past the count are replaced by `dummy`, a
+// slot whose every term is zero.  PF: the next batch's index vector is loaded
+// before this batch's records (the lists stream from DRAM; the prefetch takes
+// one DRAM round trip per batch off the index -> record chain).  It is set
+// where it measured faster (Δp, the final XSPH pass); elsewhere it measured
+// slower.
+template <int GL = kGL, bool PF = false, class Body>
 __device__ __forceinline__ void gwalk1(const int32_t* __restrict__ row, int c, int dummy, int lane,
                                        const float4* __restrict__ a, Body&& body) {
   const int4* r4 = reinterpret_cast<const int4*>(row);
-  const int full = c / (4 * GL);
-  int t = 0;
-  for (; t < full; ++t) {
-    const int4 q = __ldg(r4 + t * GL + lane);
-    const float4 v0 = __ldg(a + q.x), v1 = __ldg(a + q.y), v2 = __ldg(a + q.z), v3 = __ldg(a + q.w);
-    body(q.x, v0);
-    body(q.y, v1);
-    body(q.z, v2);
-    body(q.w, v3);
-  }
-  if (t * 4 * GL < c) {
-    int4 q = __ldg(r4 + t * GL + lane);
-    const int e = t * 4 * GL + 4 * lane;
-    q.x = e < c ? q.x : dummy;
-    q.y = e + 1 < c ? q.y : dummy;
-    q.z = e + 2 < c ? q.z : dummy;
-    q.w = e + 3 < c ? q.w : dummy;
-    const float4 v0 = __ldg(a + q.x), v1 = __ldg(a + q.y), v2 = __ldg(a + q.z), v3 = __ldg(a + q.w);
-    body(q.x, v0);
-    body(q.y, v1);
-    body(q.z, v2);
-    body(q.w, v3);
+  if constexpr (PF) {
+    const int batches = (c + 4 * GL - 1) / (4 * GL);
+    if (batches == 0) return;
+    int4 next = __ldg(r4 + lane);
+    for (int t = 0; t < batches; ++t) {
+      int4 q = next;
+      if (t + 1 < batches) next = __ldg(r4 + (t + 1) * GL + lane);
+      if (t + 1 == batches) {
+        const int e = t * 4 * GL + 4 * lane;
+        q.x = e < c ? q.x : dummy;
+        q.y = e + 1 < c ? q.y : dummy;
+        q.z = e + 2 < c ? q.z : dummy;
+        q.w = e + 3 < c ? q.w : dummy;
+      }
+      const float4 v0 = __ldg(a + q.x), v1 = __ldg(a + q.y), v2 = __ldg(a + q.z), v3 = __ldg(a + q.w);
+      body(q.x, v0);
+      body(q.y, v1);
+      body(q.z, v2);
+      body(q.w, v3);
+    }
+  } else {
+    const int full = c / (4 * GL);
+    int t = 0;
+    for (; t < full; ++t) {
+      const int4 q = __ldg(r4 + t * GL + lane);
+      const float4 v0 = __ldg(a + q.x), v1 = __ldg(a + q.y), v2 = __ldg(a + q.z), v3 = __ldg(a + q.w);
+      body(q.x, v0);
+      body(q.y, v1);
+      body(q.z, v2);
+      body(q.w, v3);
+    }
+    if (t * 4 * GL < c) {
+      int4 q = __ldg(r4 + t * GL + lane);
+      const int e = t * 4 * GL + 4 * lane;
+      q.x = e < c ? q.x : dummy;
+      q.y = e + 1 < c ? q.y : dummy;
+      q.z = e + 2 < c ? q.z : dummy;
+      q.w = e + 3 < c ? q.w : dummy;
+      const float4 v0 = __ldg(a + q.x), v1 = __ldg(a + q.y), v2 = __ldg(a + q.z), v3 = __ldg(a + q.w);
+      body(q.x, v0);
+      body(q.y, v1);
+      body(q.z, v2);
+      body(q.w, v3);
+    }
   }
 }
 
 // Two records per neighbour: entries 2l, 2l+1 of every 2*GL-entry batch (an
 // 8-byte index load), so that four records are in flight per lane, as in the
-// one-record walk.
-template <int GL = kGL, class Body>
+// one-record walk; PF as there.
+template <int GL = kGL, bool PF = false, class Body>
 __device__ __forceinline__ void gwalk2(const int32_t* __restrict__ row, int c, int dummy, int lane,
                                        const float4* __restrict__ a, const float4* __restrict__ bsrc,
                                        Body&& body) {
   const int2* r2 = reinterpret_cast<const int2*>(row);
-  const int full = c / (2 * GL);
-  int t = 0;
-  for (; t < full; ++t) {
-    const int2 q = __ldg(r2 + t * GL + lane);
-    const float4 a0 = __ldg(a + q.x), b0 = __ldg(bsrc + q.x), a1 = __ldg(a + q.y), b1 = __ldg(bsrc + q.y);
-    body(q.x, a0, b0);
-    body(q.y, a1, b1);
-  }
-  if (t * 2 * GL < c) {
-    int2 q = __ldg(r2 + t * GL + lane);
-    const int e = t * 2 * GL + 2 * lane;
-    q.x = e < c ? q.x : dummy;
-    q.y = e + 1 < c ? q.y : dummy;
-    const float4 a0 = __ldg(a + q.x), b0 = __ldg(bsrc + q.x), a1 = __ldg(a + q.y), b1 = __ldg(bsrc + q.y);
-    body(q.x, a0, b0);
-    body(q.y, a1, b1);
+  if constexpr (PF) {
+    const int batches = (c + 2 * GL - 1) / (2 * GL);
+    if (batches == 0) return;
+    int2 next = __ldg(r2 + lane);
+    for (int t = 0; t < batches; ++t) {
+      int2 q = next;
+      if (t + 1 < batches) next = __ldg(r2 + (t + 1) * GL + lane);
+      if (t + 1 == batches) {
+        const int e = t * 2 * GL + 2 * lane;
+        q.x = e < c ? q.x : dummy;
+        q.y = e + 1 < c ? q.y : dummy;
+      }
+      const float4 a0 = __ldg(a + q.x), b0 = __ldg(bsrc + q.x), a1 = __ldg(a + q.y), b1 = __ldg(bsrc + q.y);
+      body(q.x, a0, b0);
+      body(q.y, a1, b1);
+    }
+  } else {
+    const int full = c / (2 * GL);
+    int t = 0;
+    for (; t < full; ++t) {
+      const int2 q = __ldg(r2 + t * GL + lane);
+      const float4 a0 = __ldg(a + q.x), b0 = __ldg(bsrc + q.x), a1 = __ldg(a + q.y), b1 = __ldg(bsrc + q.y);
+      body(q.x, a0, b0);
+      body(q.y, a1, b1);
+    }
+    if (t * 2 * GL < c) {
+      int2 q = __ldg(r2 + t * GL + lane);
+      const int e = t * 2 * GL + 2 * lane;
+      q.x = e < c ? q.x : dummy;
+      q.y = e + 1 < c ? q.y : dummy;
+      const float4 a0 = __ldg(a + q.x), b0 = __ldg(bsrc + q.x), a1 = __ldg(a + q.y), b1 = __ldg(bsrc + q.y);
+      body(q.x, a0, b0);
+      body(q.y, a1, b1);
+    }
   }
 }
 
@@ -236,22 +280,22 @@ __device__ __forceinline__ void swalk2(const uint16_t* __restrict__ row16, int c
 }
 
 // One walk for both sources: staged (shared memory, 16-bit list) or direct.
-template <int GL, bool STAGED, class Body>
+template <int GL, bool STAGED, bool PF = false, class Body>
 __device__ __forceinline__ void walk1(const int32_t* row, const uint16_t* row16, int c, int dummy, int lane,
                                       const float4* src, Body&& body) {
   if (STAGED)
     swalk1<GL>(row16, c, dummy, lane, src, body);
   else
-    gwalk1<GL>(row, c, dummy, lane, src, body);
+    gwalk1<GL, PF>(row, c, dummy, lane, src, body);
 }
 
-template <int GL, bool STAGED, class Body>
+template <int GL, bool STAGED, bool PF = false, class Body>
 __device__ __forceinline__ void walk2(const int32_t* row, const uint16_t* row16, int c, int dummy, int lane,
                                       const float4* sa, const float4* sb, Body&& body) {
   if (STAGED)
     swalk2<GL>(row16, c, dummy, lane, sa, sb, body);
   else
-    gwalk2<GL>(row, c, dummy, lane, sa, sb, body);
+    gwalk2<GL, PF>(row, c, dummy, lane, sa, sb, body);
 }
 
 // (h - r)^2 / r for r < h, else 0 (the Del_Spikey magnitude over r, no norm).
