@@ -7,7 +7,13 @@ particle's features at its first Jacobi iteration and, as label, the sum of
 the lambdas the plain solver applied over its K iterations.  One Adam update
 on a batch drawn from that step follows each step.
 
-    python -m pbf_b200.learn --out model.npz [--scene dam_1m] [--trajectories 10] [--steps 200]
+    python -m pbf_b200.learn --out model.npz [--scene dam_1m] [--trajectories 10] [--steps 200] [--runs 4]
+
+Training reduces its weight gradients with atomics, so two runs of the same
+recipe differ; on the 1M dam they have needed from 2.2 to 2.8 solver
+iterations per step.  --runs R trains R weight initialisations and keeps the
+network whose learned solver needs the fewest iterations on a validation
+seed that neither training nor the plain-vs-learned comparison uses.
 
 The warm start targets the regime where the plain solver reaches a mean
 clamped density error near 1% of rest density: relaxation epsilon 1 (at the
@@ -29,6 +35,11 @@ from .scenes import Scene, make_scene
 TRAIN_EPSILON = 1.0
 # jitter seeds of the training trajectories (evaluation uses other seeds)
 TRAIN_SEEDS = tuple(1000 + 17 * i for i in range(10))
+# jitter seed of the validation run stored with a trained model: neither a
+# training seed nor the seed of the plain-vs-learned comparison (4242)
+VALIDATION_SEED = 5151
+# initialisation seeds of the weights, one per training run (--runs)
+INIT_SEEDS = (7, 11, 13, 17, 19, 23, 29, 31)
 MODEL_DIR = Path(__file__).resolve().parent / "models"
 DEFAULT_MODEL = MODEL_DIR / "warm_start_dam_eps1.npz"
 
@@ -140,6 +151,19 @@ def run_solver(scene: Scene, steps: int, params=None, norm=None, warmup: int = 0
     return {"residual": np.array(res), "iterations": np.array(its)}
 
 
+def validate(scene_name: str, params: np.ndarray, norm: np.ndarray, seed: int = VALIDATION_SEED,
+             steps: int = 20, warmup: int = 100) -> dict:
+    """The learned solver with this network on a held-out seed, as the
+    comparison runs it (residual_tol 1%, at most 10 iterations): mean
+    iterations per step and mean clamped density error over `steps` steps
+    after `warmup` steps.  The training loss alone does not predict the
+    iteration count (networks of lower loss have needed more iterations)."""
+    sc = warm_start_scene(scene_name, seed=seed, solver=1, residual_tol=0.01, max_iterations=10)
+    r = run_solver(sc, steps, params, norm, warmup=warmup)
+    return {"seed": seed, "steps": f"{warmup}..{warmup + steps}", "mean_iterations": float(r["iterations"].mean()),
+            "mean_density_error": float(r["residual"].mean())}
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", type=Path, default=DEFAULT_MODEL)
@@ -149,15 +173,38 @@ def main(argv=None) -> int:
     ap.add_argument("--batch", type=int, default=65536)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--adam-per-step", type=int, default=1)
+    ap.add_argument("--no-validate", action="store_true", help="skip the held-out learned-solver run")
+    ap.add_argument("--runs", type=int, default=1,
+                    help="train this many initialisations and keep the one the validation run favours")
     args = ap.parse_args(argv)
+    if args.runs > 1 and args.no_validate:
+        ap.error("--runs > 1 selects by the validation run; drop --no-validate")
     scene = warm_start_scene(args.scene)
-    t0 = time.time()
-    params, norm, hist = train(scene, TRAIN_SEEDS[: args.trajectories], args.steps, args.adam_per_step, args.batch,
-                               args.lr, log=lambda m: print(m, flush=True))
+    best = None
+    runs = []
+    for r in range(args.runs):
+        init = INIT_SEEDS[r % len(INIT_SEEDS)]
+        t0 = time.time()
+        params, norm, hist = train(scene, TRAIN_SEEDS[: args.trajectories], args.steps, args.adam_per_step,
+                                   args.batch, args.lr, init_seed=init, log=lambda m: print(m, flush=True))
+        seconds = time.time() - t0
+        val = None if args.no_validate else validate(args.scene, params, norm)
+        runs.append({"init_seed": init, "final_loss": float(hist[-1, 2]) if len(hist) else None,
+                     "seconds": seconds, "validation": val})
+        print(json.dumps(runs[-1]), flush=True)
+        key = (val["mean_iterations"], val["mean_density_error"]) if val else (0.0, 0.0)
+        if best is None or key < best[0]:
+            best = (key, params, norm, runs[-1])
+    _, params, norm, chosen = best
     meta = {"scene": scene.name, "lambda_epsilon": scene.lambda_epsilon, "solve_steps": scene.solve_steps,
             "trajectories": args.trajectories, "steps": args.steps, "batch": args.batch, "lr": args.lr,
             "adam_per_step": args.adam_per_step, "seeds": list(TRAIN_SEEDS[: args.trajectories]),
-            "final_loss": float(hist[-1, 2]) if len(hist) else None, "seconds": time.time() - t0}
+            "init_seed": chosen["init_seed"], "final_loss": chosen["final_loss"], "seconds": chosen["seconds"]}
+    if chosen["validation"]:
+        meta["validation"] = chosen["validation"]
+    if args.runs > 1:
+        meta["selection"] = {"criterion": "fewest mean iterations on the validation seed, then lower error",
+                             "runs": runs}
     save_model(args.out, params, norm, meta)
     print(json.dumps(meta), flush=True)
     return 0

@@ -26,3 +26,15 @@ def test_oracle_gelu_is_the_erf_form():
     from math import erf, sqrt
     ref = np.array([0.5 * x * (1 + erf(x / sqrt(2))) for x in xs])
     assert np.allclose(M.gelu(xs), ref, rtol=0, atol=1e-15)
+
+
+def test_training_cli_selection_needs_the_validation_run():
+    """--runs R keeps the network the held-out validation run favours, so it
+    cannot be combined with --no-validate (rejected before any device work);
+    the validation seed is neither a training seed nor the comparison's."""
+    import pytest
+    from pbf_b200 import learn
+    with pytest.raises(SystemExit):
+        learn.main(["--runs", "2", "--no-validate"])
+    assert learn.VALIDATION_SEED not in learn.TRAIN_SEEDS and learn.VALIDATION_SEED != 4242
+    assert len(set(learn.INIT_SEEDS)) == len(learn.INIT_SEEDS)
