@@ -67,6 +67,43 @@ def dist_env():
         os.environ.get("LOCAL_RANK", "0"))
 
 
+class RankGroup:
+    """The ranks of one run, one process per GPU (torchrun sets RANK,
+    WORLD_SIZE, MASTER_ADDR/PORT): a barrier and the max of a value over the
+    ranks (device times are reported as the max over ranks).  The bench uses
+    NCCL on CUDA tensors; the same calls run on gloo with CPU tensors.  A
+    single rank makes no process group and every call is a no-op.  The group
+    has a short timeout, so that ranks waiting on a missing one end with an
+    error."""
+
+    def __init__(self, world: int, backend: str = "nccl", device: str = "cuda", timeout_s: float = 120.0):
+        self.world = world
+        self.device = device
+        self.dist = None
+        if world > 1:
+            import datetime
+            import torch.distributed as dist
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+            self.dist = dist
+
+    def barrier(self) -> None:
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def max(self, v: float) -> float:
+        if self.dist is None:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self) -> None:
+        if self.dist is not None:
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -390,12 +427,7 @@ def main():
     import numpy as np
     import torch
     torch.cuda.set_device(local)
-    pg = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-        pg = dist
+    ranks = RankGroup(world)
 
     from pbf_b200 import Particles
     p = scene.params()
@@ -405,17 +437,11 @@ def main():
     stream = torch.cuda.ExternalStream(g.stream_handle())
 
     def barrier():
-        if pg is not None:
-            pg.barrier()
+        ranks.barrier()
         torch.cuda.synchronize()
         g.sync()
 
-    def max_over_ranks(v: float) -> float:
-        if pg is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
+    max_over_ranks = ranks.max
 
     # warm-up: 3 steps, the autotuner (times each launch shape on 3 steps from
     # this state, then restores it), then W steps (the last captures the graph)
@@ -509,8 +535,7 @@ def main():
             cpu = run_reference_cpu(scene, 100, 1, args.cpu_seconds)
         except Exception as e:  # reported, never fatal for the GPU line
             cpu = {"error": str(e)}
-    if pg is not None:
-        pg.barrier()
+    ranks.barrier()
 
     if rank == 0:
         value = scene.n * K * world / t_dev
@@ -547,8 +572,7 @@ def main():
         }
         print(json.dumps(line), flush=True)
     g.close()
-    if pg is not None:
-        pg.destroy_process_group()
+    ranks.close()
     return 0
 
 
