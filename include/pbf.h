@@ -368,6 +368,14 @@ int pbf_mlp_gradients(pbf_ctx* ctx, const float* features, const float* targets,
                       float* loss);
 /* Network output for n host samples of normalised features. */
 int pbf_mlp_predict(pbf_ctx* ctx, const float* features, size_t n, float* y);
+/* Self-test of the network kernel's failure path; no counterpart in the
+ * reference.  One 128-row tile is launched with its tensor-core MMAs and
+ * their completion signal left out, so every bounded wait of the kernel on
+ * that signal gives up.  The kernel then raises PBF_FLAG_WAIT_TIMEOUT in
+ * *flags (its own status word, not the context's error flags), frees its
+ * tensor memory and returns; the context stays usable.  Needs a network
+ * (pbf_mlp_init or pbf_mlp_set) and a capacity of at least 278 particles. */
+int pbf_selftest_mlp_wait_timeout(pbf_ctx* ctx, uint32_t* flags);
 
 /* ---- neighbor search that allocates nothing ----
  * No counterpart in the reference.  For callers that may not allocate device

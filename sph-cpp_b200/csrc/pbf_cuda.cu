@@ -1084,7 +1084,10 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) kl_features(Dev P, F
 // WARM: features from featb (column 15 flags the reference-ordered nudge
 // path), lambda = the output kept between l1 and kWarmMaxGain * l1.  PREDICT: normalised float features, y = the output.  A wait that
 // gives up raises PBF_FLAG_WAIT_TIMEOUT; every CTA frees its TMEM.
-template <bool WARM>
+// NO_ARRIVE (the failure-path self-test only): the MMAs and their commits
+// are left out, so nothing arrives on the barrier and every bounded wait runs
+// out; nothing asynchronous is in flight when the kernel gives up.
+template <bool WARM, bool NO_ARRIVE = false>
 __global__ void __launch_bounds__(pbf::tc::kThreads, 6) kl_mlp_tc(pbf::MlpDev M, int n,
                                                               const __nv_bfloat16* __restrict__ featb,
                                                               const float* __restrict__ feats, float4* xl,
@@ -1155,8 +1158,10 @@ __global__ void __launch_bounds__(pbf::tc::kThreads, 6) kl_mlp_tc(pbf::MlpDev M,
     __syncthreads();
     if (tid == 0) {
       T::fence_after_sync();
-      T::mma_bf16(tmem, T::smem_desc(a1, 128, 256), dB1, T::kIdescM128N64, 0u);
-      T::mma_commit(bar);
+      if (!NO_ARRIVE) {
+        T::mma_bf16(tmem, T::smem_desc(a1, 128, 256), dB1, T::kIdescM128N64, 0u);
+        T::mma_commit(bar);
+      }
     }
     if (!T::bar_wait(bar, phase)) fail = 1;
     phase ^= 1u;
@@ -1183,11 +1188,13 @@ __global__ void __launch_bounds__(pbf::tc::kThreads, 6) kl_mlp_tc(pbf::MlpDev M,
     __syncthreads();  // every layer-1 accumulator read before layer 2 overwrites them
     if (tid == 0) {
       T::fence_after_sync();
+      if (!NO_ARRIVE) {
 #pragma unroll
-      for (int ks = 0; ks < 4; ++ks)
-        T::mma_bf16(tmem, T::smem_desc(a2 + 256u * ks, 128, 1024), T::smem_desc(b2 + 256u * ks, 128, 1024),
-                    T::kIdescM128N64, ks > 0 ? 1u : 0u);
-      T::mma_commit(bar);
+        for (int ks = 0; ks < 4; ++ks)
+          T::mma_bf16(tmem, T::smem_desc(a2 + 256u * ks, 128, 1024), T::smem_desc(b2 + 256u * ks, 128, 1024),
+                      T::kIdescM128N64, ks > 0 ? 1u : 0u);
+        T::mma_commit(bar);
+      }
     }
     if (!T::bar_wait(bar, phase)) fail = 1;
     phase ^= 1u;
@@ -3494,6 +3501,25 @@ int pbf_mlp_predict(pbf_ctx* ctx, const float* features, size_t n, float* y) {
   // the context's error word (the step's flags are kept: a timeout raised by
   // an earlier step fails this call too, the context's tensor-core path has failed)
   if (err & PBF_FLAG_WAIT_TIMEOUT) return fail(ctx, PBF_ERR_DEVICE, "mlp_predict: a tensor-core wait timed out");
+  return PBF_OK;
+}
+
+int pbf_selftest_mlp_wait_timeout(pbf_ctx* ctx, uint32_t* flags) {
+  if (!ctx || !flags) return PBF_ERR_ARG;
+  if (!ctx->mlp_ready) return fail(ctx, PBF_ERR_STATE, "no network: call pbf_mlp_init or pbf_mlp_set");
+  const int rows = pbf::tc::kRows;  // one tile, one CTA
+  const size_t need = (size_t)rows * (pbf::kMlpIn + 1) + 1;
+  if (need > 6 * ctx->capacity)
+    return fail(ctx, PBF_ERR_CAPACITY, "the self-test needs a context of at least %zu particles", need / 6 + 1);
+  float* df = ctx->stage;
+  float* dy = ctx->stage + (size_t)rows * pbf::kMlpIn;
+  uint32_t* status = reinterpret_cast<uint32_t*>(dy + rows);
+  CK(cudaMemsetAsync(ctx->stage, 0, need * sizeof(float), ctx->stream));
+  kl_mlp_tc<false, true><<<1, pbf::tc::kThreads, 0, ctx->stream>>>(mlp_dev(ctx), rows, nullptr, df, nullptr, nullptr,
+                                                                   nullptr, dy, status);
+  if (int rc = check_launch(ctx, "selftest_mlp_wait_timeout")) return rc;
+  CK(cudaMemcpyAsync(flags, status, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
   return PBF_OK;
 }
 

@@ -317,6 +317,13 @@ class Particles:
         self._check(self._lib.pbf_mlp_predict(self._ctx, _ptr(f), f.shape[0], _ptr(y)), "mlp_predict")
         return y
 
+    def selftest_mlp_wait_timeout(self) -> int:
+        """Run the network kernel with nothing arriving on its completion
+        barrier (pbf_selftest_mlp_wait_timeout); returns the flags it raised."""
+        out = C.c_uint32(0)
+        self._check(self._lib.pbf_selftest_mlp_wait_timeout(self._ctx, C.byref(out)), "selftest_mlp_wait_timeout")
+        return int(out.value)
+
     # -- instrumentation --
     def set_timing(self, on: bool) -> None:
         self._check(self._lib.pbf_set_timing(self._ctx, int(on)), "set_timing")

@@ -19,6 +19,7 @@ PBF_ERR_IO = -8
 
 PBF_FLAG_KEY_RANGE = 1
 PBF_FLAG_NONFINITE = 2
+PBF_FLAG_WAIT_TIMEOUT = 4
 
 ARRAY_POSITIONS = 0
 ARRAY_POSITION_STARS = 1
@@ -192,6 +193,7 @@ SIGNATURES = {
     "pbf_mlp_train": (_i, [_vp, _i, _i, C.c_float, C.c_uint64, _P(C.c_float)]),
     "pbf_mlp_gradients": (_i, [_vp, _vp, _vp, _sz, _vp, _P(C.c_float)]),
     "pbf_mlp_predict": (_i, [_vp, _vp, _sz, _vp]),
+    "pbf_selftest_mlp_wait_timeout": (_i, [_vp, _vp]),
 }
 
 _lib = None

@@ -126,3 +126,25 @@ def test_residual_controlled_iterations(trained_8k):
             if st["solver_iterations"] < 6:
                 assert st["solver_residual"] <= tol
                 assert st["mean_density_error"] <= tol * 1.02 + 1e-6
+
+
+def test_network_kernel_gives_up_a_wait_and_the_context_stays_usable():
+    """Failure detection without a GPU fault: the network kernel launched with
+    nothing arriving on its completion barrier gives up its bounded waits,
+    raises the timeout flag in its own status word and frees its tensor
+    memory; the context's error flags stay clear and the next network call
+    still matches the float64 oracle."""
+    g = _ctx_with_net()
+    flags = g.selftest_mlp_wait_timeout()
+    assert flags & _abi.PBF_FLAG_WAIT_TIMEOUT
+    params, _ = g.mlp_get()
+    x = np.random.default_rng(1).normal(0, 1, (600, _abi.MLP_FEATURES)).astype(np.float32)
+    y = g.mlp_predict(x)
+    ref, _ = MO.forward(params.astype(np.float64), x.astype(np.float64))
+    assert np.abs(y - ref).max() <= Y_TOL * max(np.abs(ref).max(), 0.1)
+    g.upload(warm_start_scene("dam_2k").positions())
+    g.step(1)
+    assert g.stats()["error_flags"] == 0
+    g2 = Particles(warm_start_scene("dam_2k").params(), 4096)
+    with pytest.raises(RuntimeError, match="no network"):
+        g2.selftest_mlp_wait_timeout()
