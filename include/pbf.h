@@ -315,7 +315,7 @@ enum {
   PBF_TUNE_APPLY_VORTICITY = 4,
   PBF_TUNE_FAMILIES = 5
 };
-#define PBF_TUNE_CANDIDATES 5  /* (lanes, block, staged) = (4,128,0) (4,256,0) (8,128,0) (8,256,0) (4,128,1) */
+#define PBF_TUNE_CANDIDATES 7  /* (lanes, block, staged) = (4,128,0) (4,256,0) (8,128,0) (8,256,0) (2,128,0) (2,256,0) (4,128,1) */
 typedef struct {
   int lanes[PBF_TUNE_FAMILIES];
   int block[PBF_TUNE_FAMILIES];

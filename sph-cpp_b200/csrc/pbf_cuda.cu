@@ -2142,13 +2142,15 @@ template <class Fn>
 void with_lanes(int lanes, Fn&& fn) {
   if (lanes == 4)
     fn(std::integral_constant<int, 4>{});
+  else if (lanes == 2)
+    fn(std::integral_constant<int, 2>{});
   else
     fn(std::integral_constant<int, 8>{});
 }
 
 bool shape_ok(int lanes, int block, int staged) {
   if (staged) return staged == 1 && lanes == 4 && block == kStageThreads;
-  return (lanes == 4 || lanes == 8) && (block == 128 || block == 256);
+  return (lanes == 2 || lanes == 4 || lanes == 8) && (block == 128 || block == 256);
 }
 
 bool any_staged(const pbf_ctx* ctx) {
@@ -3579,9 +3581,9 @@ int pbf_set_tuning(pbf_ctx* ctx, const pbf_tuning* t) {
 }
 
 namespace {
-constexpr int kCandLanes[PBF_TUNE_CANDIDATES] = {4, 4, 8, 8, 4};
-constexpr int kCandBlock[PBF_TUNE_CANDIDATES] = {128, 256, 128, 256, kStageThreads};
-constexpr int kCandStaged[PBF_TUNE_CANDIDATES] = {0, 0, 0, 0, 1};
+constexpr int kCandLanes[PBF_TUNE_CANDIDATES] = {4, 4, 8, 8, 2, 2, 4};
+constexpr int kCandBlock[PBF_TUNE_CANDIDATES] = {128, 256, 128, 256, 128, 256, kStageThreads};
+constexpr int kCandStaged[PBF_TUNE_CANDIDATES] = {0, 0, 0, 0, 0, 0, 1};
 
 int family_of(const char* name) {
   if (!std::strcmp(name, "density_lambda") || !std::strcmp(name, "residual_check")) return PBF_TUNE_DENSITY;

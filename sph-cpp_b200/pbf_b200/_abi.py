@@ -34,7 +34,7 @@ MLP_NORM = 25
 
 TUNE_FAMILIES = ("density", "delta_p", "viscosity", "vorticity", "apply_vorticity")
 # (lanes per particle, threads per block, staged in shared memory)
-TUNE_CANDIDATES = ((4, 128, 0), (4, 256, 0), (8, 128, 0), (8, 256, 0), (4, 128, 1))
+TUNE_CANDIDATES = ((4, 128, 0), (4, 256, 0), (8, 128, 0), (8, 256, 0), (2, 128, 0), (2, 256, 0), (4, 128, 1))
 
 NOALLOC_MAX_PARTICLES = 65536
 NOALLOC_MAX_BINS = 262144
