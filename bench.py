@@ -260,7 +260,9 @@ def solver_run(scene, steps: int, warmup: int, params=None, norm=None, autotune:
         tuning = None
         for i in range(warmup):
             if autotune and i == warmup // 2:
-                tuning, _ = g.autotune(2)
+                # 6 timed steps per candidate: the learned step's cost varies with the
+                # iterations each step needs, and 2 steps picked shapes 2-4% slower
+                tuning, _ = g.autotune(6)
             g.step(1)
         g.sync()
         e0 = torch.cuda.Event(enable_timing=True)
