@@ -846,6 +846,7 @@ struct LearnIO {
   int first;              // first Jacobi iteration of the step
   float tol;              // kDlCheck: residual tolerance
   int final_check;        // kDlCheck: the step's last allowed check (records, never extends)
+  pbf::SolveLoop loop;    // kDlCheck inside the graph's conditional loop
 };
 
 // The sums a density + lambda gather produces for one particle, combined
@@ -943,14 +944,18 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) kf_density_lambda(De
                                                             const int32_t* __restrict__ cnt,
                                                             const float4* __restrict__ pst, float4* xl, float4* vel,
                                                             float* lam, uint32_t* nudge, LearnIO io) {
-  if (MODE == kDlCheck && io.state->done) return;
+  if (MODE == kDlCheck && io.state->done) {
+    // a check after the step converged: it ends the loop it runs in
+    if (io.loop.use && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(io.loop.cond, 0u);
+    return;
+  }
   const int tiles = pbf::tiles_of<GL>(n);
   float err = 0.0f;
   for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x)
     density_lambda_tile<MODE, GL>(tile, P, F, n, stride, nbr, cnt, pst, xl, vel, lam, nudge, io, err);
   if (MODE == kDlCheck) {
     pbf::block_partial<kBlock>(err, io.partials + blockIdx.x);
-    pbf::decide_if_last<kBlock>(io.state, io.partials, n, io.tol, io.final_check);
+    pbf::decide_if_last<kBlock>(io.state, io.partials, n, io.tol, io.final_check, io.loop);
   }
 }
 
@@ -998,7 +1003,10 @@ __global__ void __launch_bounds__(kStageThreads) ks_density_lambda(Dev P, Fast F
                                                                   float4* vel, float* lam, uint32_t* nudge, LearnIO io,
                                                                   TileIO T) {
   __shared__ float4 stage[kStageMax + 1];
-  if (MODE == kDlCheck && io.state->done) return;
+  if (MODE == kDlCheck && io.state->done) {
+    if (io.loop.use && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(io.loop.cond, 0u);
+    return;
+  }
   const int tiles = (n + kTile - 1) / kTile;
   float err = 0.0f;
   for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
@@ -1012,7 +1020,7 @@ __global__ void __launch_bounds__(kStageThreads) ks_density_lambda(Dev P, Fast F
   }
   if (MODE == kDlCheck) {
     pbf::block_partial<kStageThreads>(err, io.partials + blockIdx.x);
-    pbf::decide_if_last<kStageThreads>(io.state, io.partials, n, io.tol, io.final_check);
+    pbf::decide_if_last<kStageThreads>(io.state, io.partials, n, io.tol, io.final_check, io.loop);
   }
 }
 
@@ -1859,6 +1867,7 @@ struct pbf_ctx {
   size_t lstride_cap = 0;  // list row stride the list buffer was allocated for
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t side = nullptr;  // captures the body of the learned solver's conditional loop
   bool lists_valid = false;
 
   float4 *posH = nullptr, *pstH = nullptr, *velH = nullptr, *scrH = nullptr;
@@ -2384,31 +2393,75 @@ void launch_learned_solve(pbf_ctx* ctx) {
           P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS, ctx->posS, ctx->velS, ctx->state, nullptr);
     });
   }
-  for (int r = 1; r <= iters; ++r) {
-    const bool final_check = r == iters;
-    io.final_check = final_check ? 1 : 0;
+  // a residual check (final: the step's last, which only records) and a
+  // plain position update, each skipping itself once the step is done
+  auto check = [&](cudaStream_t cs, const LearnIO& cio) {
     if (T.staged[PBF_TUNE_DENSITY]) {
       Launch L(ctx, "residual_check");
-      ks_density_lambda<kDlCheck><<<gpc, kStageThreads, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl,
-                                                                ctx->velS, ctx->lamH, ctx->nudge, io, tio);
+      ks_density_lambda<kDlCheck><<<gpc, kStageThreads, 0, cs>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS,
+                                                                 ctx->xl, ctx->velS, ctx->lamH, ctx->nudge, cio, tio);
     } else {
       with_lanes(T.lanes[PBF_TUNE_DENSITY], [&](auto gl) {
         Launch L(ctx, "residual_check");
-        kf_density_lambda<kDlCheck, decltype(gl)::value><<<gpc, bd, 0, s>>>(
-            P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl, ctx->velS, ctx->lamH, ctx->nudge, io);
+        kf_density_lambda<kDlCheck, decltype(gl)::value><<<gpc, bd, 0, cs>>>(
+            P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl, ctx->velS, ctx->lamH, ctx->nudge, cio);
       });
     }
-    if (final_check) break;
+  };
+  auto update = [&](cudaStream_t cs) {
     if (T.staged[PBF_TUNE_DELTA_P]) {
       Launch L(ctx, "dp_update");
-      ks_dp_update<SCORR, false, true><<<gpd, kStageThreads, 0, s>>>(
+      ks_dp_update<SCORR, false, true><<<gpd, kStageThreads, 0, cs>>>(
           P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS, ctx->posS, ctx->velS, ctx->state, ctx->lamsumH, tio);
     } else {
       with_lanes(T.lanes[PBF_TUNE_DELTA_P], [&](auto gl) {
         Launch L(ctx, "dp_update");
-        kf_dp_update<SCORR, false, true, decltype(gl)::value><<<gpd, bp, 0, s>>>(
+        kf_dp_update<SCORR, false, true, decltype(gl)::value><<<gpd, bp, 0, cs>>>(
             P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS, ctx->posS, ctx->velS, ctx->state, ctx->lamsumH);
       });
+    }
+  };
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(s, &cap);
+  if (cap == cudaStreamCaptureStatusActive && iters > 1) {
+    // Captured into the step's graph: the plain iterations become a WHILE
+    // node whose body is (check, update) and whose condition the check sets
+    // (SolveLoop), so a converged step launches nothing more; the final
+    // check follows the node.  Errors here invalidate the capture, which the
+    // caller reports.
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cudaStreamGetCaptureInfo(s, &cap, nullptr, &g, &deps, &ndeps);
+    cudaGraphConditionalHandle h = 0;
+    cudaGraphConditionalHandleCreate(&h, g, 1u, cudaGraphCondAssignDefault);
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    if (cudaGraphAddNode(&node, g, deps, ndeps, &cp) == cudaSuccess) {
+      cudaGraph_t body = cp.conditional.phGraph_out[0];
+      cudaStreamBeginCaptureToGraph(ctx->side, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+      LearnIO lio = io;
+      lio.final_check = 0;
+      lio.loop = pbf::SolveLoop{h, 1, iters};
+      check(ctx->side, lio);
+      update(ctx->side);
+      cudaStreamEndCapture(ctx->side, &body);
+      cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
+    }
+    LearnIO fio = io;
+    fio.final_check = 1;
+    check(s, fio);
+  } else {
+    for (int r = 1; r <= iters; ++r) {
+      const bool final_check = r == iters;
+      io.final_check = final_check ? 1 : 0;
+      check(s, io);
+      if (final_check) break;
+      update(s);
     }
   }
   Launch L(ctx, "update_velocities");
@@ -2606,7 +2659,9 @@ void launch_step(pbf_ctx* ctx) {
 }
 
 int launches_per_step(const pbf_ctx* ctx) {
-  // kernels only (the memsets are not): ext/predict/hash + 3 scan + radix
+  // kernels only (the memsets are not), as launched eagerly (a captured
+  // learned step runs its plain iterations in a conditional graph node and
+  // launches fewer once converged): ext/predict/hash + 3 scan + radix
   // passes x (histogram, 3 scan, scatter) + reorder + runs + fill + K x
   // (density/lambda, [exact: lambda fix-up], delta-p) + (K==0: velocity)
   // + 2 if gamma + 4 (visc, vort, apply, visc)
@@ -2674,7 +2729,8 @@ static int create_ctx(const pbf_params* p, size_t capacity, const pbf_scene* sce
     ctx->partials_cap = ctx->sms * per_sm;
     if ((rc = update_shapes(ctx))) return bail(rc);
   }
-  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking) != cudaSuccess) {
     fail(ctx, PBF_ERR_CUDA, "cudaStreamCreate failed");
     return bail(PBF_ERR_CUDA);
   }
@@ -2752,6 +2808,7 @@ void pbf_destroy(pbf_ctx* ctx) {
     cudaEventDestroy(m.stop);
   }
   for (void* p : ctx->allocations) cudaFree(p);
+  if (ctx->side) cudaStreamDestroy(ctx->side);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }

@@ -277,7 +277,17 @@ struct SolveState {
   uint32_t done;        // residual at or below the tolerance: the rest of the step's iterations skip
   uint32_t iterations;  // Jacobi iterations applied this step
   uint32_t ticket;      // blocks of the running check that have written their partial sum
-  uint32_t pad;
+  uint32_t loops;       // checks run inside the graph's conditional loop this step
+};
+
+// The graph's conditional loop around the learned solver's plain iterations
+// (a WHILE node whose body is one residual check and one position update;
+// the check ends the loop).  use = 0: no loop (eager launches, or the check
+// after the loop).
+struct SolveLoop {
+  cudaGraphConditionalHandle cond;
+  int use;
+  int iters;  // max_iterations: the loop runs at most iters - 1 times
 };
 
 // Sum of v over the block (every thread calls it; blockDim.x a multiple of 32,
@@ -306,7 +316,7 @@ __device__ __forceinline__ void block_partial(float v, double* out) {
 // check of a step only records the residual).
 template <int THREADS>
 __device__ __forceinline__ void decide_if_last(SolveState* st, const double* partials, int n, float tol,
-                                               int final_check) {
+                                               int final_check, SolveLoop loop) {
   __shared__ unsigned last;
   __shared__ double red[THREADS];
   if (threadIdx.x == 0) {
@@ -330,6 +340,14 @@ __device__ __forceinline__ void decide_if_last(SolveState* st, const double* par
   st->ticket = 0u;
   if (mean <= (double)tol) st->done = 1u;
   else if (!final_check) st->iterations += 1u;
+  if (loop.use) {
+    // One more pass of the loop only while the step is not done and another
+    // plain iteration is allowed; `loops` bounds the loop whatever the
+    // residuals do.
+    st->loops += 1u;
+    const bool more = !st->done && st->iterations + 1u < (uint32_t)loop.iters && st->loops < (uint32_t)loop.iters;
+    cudaGraphSetConditional(loop.cond, more ? 1u : 0u);
+  }
 }
 
 }  // namespace pbf

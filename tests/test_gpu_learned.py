@@ -148,3 +148,41 @@ def test_network_kernel_gives_up_a_wait_and_the_context_stays_usable():
     g2 = Particles(warm_start_scene("dam_2k").params(), 4096)
     with pytest.raises(RuntimeError, match="no network"):
         g2.selftest_mlp_wait_timeout()
+
+
+@pytest.mark.parametrize("tol", [1e-4, 0.005])
+def test_captured_iteration_loop_matches_eager_launches(tol):
+    """In a captured step the learned solver's plain iterations are a WHILE
+    node of the graph that the residual check ends; eager launches (per-kernel
+    timing on) run the same iterations as a loop of launches that skip
+    themselves.  Both give the same positions, velocities and iteration
+    counts, bit for bit, with one step or four steps per graph.  Once the dam
+    compresses, tol 1e-4 is never reached: those steps run the loop body three
+    times and leave it at the iteration cap (4); at tol 0.005 the check inside
+    the loop ends it."""
+    from pbf_b200.learn import DEFAULT_MODEL, load_model
+    params, norm, _ = load_model(DEFAULT_MODEL)
+    sc = warm_start_scene("dam_8k", solver=1, residual_tol=tol, max_iterations=4)
+    runs = {}
+    for mode in ("eager", "graph1", "graph4"):
+        g = Particles(sc.params(), sc.n)
+        g.mlp_set(params, norm)
+        g.upload(sc.positions())
+        g.set_timing(mode == "eager")
+        its = []
+        for k in range(18):  # 72 steps, the iteration counts of every fourth
+            if mode == "graph4":
+                g.step(4)
+            else:
+                for _ in range(4):
+                    g.step(1)
+            its.append(g.stats()["solver_iterations"])
+        runs[mode] = (g.positions(), g.velocities(), its)
+        assert g.stats()["error_flags"] == 0
+    x, v, its = runs["eager"]
+    if tol < 1e-3:  # the first steps (a falling lattice, no compression) converge at once
+        assert its.count(4) >= 12, its
+    for mode in ("graph1", "graph4"):
+        assert np.array_equal(runs[mode][0], x), mode
+        assert np.array_equal(runs[mode][1], v), mode
+        assert runs[mode][2] == its, (mode, runs[mode][2], its)
