@@ -299,7 +299,7 @@ int pbf_scene_stats(pbf_ctx* ctx, int scene, pbf_stats_t* out);
 /* ---- launch shapes of the fast-math gather kernels ----
  * No counterpart in the reference (its loops are OpenMP for_each_index).
  * Each family of gather kernels runs with `lanes` threads per particle
- * walking one neighbor list together (4 or 8) in blocks of `block` threads
+ * walking one neighbor list together (2, 4 or 8) in blocks of `block` threads
  * (128 or 256), either reading the neighbours' records from global memory or,
  * `staged` (4 lanes, 128 threads only), from shared memory: each block copies
  * the neighbour bins of its 32-particle tile there first and walks 16-bit

@@ -3630,7 +3630,7 @@ int pbf_set_tuning(pbf_ctx* ctx, const pbf_tuning* t) {
   for (int f = 0; f < PBF_TUNE_FAMILIES; ++f)
     if (!shape_ok(t->lanes[f], t->block[f], t->staged[f]))
       return fail(ctx, PBF_ERR_ARG, "gather family %d: %d lanes x %d threads%s is not a supported shape "
-                  "(lanes 4 or 8, block 128 or 256; staged: 4 x 128)", f, t->lanes[f], t->block[f],
+                  "(lanes 2, 4 or 8, block 128 or 256; staged: 4 x 128)", f, t->lanes[f], t->block[f],
                   t->staged[f] ? " staged" : "");
   ctx->tune = *t;
   drop_graphs(ctx);

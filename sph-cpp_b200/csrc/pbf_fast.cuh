@@ -9,7 +9,7 @@
 //  - branch-free: clamping (h^2 - d^2) and (h - r) at 0 zeroes the pairs with
 //    h < r < s, which stay in the lists because x* moves during the iterations;
 //  - kernel constants (norms, 1/rho0, mass) folded on the host;
-//  - GL = 4 or 8 lanes per particle (the launch shape the autotuner picks)
+//  - GL = 2, 4 or 8 lanes per particle (the launch shape the autotuner picks)
 //    walk its row-major, padded list together (see Group, gwalk1) and
 //    combine their partial sums with shuffles.
 // A particle sitting exactly on a neighbour (d^2 < 1e-16, the reference's
@@ -48,7 +48,7 @@ inline Fast make_fast(const Dev& d) {
   return f;
 }
 
-// Lane groups: GL consecutive threads share one particle (GL = 4 or 8, the
+// Lane groups: GL consecutive threads share one particle (GL = 2, 4 or 8, the
 // launch shape the autotuner picks per kernel family; kGL is the default).
 // Lane l walks entries l, l + GL, ... of the particle's row-major list, so one
 // warp-wide load touches GL consecutive entries of each of 32/GL lists, and
