@@ -186,3 +186,21 @@ def test_captured_iteration_loop_matches_eager_launches(tol):
         assert np.array_equal(runs[mode][0], x), mode
         assert np.array_equal(runs[mode][1], v), mode
         assert runs[mode][2] == its, (mode, runs[mode][2], its)
+
+
+def test_timing_counts_every_learned_kernel():
+    """Eager learned steps (per-kernel timing on) launch exactly what
+    launches_per_step reports: the features and the network, then
+    max_iterations residual checks and as many position updates, each
+    skipping itself once the step has converged."""
+    sc = warm_start_scene("dam_2k", solver=1, max_iterations=5)
+    g = Particles(sc.params(), sc.n)
+    g.mlp_init(3)
+    g.upload(sc.positions())
+    g.set_timing(True)
+    g.step(2)
+    t = g.kernel_times()
+    g.set_timing(False)
+    assert sum(v["launches"] for v in t.values()) == 2 * g.launches_per_step()
+    assert t["warm_mlp"]["launches"] == 2 and t["warm_features"]["launches"] == 2
+    assert t["residual_check"]["launches"] == 2 * 5 and t["dp_update"]["launches"] == 2 * 5
