@@ -204,3 +204,22 @@ def test_timing_counts_every_learned_kernel():
     assert sum(v["launches"] for v in t.values()) == 2 * g.launches_per_step()
     assert t["warm_mlp"]["launches"] == 2 and t["warm_features"]["launches"] == 2
     assert t["residual_check"]["launches"] == 2 * 5 and t["dp_update"]["launches"] == 2 * 5
+
+
+def test_hundred_learned_steps_in_one_graph():
+    """A hundred learned steps captured in one graph (a hundred conditional
+    loop nodes) give the same state as a hundred one-step graphs."""
+    from pbf_b200.learn import DEFAULT_MODEL, load_model
+    params, norm, _ = load_model(DEFAULT_MODEL)
+    sc = warm_start_scene("dam_2k", solver=1, residual_tol=0.005, max_iterations=4)
+    out = []
+    for per_graph in (100, 1):
+        g = Particles(sc.params(), sc.n)
+        g.mlp_set(params, norm)
+        g.upload(sc.positions())
+        for _ in range(100 // per_graph):
+            g.step(per_graph)
+        out.append((g.positions(), g.velocities(), g.stats()))
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    assert out[0][2]["solver_iterations"] == out[1][2]["solver_iterations"]
+    assert out[0][2]["error_flags"] == 0
