@@ -1093,8 +1093,9 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) kl_features(Dev P, F
 // operand) -> four M128 N64 K16 MMAs into the same columns -> layer-2
 // epilogue (bias, GELU, the dot with w3, the two halves added).
 // WARM: features from featb (column 15 flags the reference-ordered nudge
-// path), lambda = the output kept between l1 and kWarmMaxGain * l1.  PREDICT: normalised float features, y = the output.  A wait that
-// gives up raises PBF_FLAG_WAIT_TIMEOUT; every CTA frees its TMEM.
+// path), lambda = the output kept between l1 and kWarmMaxGain * l1.
+// PREDICT: normalised float features, y = the output.  A wait that gives up
+// raises PBF_FLAG_WAIT_TIMEOUT; every CTA frees its TMEM.
 // NO_ARRIVE (the failure-path self-test only): the MMAs and their commits
 // are left out, so nothing arrives on the barrier and every bounded wait runs
 // out; nothing asynchronous is in flight when the kernel gives up.
