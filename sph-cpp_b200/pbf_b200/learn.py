@@ -7,7 +7,7 @@ particle's features at its first Jacobi iteration and, as label, the sum of
 the lambdas the plain solver applied over its K iterations.  One Adam update
 on a batch drawn from that step follows each step.
 
-    python -m pbf_b200.learn --out model.npz [--scene dam_1m] [--trajectories 10] [--steps 200] [--runs 4]
+    python -m pbf_b200.learn --out model.npz [--scene dam_1m] [--trajectories 10] [--steps 200] [--runs 8]
 
 Training reduces its weight gradients with atomics, so two runs of the same
 recipe differ; on the 1M dam they have needed from 2.2 to 2.8 solver
