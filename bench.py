@@ -166,7 +166,7 @@ def kernel_bytes(name: str, n: int, nbar: float, K: int, nbins: int) -> float:
     per = {
         "ext_predict_hash": 16 + 16 + 16 + 16 + 4 + 4,           # x, v in; v, x*, key, rank out (+ histogram in L2)
         "scan_reduce": 4.0 * nbins / n,
-        "scan_partials": 0.0,
+        "scan_partials": 8.0 * nbins / n / 4096,                # one partial sum per scan tile of 4096 bins, read and written
         "scan_apply": 8.0 * nbins / n,
         "radix_hist": 4 + 2048.0 * 4 / 4096,                    # key in; per-tile digit counts out
         "radix_scan": 2048.0 * 4 / 4096,                        # digit counts (3 launches, per launch)
@@ -178,6 +178,7 @@ def kernel_bytes(name: str, n: int, nbar: float, K: int, nbins: int) -> float:
         "runs": 16 + 4,                                         # x* in (the previous slot's is a cache hit); run end out
         "fill_neighbors": 16 + 4 * nbar + 4 + 8.0 * nbins / n,  # own x*, list + count out, bin starts
         "density_lambda": 16 + L + 16 + 4 + 4,                  # x* in; list; (x*, lambda), rho, lambda out
+        "lambda_fixup": 16 + L + 16 + 4,                        # exact math after a nudge: x* in, list; (x*, lambda), lambda out
         "dp_update": 16 + L + 16 + (32.0 / K),                  # (x*, lambda) in; list; x* out; last: x in, v out
         "viscosity": 16 + 16 + L + 16,
         "vorticity": 16 + 16 + L + 16 + 16,
