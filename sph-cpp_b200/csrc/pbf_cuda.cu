@@ -1872,6 +1872,7 @@ struct pbf_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t side = nullptr;  // captures the body of the learned solver's conditional loop
+  bool capture_failed = false;  // a step's conditional loop could not be captured whole
   bool lists_valid = false;
 
   float4 *posH = nullptr, *pstH = nullptr, *velH = nullptr, *scrH = nullptr;
@@ -2431,31 +2432,38 @@ void launch_learned_solve(pbf_ctx* ctx) {
     // Captured into the step's graph: the plain iterations become a WHILE
     // node whose body is (check, update) and whose condition the check sets
     // (SolveLoop), so a converged step launches nothing more; the final
-    // check follows the node.  Errors here invalidate the capture, which the
-    // caller reports.
-    cudaGraph_t g = nullptr;
+    // check follows the node.  The node enters its loop on every graph launch
+    // and only the body's check ends it, so a node whose body was not
+    // captured whole must never run: any failure here marks the capture
+    // failed, and pbf_step discards the graph instead of launching it.
+    bool ok = false;
+    cudaGraph_t graph = nullptr;
     const cudaGraphNode_t* deps = nullptr;
     size_t ndeps = 0;
-    cudaStreamGetCaptureInfo(s, &cap, nullptr, &g, &deps, &ndeps);
     cudaGraphConditionalHandle h = 0;
-    cudaGraphConditionalHandleCreate(&h, g, 1u, cudaGraphCondAssignDefault);
     cudaGraphNodeParams cp = {};
     cp.type = cudaGraphNodeTypeConditional;
-    cp.conditional.handle = h;
     cp.conditional.type = cudaGraphCondTypeWhile;
     cp.conditional.size = 1;
     cudaGraphNode_t node = nullptr;
-    if (cudaGraphAddNode(&node, g, deps, ndeps, &cp) == cudaSuccess) {
+    if (cudaStreamGetCaptureInfo(s, &cap, nullptr, &graph, &deps, &ndeps) == cudaSuccess &&
+        cudaGraphConditionalHandleCreate(&h, graph, 1u, cudaGraphCondAssignDefault) == cudaSuccess &&
+        (cp.conditional.handle = h, cudaGraphAddNode(&node, graph, deps, ndeps, &cp) == cudaSuccess)) {
       cudaGraph_t body = cp.conditional.phGraph_out[0];
-      cudaStreamBeginCaptureToGraph(ctx->side, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
-      LearnIO lio = io;
-      lio.final_check = 0;
-      lio.loop = pbf::SolveLoop{h, 1, iters};
-      check(ctx->side, lio);
-      update(ctx->side);
-      cudaStreamEndCapture(ctx->side, &body);
-      cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
+      if (cudaStreamBeginCaptureToGraph(ctx->side, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
+          cudaSuccess) {
+        LearnIO lio = io;
+        lio.final_check = 0;
+        lio.loop = pbf::SolveLoop{h, 1, iters};
+        check(ctx->side, lio);
+        update(ctx->side);
+        const bool launched = cudaPeekAtLastError() == cudaSuccess;
+        const bool ended = cudaStreamEndCapture(ctx->side, &body) == cudaSuccess;
+        ok = launched && ended &&
+             cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies) == cudaSuccess;
+      }
     }
+    if (!ok) ctx->capture_failed = true;
     LearnIO fio = io;
     fio.final_check = 1;
     check(s, fio);
@@ -3284,12 +3292,16 @@ int pbf_step(pbf_ctx* ctx, int nsteps) {
   auto it = ctx->graphs.find(nsteps);
   if (it == ctx->graphs.end()) {
     cudaGraph_t graph = nullptr;
+    ctx->capture_failed = false;
     CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     for (int i = 0; i < nsteps; ++i) launch_step(ctx);
     cudaError_t le = cudaGetLastError();
     cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
-    if (le != cudaSuccess || ce != cudaSuccess) {
+    if (le != cudaSuccess || ce != cudaSuccess || ctx->capture_failed) {
       if (graph) cudaGraphDestroy(graph);
+      const bool loop = ctx->capture_failed;
+      ctx->capture_failed = false;
+      if (loop) return fail(ctx, PBF_ERR_CUDA, "graph capture of the learned solver's iteration loop failed");
       return fail(ctx, PBF_ERR_CUDA, "graph capture failed: %s / %s", cudaGetErrorString(le),
                   cudaGetErrorString(ce));
     }
