@@ -20,12 +20,17 @@ ROOT = PKG.parent
 LIB = PKG / "lib" / "libpbf_b200.so"
 APP = PKG / "lib" / "pbf_run"
 ORACLE_LIB = ROOT / "oracle" / "_build" / "libpbf_oracle.so"
+# The reference's source tree: PBF_REFERENCE_ROOT, else the read-only checkout
+# this build script is run beside; absent on machines that only use the
+# prebuilt oracle/_ref libraries.
 REF_SOURCES = Path(os.environ.get("PBF_REFERENCE_ROOT", "/root/reference"))
 
 NVCC_ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUDA_SOURCES = ["csrc/pbf_cuda.cu"]
 HOST_SOURCES = ["csrc/pbf_host.cpp"]
-DEPS = ["csrc/pbf_kernels.cuh", "csrc/pbf_fast.cuh", "csrc/pbf_mlp.cuh", "csrc/pbf_learn.cuh", "csrc/pbf_internal.h", "../include/pbf.h"]
+# every header the library's sources include: all of csrc/ and include/
+DEPS = sorted(str(f.relative_to(PKG)) for f in (PKG / "csrc").glob("*") if f.suffix in (".cuh", ".h")) + \
+    ["../include/pbf.h"]
 
 
 def _nvcc() -> str:

