@@ -16,14 +16,17 @@ JSON line on rank 0.
                steps on the library's stream), against the measured HBM copy
                bandwidth
   cpu_baseline the reference's own OpenMP build (oracle/_ref) on this host's
-               cores, a bounded sample of the same workload
+               cores, a bounded sample of the same workload, and the same on
+               one thread
   tuning       the launch shapes (lanes per particle, threads per block) of the
                gather kernel families the library's autotuner picked during
                the warm-up (pbf_autotune; --no-autotune keeps the defaults)
 Multi-GPU: the path does not shard in this build (replicas only): every rank
 runs its own full scene on its own GPU; value sums the ranks' particle-steps
 over the slowest rank's time.
-`--impl reference` times the reference's CPU build instead (rank 0 only).
+`--impl reference` times the reference's CPU build instead (rank 0 only), on
+the workload built from that build and numpy alone (oracle/ref_scene.py): its
+process never loads the product's library, and its `config` is the GPU arm's.
 """
 from __future__ import annotations
 
@@ -210,36 +213,62 @@ def ncu_traffic(kernel: str, scene: str) -> float | None:
 
 
 # ---------------------------------------------------------------- CPU reference
-def run_reference_cpu(scene, steps: int, warmup: int, budget_s: float | None) -> dict:
-    """The reference's own OpenMP build on all host cores (oracle/_ref);
-    the oracle restatement when the reference build is absent."""
-    from oracle.oracle import OracleSim, RefSim, host_cores, ref_available
-    p = scene.params()
-    x = scene.positions()
-    cores = host_cores()
-    if ref_available():
-        sim = RefSim(p, scene.n, threads=cores)
-        kind = "reference"
-    else:
-        os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-        sim = OracleSim(p, scene.n)
-        kind = "port"
-    sim.set_state(x)
-    for _ in range(max(warmup, 0)):
-        sim.step(1)
-    if budget_s is not None:
-        t0 = time.perf_counter()
-        sim.step(1)
-        one = time.perf_counter() - t0
-        steps = max(1, min(steps, int(budget_s / max(one, 1e-6))))
-    t0 = time.perf_counter()
-    sim.step(steps)
-    dt = time.perf_counter() - t0
-    sim.close()
-    return {"value": scene.n * steps / dt, "unit": UNIT, "cores": cores, "kind": kind,
-            "sample": f"{scene.name}: {scene.n} particles, {steps} timed full steps after {max(warmup, 0)} warm-up "
-                      f"step(s), std::chrono/perf_counter wall time, {dt:.2f} s",
-            "steps": steps, "seconds": dt}
+def workload_config(name: str, n: int, lattice, box, solve_steps: int, lambda_epsilon: float, neighbor_cap: int,
+                    world: int) -> dict:
+    """The `config` of both arms: the workload alone, nothing of either
+    implementation (launch shapes, arithmetic mode) in it."""
+    return {"workload": name, "particles": int(n), "lattice": [int(v) for v in lattice],
+            "box": [float(v) for v in box], "solve_steps": int(solve_steps),
+            "lambda_epsilon": float(lambda_epsilon), "neighbor_cap": int(neighbor_cap),
+            "scorr": "off (reference has none)", "parallelism": f"replicas x{world}",
+            "l2": "no flush: the per-step working set (neighbor lists ~230 MB + particle state) exceeds the 126 MB L2"}
+
+
+def mapped_libraries() -> list[str]:
+    """Shared libraries of this repository mapped into this process."""
+    out = set()
+    try:
+        with open("/proc/self/maps") as f:
+            for line in f:
+                path = line.split()[-1] if len(line.split()) >= 6 else ""
+                if path.endswith(".so") and path.startswith(str(ROOT)):
+                    out.add(str(Path(path).relative_to(ROOT)))
+    except OSError:
+        pass
+    return sorted(out)
+
+
+def run_reference_cpu(name: str, steps: int, warmup: int, budget_s: float | None, threads: int | None = None) -> dict:
+    """The reference's own OpenMP build (oracle/_ref) on `threads` host
+    threads (all of them by default), on the workload built from that build
+    and numpy alone (oracle/ref_scene.py)."""
+    from oracle.ref_scene import WORKLOADS, all_cores, time_reference
+    return time_reference(WORKLOADS[name], steps, warmup, threads or all_cores(), budget_s)
+
+
+def reference_arm(args) -> int:
+    """bench.py --impl reference: the reference's CPU build timed for the
+    same workload and metric as the GPU arm (rank 0 alone; other ranks exit
+    without work).  This process never loads the product's library."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from oracle.ref_scene import WORKLOADS, all_cores, time_reference
+    w = WORKLOADS[args.scene]
+    K, W = args.steps, args.warmup
+    r = time_reference(w, K, W, all_cores())
+    line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": r["steps"], "warmup": W, "ms_per_step": 1e3 * r["seconds"] / r["steps"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded jittered dam-break lattice, zero initial velocity)",
+            "config": workload_config(w.name, w.n, w.lattice, w.box_max, w.solve_steps, w.lambda_epsilon,
+                                      w.neighbor_cap, args.gpus),
+            "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
+                             "sample": r["sample"]},
+            "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "libraries_mapped": mapped_libraries()}
+    print(json.dumps(line), flush=True)
+    return 0
 
 
 # ---------------------------------------------------------------- plain vs learned
@@ -406,26 +435,12 @@ def batched_run(steps: int = 200, autotune: bool = True) -> dict:
 # ---------------------------------------------------------------- main
 def main():
     args = parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
     rank, world, local = dist_env()
     from pbf_b200 import make_scene
     scene = make_scene(args.scene, exact_math=1 if args.exact else 0)
     K, W = args.steps, args.warmup
-
-    if args.impl == "reference":
-        if rank != 0:
-            return 0
-        r = run_reference_cpu(scene, K, W, None)
-        line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
-                "steps": r["steps"], "warmup": W, "ms_per_step": 1e3 * r["seconds"] / r["steps"],
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic (seeded jittered dam-break lattice)",
-                "config": {"workload": scene.name, "particles": scene.n, "solve_steps": scene.solve_steps,
-                           "lambda_epsilon": scene.lambda_epsilon, "neighbor_cap": scene.neighbor_cap},
-                "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
-                                 "sample": r["sample"]},
-                "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        print(json.dumps(line), flush=True)
-        return 0
 
     import numpy as np
     import torch
@@ -535,7 +550,9 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cpu = run_reference_cpu(scene, 100, 1, args.cpu_seconds)
+            cpu = run_reference_cpu(scene.name, 100, 1, args.cpu_seconds)
+            one = run_reference_cpu(scene.name, 100, 0, args.cpu_seconds / 3, threads=1)
+            cpu["one_thread"] = {k: one[k] for k in ("value", "cores", "sample")}
         except Exception as e:  # reported, never fatal for the GPU line
             cpu = {"error": str(e)}
     ranks.barrier()
@@ -546,14 +563,10 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": max(W, 3),
             "ms_per_step": 1e3 * t_dev / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded jittered dam-break lattice, zero initial velocity)",
-            "config": {"workload": scene.name, "particles": scene.n, "lattice": list(scene.lattice),
-                       "box": list(scene.box_max), "solve_steps": scene.solve_steps,
-                       "lambda_epsilon": scene.lambda_epsilon, "neighbor_cap": scene.neighbor_cap,
-                       "exact_math": scene.exact_math, "scorr": "off (reference has none)",
-                       "parallelism": f"replicas x{world}",
-                       "tuning": g.tuning(), "autotuned": not args.no_autotune,
-                       "l2": "no flush: per-step working set (lists %.0f MB + state) > 126 MB L2" % (
-                           scene.n * (4 * nbar + 4) / 1e6)},
+            "config": workload_config(scene.name, scene.n, scene.lattice, scene.box_max, scene.solve_steps,
+                                      scene.lambda_epsilon, scene.neighbor_cap, world),
+            "solver": {"exact_math": scene.exact_math, "tuning": g.tuning(), "autotuned": not args.no_autotune,
+                       "neighbor_list_mb": scene.n * (4 * nbar + 4) / 1e6},
             "e2e": {"value": scene.n * K * world / t_e2e, "unit": UNIT, "h2d_bytes_per_step": scene.n * 24,
                     "d2h_bytes_per_step": scene.n * 24},
             "gpu_launches": launches,

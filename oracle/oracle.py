@@ -20,8 +20,6 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parent
 ORACLE_LIB = ROOT / "_build" / "libpbf_oracle.so"
-REF_LIB = ROOT / "_ref" / "libpbf_ref.so"
-REF_LIB_SERIAL = ROOT / "_ref" / "libpbf_ref_serial.so"
 
 # Stage numbering shared by both checkers (and the reference driver).
 STAGES = ["apply_external_forces", "predict_positions", "find_neighbors", "compute_densities",
@@ -167,64 +165,8 @@ class OracleSim:
 
 
 # ---------------------------------------------------------------- reference
-class RefParams(C.Structure):
-    _fields_ = [
-        ("time_step", C.c_float), ("gravity", C.c_float), ("gamma", C.c_float), ("visc_c", C.c_float),
-        ("lambda_epsilon", C.c_float), ("k_stiff", C.c_float), ("vorticity_coef", C.c_float),
-        ("smoothing_radius", C.c_float), ("neighbor_bin_spacing", C.c_float), ("rest_spacing", C.c_float),
-        ("boundary_min", C.c_float * 3), ("boundary_max", C.c_float * 3),
-        ("fluid_min", C.c_float * 3), ("fluid_max", C.c_float * 3), ("mover_center", C.c_float * 3),
-        ("solve_steps", C.c_uint64), ("max_particles_local", C.c_uint64), ("global_particle_count", C.c_uint64),
-        ("rest_density", C.c_float),
-    ]
-
-
-_ref_libs: dict[str, C.CDLL] = {}
-
-
-def ref_available(serial: bool = False) -> bool:
-    return (REF_LIB_SERIAL if serial else REF_LIB).exists()
-
-
-def ref_lib(serial: bool = False) -> C.CDLL:
-    path = REF_LIB_SERIAL if serial else REF_LIB
-    key = str(path)
-    if key not in _ref_libs:
-        if not path.exists():
-            raise RuntimeError(f"{path} missing: it is built from the reference sources by oracle/ref_build/Makefile")
-        lib = C.CDLL(key)
-        R = C.POINTER(RefParams)
-        sig = {
-            "ref_last_error": (C.c_char_p, []),
-            "ref_set_threads": (None, [C.c_int]),
-            "ref_get_threads": (C.c_int, []),
-            "ref_derived": (C.c_int, [R, _vp]),
-            "ref_derived_from_ini": (C.c_int, [C.c_char_p, _vp, _vp]),
-            "ref_create": (_vp, [R]),
-            "ref_destroy": (None, [_vp]),
-            "ref_set_rest_density": (None, [_vp, C.c_float]),
-            "ref_get_param": (C.c_float, [_vp, C.c_int]),
-            "ref_construct_fluid": (C.c_int64, [_vp]),
-            "ref_add": (C.c_int, [_vp, _vp, _vp, C.c_uint64]),
-            "ref_count": (C.c_uint64, [_vp]),
-            "ref_set_vec": (C.c_int, [_vp, C.c_int, _vp]),
-            "ref_get_vec": (C.c_int, [_vp, C.c_int, _vp]),
-            "ref_get_scalar": (C.c_int, [_vp, C.c_int, _vp]),
-            "ref_set_scalar": (C.c_int, [_vp, C.c_int, _vp]),
-            "ref_bin_dims": (None, [_vp, _vp]),
-            "ref_bin_id": (C.c_uint64, [_vp, _vp]),
-            "ref_get_neighbors": (C.c_int, [_vp, _vp, _vp, C.c_int]),
-            "ref_get_bins": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
-            "ref_stage": (C.c_int, [_vp, C.c_int, C.c_int]),
-            "ref_step": (C.c_int, [_vp, C.c_int]),
-            "ref_time_steps": (C.c_double, [_vp, C.c_int]),
-        }
-        for k, (r, a) in sig.items():
-            f = getattr(lib, k)
-            f.restype = r
-            f.argtypes = a
-        _ref_libs[key] = lib
-    return _ref_libs[key]
+# The reference build's bindings live in reflib (no product import there).
+from .reflib import REF_LIB, REF_LIB_SERIAL, RefParams, host_cores, ref_available, ref_lib  # noqa: E402,F401
 
 
 def ref_params_from(p, capacity: int, fluid_min=(0, 0, 0), fluid_max=(0, 0, 0)) -> RefParams:
@@ -360,10 +302,3 @@ class RefSim:
             "cap_hits": int((cnt >= self.cap).sum()),
             "error_flags": 0,
         }
-
-
-def host_cores() -> int:
-    try:
-        return len(os.sched_getaffinity(0))
-    except AttributeError:
-        return os.cpu_count() or 1
