@@ -384,12 +384,22 @@ int pbf_selftest_mlp_wait_timeout(pbf_ctx* ctx, uint32_t* flags);
  * cudaMalloc/cudaFree.  Builds the reference's neighbor lists (the same lists
  * as pbf_find_neighbors + pbf_get_neighbors) for a caller-owned device point
  * set, using only a file-scope device array of PBF_NOALLOC_SCRATCH_BYTES that
- * every GPU loading the library holds until the process exits.
- *   d_x    device, n x 3 floats (AoS), the positions to bin
- *   d_nbr  device, n x neighbor_cap int32: reference indices, -1 past the count
- *   d_cnt  device, n int32 counts
- *   stream a cudaStream_t (NULL: the legacy default stream); the work is
- *          enqueued there and the call returns without synchronising.
+ * every GPU loading the library holds until the process exits.  The sort is
+ * the regular path's stable radix sort (linear in n however the points crowd
+ * into bins) and crowded bins are walked run by run over bit-identical
+ * positions, so no input makes the search quadratic in a bin's population
+ * beyond the distance tests the reference itself makes.
+ *   d_x     device, n x 3 floats (AoS), the positions to bin
+ *   d_nbr   device, n x neighbor_cap int32: reference indices, -1 past the count
+ *   d_cnt   device, n int32 counts
+ *   d_flags device, one uint32 (may be NULL: nothing reported): receives the
+ *           call's PBF_FLAG_* bits, PBF_FLAG_KEY_RANGE when a position is
+ *           non-finite or outside the bin grid (its bins are clamped into the
+ *           grid, as the regular path does, and the lists are not the
+ *           reference's for such input)
+ *   stream  a cudaStream_t (NULL: the legacy default stream); the work is
+ *           enqueued there and the call returns without synchronising, so
+ *           read *d_flags after the stream has reached it.
  * Limits: n <= PBF_NOALLOC_MAX_PARTICLES and a grid of at most
  * PBF_NOALLOC_MAX_BINS bins; larger inputs return PBF_ERR_CAPACITY with the
  * message in pbf_last_error(NULL).  The first call on a device looks up the
@@ -398,9 +408,9 @@ int pbf_selftest_mlp_wait_timeout(pbf_ctx* ctx, uint32_t* flags);
  * on the GPU (other streams, other host threads) race — serialise them. */
 #define PBF_NOALLOC_MAX_PARTICLES 65536
 #define PBF_NOALLOC_MAX_BINS 262144
-#define PBF_NOALLOC_SCRATCH_BYTES 4719616
+#define PBF_NOALLOC_SCRATCH_BYTES 5506560
 int pbf_find_neighbors_noalloc(const pbf_params* p, const float* d_x, size_t n, int32_t* d_nbr,
-                               int32_t* d_cnt, void* stream);
+                               int32_t* d_cnt, uint32_t* d_flags, void* stream);
 
 #ifdef __cplusplus
 }

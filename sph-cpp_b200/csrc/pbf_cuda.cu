@@ -322,37 +322,6 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_apply(const uint32_t* __r
   }
 }
 
-// Counting-sort scatter of the no-allocation neighbor search: slot =
-// start(bin) + atomic rank; k_cell_sort then orders every bin by reference
-// index (the permutation of the reference's stable sort_by_key,
-// neighbors.h:130-132).
-__global__ void k_scatter(int n, const uint32_t* __restrict__ key, const uint32_t* __restrict__ rank,
-                          const uint32_t* __restrict__ cell_start, const uint32_t* __restrict__ orig,
-                          unsigned long long* pairs) {
-  const int a = blockIdx.x * blockDim.x + threadIdx.x;
-  if (a >= n) return;
-  const uint32_t slot = cell_start[key[a]] + rank[a];
-  pairs[slot] = ((unsigned long long)orig[a] << 32) | (unsigned long long)a;
-}
-
-// Per-bin insertion sort of the scattered pairs into ascending reference
-// index (the no-allocation neighbor search uses this form).
-__global__ void k_cell_sort(int nbins, const uint32_t* __restrict__ cell_start, unsigned long long* pairs) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= nbins) return;
-  const uint32_t b0 = cell_start[c], b1 = cell_start[c + 1];
-  if (b1 - b0 < 2) return;
-  for (uint32_t i = b0 + 1; i < b1; ++i) {
-    const unsigned long long v = pairs[i];
-    uint32_t j = i;
-    while (j > b0 && pairs[j - 1] > v) {
-      pairs[j] = pairs[j - 1];
-      --j;
-    }
-    pairs[j] = v;
-  }
-}
-
 // ---- stable LSD radix sort of (bin key, pair) ----
 // The hash kernels write every particle's key and pair (reference index << 32
 // | home slot) at its reference index, so the input is in reference-index
@@ -3803,6 +3772,21 @@ int pbf_launches_per_step(pbf_ctx* ctx, int64_t* out) {
 // cudaFree imply.  All working memory lives in the file-scope array below
 // (PBF_NOALLOC_SCRATCH_BYTES, held on every GPU that loads the library until
 // the process exits); the caller passes only its inputs and outputs.
+// The steps are the regular neighbor search's:
+//   hash      bin key and (index << 32 | index) at the caller's index, plus
+//             the bin histogram (calculate_bins, neighbors.h:120-125)
+//   bounds    exclusive scan of the histogram = begin/end of every bin
+//             (find_bin_bounds, neighbors.h:137-148)
+//   sort      the stable LSD radix passes of the regular path, ping-ponging
+//             between two key/pair buffers of the array: O(n) per pass however
+//             particles crowd into bins (sort_bins, neighbors.h:130-132)
+//   gather    positions into sorted order, with their reference indices
+//   runs      runs of bit-identical positions among consecutive sorted slots
+//   fill      the lists in reference index space (fill_neighbors,
+//             neighbors.h:197-230); a bin of more than kRunBin particles is
+//             walked run by run, one distance test per run
+//   flags     the error word (out-of-grid or non-finite positions) copied to
+//             the caller's flag word.
 namespace {
 
 constexpr size_t kAlign = 256;
@@ -3810,15 +3794,22 @@ constexpr size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign;
 constexpr size_t kNaN = PBF_NOALLOC_MAX_PARTICLES;
 constexpr size_t kNaB = PBF_NOALLOC_MAX_BINS;
 constexpr size_t kNaParts = (kNaB + 1 + kScanTile - 1) / kScanTile;
+constexpr size_t kNaTiles = (kNaN + kRadixTile - 1) / kRadixTile;
+constexpr size_t kNaHist = (size_t)kRadixDigits * kNaTiles;
+constexpr size_t kNaHistParts = (kNaHist + 1 + kScanTile - 1) / kScanTile;
 // layout of the scratch array (byte offsets)
 constexpr size_t kOffCount = 0;
 constexpr size_t kOffStart = align_up(kOffCount + 4 * kNaB);
 constexpr size_t kOffParts = align_up(kOffStart + 4 * (kNaB + 1));
-constexpr size_t kOffKey = align_up(kOffParts + 4 * kNaParts);
-constexpr size_t kOffRank = align_up(kOffKey + 4 * kNaN);
-constexpr size_t kOffIdent = align_up(kOffRank + 4 * kNaN);
-constexpr size_t kOffPairs = align_up(kOffIdent + 4 * kNaN);
-constexpr size_t kOffSortedX = align_up(kOffPairs + 8 * kNaN);
+constexpr size_t kOffKeyA = align_up(kOffParts + 4 * kNaParts);
+constexpr size_t kOffKeyB = align_up(kOffKeyA + 4 * kNaN);
+constexpr size_t kOffPairA = align_up(kOffKeyB + 4 * kNaN);
+constexpr size_t kOffPairB = align_up(kOffPairA + 8 * kNaN);
+constexpr size_t kOffHist = align_up(kOffPairB + 8 * kNaN);
+constexpr size_t kOffHistOff = align_up(kOffHist + 4 * kNaHist);
+constexpr size_t kOffHistParts = align_up(kOffHistOff + 4 * (kNaHist + 1));
+constexpr size_t kOffRunEnd = align_up(kOffHistParts + 4 * kNaHistParts);
+constexpr size_t kOffSortedX = align_up(kOffRunEnd + 4 * kNaN);
 constexpr size_t kOffSortedId = align_up(kOffSortedX + 16 * kNaN);
 constexpr size_t kOffErr = align_up(kOffSortedId + 4 * kNaN);
 constexpr size_t kNoallocBytes = align_up(kOffErr + 4);
@@ -3831,17 +3822,20 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
 std::mutex g_noalloc_mu;
 void* g_noalloc_addr[128] = {nullptr};
 
-// calculate_bins over caller AoS positions (neighbors.h:120-125) + histogram.
-__global__ void k_noalloc_hash(Dev P, int n, const float* __restrict__ x, uint32_t* key, uint32_t* rank,
-                               uint32_t* ident, uint32_t* cell_count, uint32_t* err) {
+// calculate_bins over caller AoS positions (neighbors.h:120-125), the sort's
+// input at the caller's index and the bin histogram (one atomic per distinct
+// bin of a warp).
+__global__ void k_noalloc_hash(Dev P, int n, const float* __restrict__ x, uint32_t* key, unsigned long long* pair,
+                               uint32_t* cell_count, uint32_t* err) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= n) return;
   uint32_t k;
   if (!pbf::bin_of(P, pbf::region_of(P, 0), x[3 * (size_t)a], x[3 * (size_t)a + 1], x[3 * (size_t)a + 2], k))
     atomicOr(err, PBF_FLAG_KEY_RANGE);
   key[a] = k;
-  ident[a] = (uint32_t)a;
-  rank[a] = atomicAdd(&cell_count[k], 1u);
+  pair[a] = ((unsigned long long)a << 32) | (unsigned long long)a;
+  const unsigned peers = __match_any_sync(__activemask(), k);
+  if ((peers & ((1u << (threadIdx.x & 31)) - 1u)) == 0u) atomicAdd(&cell_count[k], (uint32_t)__popc(peers));
 }
 
 __global__ void k_noalloc_gather(int n, const unsigned long long* __restrict__ pairs, const float* __restrict__ x,
@@ -3854,11 +3848,37 @@ __global__ void k_noalloc_gather(int n, const unsigned long long* __restrict__ p
   sorted_id[b] = (uint32_t)(pr >> 32);
 }
 
-// Variant of the list fill that writes the lists straight into the caller's output
-// in reference index space: out[id][k], -1 past the count.
+// A crowded bin [q0, q1) run by run (runs of bit-identical positions from
+// k_runs): one distance test per run; on a hit the run's particles are
+// appended in order, the particle's own slot left out, while the list has
+// room.  Equal positions give equal tests, so the list is the one-by-one
+// walk's.  Returns the new length.
+__device__ __noinline__ int noalloc_fill_runs(float px, float py, float pz, float s2, int cap, uint32_t self,
+                                              uint32_t q0, uint32_t q1, const float4* __restrict__ pst,
+                                              const uint32_t* __restrict__ run_end,
+                                              const uint32_t* __restrict__ sorted_id, int32_t* row, int count) {
+  for (uint32_t q = q0; q < q1;) {
+    const float4 xq = pst[q];
+    const uint32_t qe = min(run_end[q], q1);
+    const float d2 = pbf::mag2<true>(pbf::xsub(px, xq.x), pbf::xsub(py, xq.y), pbf::xsub(pz, xq.z));
+    if (d2 < s2) {
+      for (uint32_t r = q; r < qe && count < cap; ++r) {
+        if (r == self) continue;
+        row[count++] = (int32_t)sorted_id[r];
+      }
+      if (count >= cap) break;
+    }
+    q = qe;
+  }
+  return count;
+}
+
+// The list fill writing straight into the caller's output in reference index
+// space: out[id][k], -1 past the count.
 __global__ void __launch_bounds__(kBlock) k_noalloc_fill(Dev P, int n, const float4* __restrict__ pst,
                                                          const uint32_t* __restrict__ sorted_id,
-                                                         const uint32_t* __restrict__ cell_start, int32_t* out,
+                                                         const uint32_t* __restrict__ cell_start,
+                                                         const uint32_t* __restrict__ run_end, int32_t* out,
                                                          int32_t* out_cnt, uint32_t* err) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= n) return;
@@ -3878,6 +3898,11 @@ __global__ void __launch_bounds__(kBlock) k_noalloc_fill(Dev P, int n, const flo
           continue;
         }
         const uint32_t q0 = cell_start[nb], q1 = cell_start[nb + 1];
+        if (q1 - q0 > kRunBin) {
+          count = noalloc_fill_runs(xp.x, xp.y, xp.z, P.s2, cap, (uint32_t)b, q0, q1, pst, run_end, sorted_id,
+                                    row, count);
+          continue;
+        }
         for (uint32_t q = q0; q < q1; ++q) {
           if (q == (uint32_t)b) continue;
           const float4 xq = pst[q];
@@ -3897,7 +3922,7 @@ __global__ void __launch_bounds__(kBlock) k_noalloc_fill(Dev P, int n, const flo
 }  // namespace
 
 extern "C" int pbf_find_neighbors_noalloc(const pbf_params* p, const float* d_x, size_t n, int32_t* d_nbr,
-                                          int32_t* d_cnt, void* stream_handle) {
+                                          int32_t* d_cnt, uint32_t* d_flags, void* stream_handle) {
   if (!p || (n && (!d_x || !d_nbr || !d_cnt))) return fail(nullptr, PBF_ERR_ARG, "null argument");
   if (n > PBF_NOALLOC_MAX_PARTICLES)
     return fail(nullptr, PBF_ERR_CAPACITY, "pbf_find_neighbors_noalloc: %zu particles exceed the maximum of %d",
@@ -3908,9 +3933,15 @@ extern "C" int pbf_find_neighbors_noalloc(const pbf_params* p, const float* d_x,
   if (d.nbins > PBF_NOALLOC_MAX_BINS)
     return fail(nullptr, PBF_ERR_CAPACITY, "pbf_find_neighbors_noalloc: grid of %d bins exceeds the maximum of %d",
                 d.nbins, PBF_NOALLOC_MAX_BINS);
-  if (n == 0) return PBF_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream_handle);
+  cudaError_t e;
+  if (n == 0) {
+    if (d_flags && (e = cudaMemsetAsync(d_flags, 0, 4, s)) != cudaSuccess)
+      return fail(nullptr, PBF_ERR_CUDA, "cudaMemsetAsync failed: %s", cudaGetErrorString(e));
+    return PBF_OK;
+  }
   int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  e = cudaGetDevice(&dev);
   if (e != cudaSuccess || dev < 0 || dev >= 128)
     return fail(nullptr, PBF_ERR_CUDA, "cudaGetDevice failed: %s", cudaGetErrorString(e));
   unsigned char* base;
@@ -3925,32 +3956,53 @@ extern "C" int pbf_find_neighbors_noalloc(const pbf_params* p, const float* d_x,
     }
     base = static_cast<unsigned char*>(g_noalloc_addr[dev]);
   }
-  cudaStream_t s = static_cast<cudaStream_t>(stream_handle);
   auto* cell_count = reinterpret_cast<uint32_t*>(base + kOffCount);
   auto* cell_start = reinterpret_cast<uint32_t*>(base + kOffStart);
   auto* parts = reinterpret_cast<uint32_t*>(base + kOffParts);
-  auto* key = reinterpret_cast<uint32_t*>(base + kOffKey);
-  auto* rank = reinterpret_cast<uint32_t*>(base + kOffRank);
-  auto* ident = reinterpret_cast<uint32_t*>(base + kOffIdent);
-  auto* pairs = reinterpret_cast<unsigned long long*>(base + kOffPairs);
+  uint32_t* kin = reinterpret_cast<uint32_t*>(base + kOffKeyA);
+  uint32_t* kout = reinterpret_cast<uint32_t*>(base + kOffKeyB);
+  auto* vin = reinterpret_cast<unsigned long long*>(base + kOffPairA);
+  auto* vout = reinterpret_cast<unsigned long long*>(base + kOffPairB);
+  auto* hist = reinterpret_cast<uint32_t*>(base + kOffHist);
+  auto* hist_off = reinterpret_cast<uint32_t*>(base + kOffHistOff);
+  auto* hist_parts = reinterpret_cast<uint32_t*>(base + kOffHistParts);
+  auto* run_end = reinterpret_cast<uint32_t*>(base + kOffRunEnd);
   auto* sorted_x = reinterpret_cast<float4*>(base + kOffSortedX);
   auto* sorted_id = reinterpret_cast<uint32_t*>(base + kOffSortedId);
   auto* err = reinterpret_cast<uint32_t*>(base + kOffErr);
-  // The array keeps the previous call's contents: clear what must start at zero.
+  // The array keeps the previous call's contents: clear what must start at
+  // zero (the histogram and the error word; every other buffer is written in
+  // full before it is read).
   e = cudaMemsetAsync(cell_count, 0, 4 * (size_t)d.nbins, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, 4, s);
   if (e != cudaSuccess) return fail(nullptr, PBF_ERR_CUDA, "cudaMemsetAsync failed: %s", cudaGetErrorString(e));
   const int nn = (int)n, g = blocks_for(n);
   const int nparts = (int)(((size_t)d.nbins + 1 + kScanTile - 1) / kScanTile);
-  k_noalloc_hash<<<g, kBlock, 0, s>>>(d, nn, d_x, key, rank, ident, cell_count, err);
+  k_noalloc_hash<<<g, kBlock, 0, s>>>(d, nn, d_x, kin, vin, cell_count, err);
   k_scan_reduce<<<nparts, kScanThreads, 0, s>>>(cell_count, d.nbins, parts);
   k_scan_partials<<<1, kScanThreads, 0, s>>>(parts, nparts);
   k_scan_apply<<<nparts, kScanThreads, 0, s>>>(cell_count, d.nbins, parts, cell_start);
-  k_scatter<<<g, kBlock, 0, s>>>(nn, key, rank, cell_start, ident, pairs);
-  k_cell_sort<<<blocks_for(d.nbins), kBlock, 0, s>>>(d.nbins, cell_start, pairs);
-  k_noalloc_gather<<<g, kBlock, 0, s>>>(nn, pairs, d_x, sorted_x, sorted_id);
-  k_noalloc_fill<<<g, kBlock, 0, s>>>(d, nn, sorted_x, sorted_id, cell_start, d_nbr, d_cnt, err);
-  e = cudaGetLastError();
+  const int tiles = (int)(((size_t)n + kRadixTile - 1) / kRadixTile);
+  const int hm = kRadixDigits * tiles;
+  const int hp = (int)(((size_t)hm + 1 + kScanTile - 1) / kScanTile);
+  const int passes = radix_passes_for(d.nbins);
+  for (int pass = 0; pass < passes; ++pass) {
+    const int shift = pass * kRadixBits;
+    const bool last = pass == passes - 1;
+    k_radix_hist<<<tiles, kRadixThreads, 0, s>>>(kin, nn, shift, tiles, hist);
+    k_scan_reduce<<<hp, kScanThreads, 0, s>>>(hist, hm, hist_parts);
+    k_scan_partials<<<1, kScanThreads, 0, s>>>(hist_parts, hp);
+    k_scan_apply<<<hp, kScanThreads, 0, s>>>(hist, hm, hist_parts, hist_off);
+    k_radix_scatter<<<tiles, kRadixThreads, 0, s>>>(kin, vin, nn, shift, tiles, hist_off, last ? nullptr : kout,
+                                                   vout);
+    std::swap(kin, kout);
+    std::swap(vin, vout);
+  }
+  k_noalloc_gather<<<g, kBlock, 0, s>>>(nn, vin, d_x, sorted_x, sorted_id);
+  k_runs<<<blocks_for(n, kRunBlock), kRunBlock, 0, s>>>(nn, sorted_x, run_end);
+  k_noalloc_fill<<<g, kBlock, 0, s>>>(d, nn, sorted_x, sorted_id, cell_start, run_end, d_nbr, d_cnt, err);
+  if (d_flags) e = cudaMemcpyAsync(d_flags, err, 4, cudaMemcpyDeviceToDevice, s);
+  if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) return fail(nullptr, PBF_ERR_CUDA, "noalloc neighbor search launch: %s", cudaGetErrorString(e));
   return PBF_OK;
 }

@@ -38,6 +38,7 @@ TUNE_CANDIDATES = ((4, 128, 0), (4, 256, 0), (8, 128, 0), (8, 256, 0), (2, 128, 
 
 NOALLOC_MAX_PARTICLES = 65536
 NOALLOC_MAX_BINS = 262144
+NOALLOC_SCRATCH_BYTES = 5506560
 
 F3 = C.c_float * 3
 
@@ -184,7 +185,7 @@ SIGNATURES = {
     "pbf_get_tuning": (_i, [_vp, _P(PbfTuning)]),
     "pbf_set_tuning": (_i, [_vp, _P(PbfTuning)]),
     "pbf_autotune": (_i, [_vp, _i, _P(PbfTuning), _P(C.c_double)]),
-    "pbf_find_neighbors_noalloc": (_i, [_P(PbfParams), _vp, _sz, _vp, _vp, _vp]),
+    "pbf_find_neighbors_noalloc": (_i, [_P(PbfParams), _vp, _sz, _vp, _vp, _vp, _vp]),
     "pbf_mlp_init": (_i, [_vp, C.c_uint64]),
     "pbf_mlp_get": (_i, [_vp, _vp, _vp]),
     "pbf_mlp_set": (_i, [_vp, _vp, _vp]),
