@@ -62,6 +62,8 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU baseline sample")
     ap.add_argument("--no-autotune", action="store_true", help="default launch shapes instead of the autotuner's")
     ap.add_argument("--no-batched", action="store_true", help="skip the 64-scene batch measurement")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the 16.8M dam, the 200-step trajectory and the s_corr run")
     return ap.parse_args()
 
 
@@ -432,6 +434,65 @@ def batched_run(steps: int = 200, autotune: bool = True) -> dict:
     return out
 
 
+# ---------------------------------------------------------------- more workloads
+def timed_steps(g, stream, steps: int) -> float:
+    """Seconds of `steps` graph-replayed steps on the library's stream (CUDA events)."""
+    import torch
+    g.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        g.step(1)
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / 1e3
+
+
+def plain_run(scene, steps: int, warmup: int, tuning=None) -> dict:
+    """particle-steps/s of `steps` graph-replayed steps of `scene` after
+    `warmup` steps, with the given launch shapes (the 1M dam's autotuned ones)."""
+    import torch
+    from pbf_b200 import Particles
+    with Particles(scene.params(), scene.n) as g:
+        if tuning:
+            g.set_tuning(tuning)
+        stream = torch.cuda.ExternalStream(g.stream_handle())
+        g.upload(scene.positions())
+        for _ in range(warmup):
+            g.step(1)
+        t = timed_steps(g, stream, steps)
+        st = g.stats()
+    return {"workload": f"{scene.name}: {scene.n} particles, K = {scene.solve_steps}, cap {scene.neighbor_cap}, "
+                        f"eps {scene.lambda_epsilon}, s_corr k = {scene.scorr[0]}",
+            "value": scene.n * steps / t, "unit": UNIT, "ms_per_step": 1e3 * t / steps, "steps": steps,
+            "warmup": warmup, "mean_density_error": st["mean_density_error"], "mean_neighbors": st["mean_neighbors"],
+            "error_flags": st["error_flags"]}
+
+
+def trajectory_run(scene, steps: int = 200, window: int = 50, tuning=None) -> dict:
+    """The whole `steps`-step dam break from its initial state, timed in
+    windows of `window` graph-replayed steps (the step cost grows as the
+    dam collapses and the bins crowd)."""
+    import torch
+    from pbf_b200 import Particles
+    with Particles(scene.params(), scene.n) as g:
+        if tuning:
+            g.set_tuning(tuning)
+        stream = torch.cuda.ExternalStream(g.stream_handle())
+        g.upload(scene.positions())
+        g.step(1)                      # captures the one-step graph
+        g.upload(scene.positions())    # back to the initial state
+        ts, errs = [], []
+        for _ in range(steps // window):
+            ts.append(timed_steps(g, stream, window))
+            errs.append(g.stats()["mean_density_error"])
+    total = sum(ts)
+    return {"workload": f"{scene.name}: steps 0..{steps} from the initial state, K = {scene.solve_steps}",
+            "value": scene.n * steps / total, "unit": UNIT, "ms_per_step": 1e3 * total / steps,
+            "windows": [{"steps": f"{i * window}..{(i + 1) * window}", "ms_per_step": 1e3 * t / window,
+                         "mean_density_error_at_end": e} for i, (t, e) in enumerate(zip(ts, errs))]}
+
+
 # ---------------------------------------------------------------- main
 def main():
     args = parse_args()
@@ -547,6 +608,19 @@ def main():
         except Exception as e:  # reported, never fatal for the GPU line
             batched = {"error": str(e)}
 
+    extra = None
+    if rank == 0 and world == 1 and not args.no_extra:
+        extra = {}
+        shapes = g.tuning()
+        for key, fn in (("dam_16m", lambda: plain_run(make_scene("dam_16m"), 10, 3, shapes)),
+                        ("trajectory_200", lambda: trajectory_run(make_scene(args.scene), 200, 50, shapes)),
+                        ("scorr_on", lambda: plain_run(make_scene(args.scene, scorr=(0.1, 4.0, 0.2)), K, max(W, 3),
+                                                       shapes))):
+            try:
+                extra[key] = fn()
+            except Exception as e:  # reported, never fatal for the GPU line
+                extra[key] = {"error": str(e)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -584,6 +658,7 @@ def main():
             "clocks": clk.summary(),
             "learned_vs_plain": learned,
             "batched": batched,
+            "extra": extra,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
