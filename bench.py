@@ -62,6 +62,9 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU baseline sample")
     ap.add_argument("--no-autotune", action="store_true", help="default launch shapes instead of the autotuner's")
     ap.add_argument("--no-batched", action="store_true", help="skip the 64-scene batch measurement")
+    ap.add_argument("--profile-learned", type=int, default=0, metavar="K",
+                    help="only run K steps of the learned warm start (eps 1, after its warm-up) and print "
+                         "ms/step: the command the learned kernels' ncu summaries are captured from")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the 16.8M dam, the 200-step trajectory and the s_corr run")
     return ap.parse_args()
@@ -498,6 +501,14 @@ def main():
     args = parse_args()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.profile_learned:
+        from pbf_b200.learn import DEFAULT_MODEL, load_model, warm_start_scene
+        params, norm, _ = load_model(DEFAULT_MODEL)
+        sc = warm_start_scene(args.scene, seed=4242).with_(solver=1, residual_tol=0.01, max_iterations=10)
+        r = solver_run(sc, args.profile_learned, args.warmup, params, norm, autotune=False)
+        print(json.dumps({"learned_ms_per_step": r["ms_per_step"], "iterations": r["mean_iterations"],
+                          "kernel_ms_per_step": r["kernel_ms_per_step"]}), flush=True)
+        return 0
     rank, world, local = dist_env()
     from pbf_b200 import make_scene
     scene = make_scene(args.scene, exact_math=1 if args.exact else 0)

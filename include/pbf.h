@@ -19,9 +19,15 @@
  *  - Work is stream-ordered on the context's own CUDA stream; functions that
  *    return host data synchronise that stream.  One context per host thread;
  *    a context is not re-entrant.
- *  - Spans: the reference's IndexSpan arguments are kept for call-surface
- *    fidelity.  A single rank always passes [0, N); any other span returns
- *    PBF_ERR_SPAN.
+ *  - Spans: the reference's IndexSpan arguments, [b, e) over reference
+ *    indices.  A single rank passes [0, N).  A multi-rank driver (the x-slab
+ *    decomposition, Simulation/Source/main.adios) passes [0, R) for its R
+ *    resident particles, the first R reference indices; the others are halo
+ *    particles: the stage reads them as neighbours and leaves them as they
+ *    are.  find_neighbors bins every held particle (its bin span must be
+ *    [0, N)) and fills lists for its fill span only (the others get empty
+ *    lists).  Spans not starting at 0 or ending past N return PBF_ERR_SPAN.
+ *    The fused pbf_step always covers every particle.
  *  - Device memory is owned by the context (allocated once in pbf_create,
  *    sized by capacity); the caller keeps ownership of its host arrays.
  */
@@ -39,7 +45,7 @@ extern "C" {
 #define PBF_ERR_ARG -1        /* bad argument (null pointer, size) */
 #define PBF_ERR_CUDA -2       /* CUDA runtime error */
 #define PBF_ERR_CAPACITY -3   /* n > capacity (reference: array.h:128-129) */
-#define PBF_ERR_SPAN -4       /* span other than [0, N) */
+#define PBF_ERR_SPAN -4       /* span not [0, e) with e <= N */
 #define PBF_ERR_PARAMS -5     /* parameters outside what the reference grid supports */
 #define PBF_ERR_STATE -6      /* call out of order (e.g. no neighbor lists yet) */
 #define PBF_ERR_DEVICE -7     /* device-side check tripped (see pbf_stats_t.error_flags) */

@@ -199,6 +199,21 @@ int64_t ref_construct_fluid(void* h) {
   }
 }
 
+// construct_fluid over a given box with an initial velocity (particles.h:231-250),
+// as the multi-rank driver's distribute_fluid calls it (distributor.h:318-353).
+int64_t ref_construct_fluid_box(void* h, const float mn[3], const float mx[3], const float vel[3]) {
+  auto* s = static_cast<RefSim*>(h);
+  try {
+    AABB<Real, Dim> box;
+    box.min = V3{mn[0], mn[1], mn[2]};
+    box.max = V3{mx[0], mx[1], mx[2]};
+    return (int64_t)s->parts->construct_fluid(box, V3{vel[0], vel[1], vel[2]});
+  } catch (std::exception const& e) {
+    g_error = e.what();
+    return -1;
+  }
+}
+
 // Append particles with x* = x (particles.h:161-176).
 int ref_add(void* h, const float* x, const float* v, uint64_t n) {
   auto* s = static_cast<RefSim*>(h);
@@ -216,6 +231,18 @@ int ref_add(void* h, const float* x, const float* v, uint64_t n) {
 }
 
 uint64_t ref_count(void* h) { return static_cast<RefSim*>(h)->parts->local_count(); }
+
+// Drop the last k particles (particles.h:146-154): the multi-rank driver's
+// halo invalidation and OOB removal.
+int ref_remove(void* h, uint64_t k) {
+  auto* p = static_cast<RefSim*>(h)->parts;
+  if (k > p->local_count()) {
+    g_error = "ref_remove: more particles than held";
+    return -1;
+  }
+  p->remove(k);
+  return 0;
+}
 
 // Overwrite per-particle arrays (AoS float3) of the current particles.
 // which: 0 positions, 1 position_stars, 2 velocities, 3 scratch
@@ -324,6 +351,37 @@ int ref_stage(void* h, int stage, int sub) {
       case 10: p->compute_vorticity(span); break;
       case 11: p->apply_vorticity(span); break;
       case 12: p->update_positions(span); break;
+      default: g_error = "unknown stage"; return -1;
+    }
+    return 0;
+  } catch (std::exception const& e) {
+    g_error = e.what();
+    return -1;
+  }
+}
+
+// One stage over explicit spans, as the multi-rank driver calls them
+// (Simulation/Source/main.adios: resident and local spans): [a0, a1) is the
+// stage's span; [b0, b1) the second span of find_neighbors (fill) and
+// apply_surface_tension.  Stage numbers as in ref_stage.
+int ref_stage_span(void* h, int stage, int sub, uint64_t a0, uint64_t a1, uint64_t b0, uint64_t b1) {
+  auto* p = static_cast<RefSim*>(h)->parts;
+  const IndexSpan a{a0, a1}, b{b0, b1};
+  try {
+    switch (stage) {
+      case 0: p->apply_external_forces(a); break;
+      case 1: p->predict_positions(a); break;
+      case 2: p->find_neighbors(a, b); break;
+      case 3: p->compute_densities(a); break;
+      case 4: p->compute_pressure_lambdas(a); break;
+      case 5: p->compute_pressure_dps(a, sub); break;
+      case 6: p->update_position_stars(a); break;
+      case 7: p->update_velocities(a); break;
+      case 8: p->apply_surface_tension(a, b); break;
+      case 9: p->apply_viscosity(a); break;
+      case 10: p->compute_vorticity(a); break;
+      case 11: p->apply_vorticity(a); break;
+      case 12: p->update_positions(a); break;
       default: g_error = "unknown stage"; return -1;
     }
     return 0;

@@ -58,8 +58,17 @@ class Workload:
         return int(self.lattice[0] * self.lattice[1] * self.lattice[2])
 
     @property
-    def fluid_max(self) -> tuple[float, float, float]:
+    def fluid_extent(self) -> tuple[float, float, float]:
+        """The lattice's extent, lattice * spacing per axis."""
         return tuple(float(self.lattice[a] * self.spacing) for a in range(3))
+
+    @property
+    def fluid_max(self) -> tuple[float, float, float]:
+        """The box construct_fluid fills: half a spacing past the lattice's
+        extent, so that its floor(extent / spacing) count is the lattice's
+        whatever the rounding of extent / spacing (the points themselves are
+        index * spacing + min + spacing / 2, independent of the box's max)."""
+        return tuple(float((self.lattice[a] + 0.5) * self.spacing) for a in range(3))
 
 
 # The benchmark's dam breaks (lattice, box, Jacobi iterations, neighbor cap).
@@ -117,7 +126,7 @@ def rest_density(w: Workload, r: int = 4) -> float:
     the reference's own construct_fluid, find_neighbors and compute_densities."""
     lib = ref_lib()
     n1 = 2 * r + 1
-    ext = tuple(float(n1 * w.spacing) for _ in range(3))
+    ext = tuple(float((n1 + 0.5) * w.spacing) for _ in range(3))
     rp = ref_params(w, box_max=ext, fluid_max=ext, capacity=n1 ** 3)
     h = lib.ref_create(C.byref(rp))
     if not h:

@@ -60,8 +60,11 @@ def ref_lib(serial: bool = False) -> C.CDLL:
             "ref_set_rest_density": (None, [_vp, C.c_float]),
             "ref_get_param": (C.c_float, [_vp, C.c_int]),
             "ref_construct_fluid": (C.c_int64, [_vp]),
+            "ref_construct_fluid_box": (C.c_int64, [_vp, _vp, _vp, _vp]),
             "ref_add": (C.c_int, [_vp, _vp, _vp, C.c_uint64]),
             "ref_count": (C.c_uint64, [_vp]),
+            "ref_remove": (C.c_int, [_vp, C.c_uint64]),
+            "ref_stage_span": (C.c_int, [_vp, C.c_int, C.c_int, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64]),
             "ref_set_vec": (C.c_int, [_vp, C.c_int, _vp]),
             "ref_get_vec": (C.c_int, [_vp, C.c_int, _vp]),
             "ref_get_scalar": (C.c_int, [_vp, C.c_int, _vp]),

@@ -181,7 +181,7 @@ __global__ void k_permute_w_in(int n, const float* __restrict__ src, const uint3
 // apply_external_forces (particles.h:263-270)
 __global__ void k_external(Dev P, int n, float4* vel) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
-  if (a >= n) return;
+  if (a >= n || !pbf::in_span(P, a)) return;
   vel[a].y = pbf::xadd(vel[a].y, P.gdt);
 }
 
@@ -197,7 +197,7 @@ __device__ __forceinline__ float3 predict(const Dev& P, const pbf::Region& R, fl
 __global__ void k_predict(Dev P, int n, const float4* __restrict__ pos, const float4* __restrict__ vel,
                           float4* pst) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
-  if (a >= n) return;
+  if (a >= n || !pbf::in_span(P, a)) return;
   const float3 s = predict(P, pbf::region_of(P, a), pos[a], vel[a]);
   pst[a] = make_float4(s.x, s.y, s.z, 0.0f);
 }
@@ -680,6 +680,10 @@ __global__ void __launch_bounds__(kBlock) k_density(Dev P, int n, size_t stride,
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= n) return;
   float4 xp = pst[b];
+  if (!pbf::in_span(P, b)) {  // outside the span: x* and rho stay
+    pst_out[b] = xp;
+    return;
+  }
   const int c = cnt[b];
   float rho = pbf::M<X>(P.m, P.W0);
   bool nudged = false;
@@ -730,7 +734,7 @@ __global__ void __launch_bounds__(kBlock) k_lambda(Dev P, int n, size_t stride, 
                                                    const int32_t* __restrict__ cnt, const float4* __restrict__ pst,
                                                    const float4* __restrict__ vel, float* lam) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= n) return;
+  if (b >= n || !pbf::in_span(P, b)) return;
   const float4 xp = pst[b];
   const int c = cnt[b];
   float3 sg = make_float3(0.f, 0.f, 0.f);
@@ -1260,7 +1264,7 @@ __global__ void __launch_bounds__(kBlock) k_dp(Dev P, int n, size_t stride, cons
                                                const int32_t* __restrict__ cnt, const float4* __restrict__ pst,
                                                const float* __restrict__ lam, float4* scr) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= n) return;
+  if (b >= n || !pbf::in_span(P, b)) return;
   const float4 xp = pst[b];
   const float lp = lam[b];
   const int c = cnt[b];
@@ -1277,7 +1281,7 @@ __global__ void __launch_bounds__(kBlock) k_dp(Dev P, int n, size_t stride, cons
 // update_position_stars (particles.h:363-370), per-stage.
 __global__ void k_update_xs(Dev P, int n, float4* pst, const float4* __restrict__ scr) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= n) return;
+  if (b >= n || !pbf::in_span(P, b)) return;
   const float4 x = pst[b], d = scr[b];
   const float3 s = pbf::boundary(P, pbf::region_of(P, b),
                                  make_float3(pbf::xadd(x.x, d.x), pbf::xadd(x.y, d.y), pbf::xadd(x.z, d.z)));
@@ -1295,9 +1299,22 @@ __device__ __forceinline__ float3 velocity_of(const Dev& P, float4 xs, float4 x)
 __global__ void k_update_v(Dev P, int n, const float4* __restrict__ pst, const float4* __restrict__ pos,
                            float4* vel) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= n) return;
+  if (b >= n || !pbf::in_span(P, b)) return;
   const float3 v = velocity_of(P, pst[b], pos[b]);
   vel[b] = make_float4(v.x, v.y, v.z, vel[b].w);
+}
+
+// update_positions (particles.h:390-394) over a span: x = x* inside it.
+__global__ void k_update_positions(Dev P, int n, const float4* __restrict__ pst, float4* pos) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n || !pbf::in_span(P, b)) return;
+  pos[b] = pst[b];
+}
+
+// Empty neighbor lists for the particles outside a fill span.
+__global__ void k_clear_outside_span(int n, const uint32_t* __restrict__ orig, uint32_t end, int32_t* cnt) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < n && orig[b] >= end) cnt[b] = 0;
 }
 
 // Fused delta-p + x* update (+ velocity update on the last iteration): reads
@@ -1346,7 +1363,7 @@ __global__ void __launch_bounds__(kBlock) k_color(Dev P, int n, size_t stride, c
                                                   const int32_t* __restrict__ cnt, const float4* __restrict__ pst,
                                                   const float4* __restrict__ vel, float4* scr) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= n) return;
+  if (b >= n || !pbf::in_span(P, b)) return;
   const float4 xp = pst[b];
   const int c = cnt[b];
   float3 col = make_float3(0.f, 0.f, 0.f);
@@ -1368,7 +1385,7 @@ __global__ void __launch_bounds__(kBlock) k_surface(Dev P, int n, size_t stride,
                                                     const int32_t* __restrict__ cnt, const float4* __restrict__ pst,
                                                     const float4* __restrict__ scr, float4* vel) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= n) return;
+  if (b >= n || !pbf::in_span(P, b)) return;
   const float4 xp = pst[b], sp = scr[b];
   const float rp = vel[b].w;
   const int c = cnt[b];
@@ -1406,6 +1423,10 @@ __global__ void __launch_bounds__(kBlock) k_viscosity(Dev P, int n, size_t strid
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= n) return;
   const float4 xp = pst[b], vp = vin[b];
+  if (!FINAL && !pbf::in_span(P, b)) {  // outside the span: v stays
+    vout[b] = vp;
+    return;
+  }
   const int c = cnt[b];
   float3 dv = make_float3(0.f, 0.f, 0.f);
   for (int k = 0; k < c; ++k) {
@@ -1440,7 +1461,7 @@ __global__ void __launch_bounds__(kBlock) k_vorticity(Dev P, int n, size_t strid
                                                       const int32_t* __restrict__ cnt, const float4* __restrict__ pst,
                                                       const float4* __restrict__ vel, float4* scr, float4* xl) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= n) return;
+  if (b >= n || !pbf::in_span(P, b)) return;
   const float4 xp = pst[b], vp = vel[b];
   const int c = cnt[b];
   float3 w = make_float3(0.f, 0.f, 0.f);
@@ -1470,7 +1491,7 @@ __global__ void __launch_bounds__(kBlock) k_apply_vorticity(Dev P, int n, size_t
                                                             const float4* __restrict__ pst,
                                                             const float4* __restrict__ scr, float4* vel) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= n) return;
+  if (b >= n || !pbf::in_span(P, b)) return;
   const float4 xp = PACKED ? xl[b] : pst[b];
   const int c = cnt[b];
   float3 eta = make_float3(0.f, 0.f, 0.f);
@@ -1975,6 +1996,7 @@ int make_dev(pbf_ctx* ctx, const pbf_params& p, Dev& d, int64_t dims[3]) {
   const double nb = (double)dims[0] * (double)dims[1] * (double)dims[2];
   if (nb >= 2147483647.0) return fail(ctx, PBF_ERR_PARAMS, "grid of %.0f bins exceeds 2^31", nb);
   std::memset(&d, 0, sizeof(d));
+  d.span_end = 0xffffffffu;
   const float h = p.smoothing_radius;
   d.dt = p.time_step;
   d.gdt = p.gravity * p.time_step;
@@ -2108,10 +2130,24 @@ void drop_graphs(pbf_ctx* ctx) {
   ctx->graphs.clear();
 }
 
+// Stage spans are [0, e) with e <= n: the particles of reference index below
+// e (a multi-rank driver's resident particles, Simulation/Source/main.adios);
+// the others are halo particles the stage reads but leaves as they are.
 int check_span(pbf_ctx* ctx, size_t b, size_t e) {
-  if (b != 0 || e != ctx->n)
-    return fail(ctx, PBF_ERR_SPAN, "span [%zu, %zu) given; a single rank supports only [0, %zu)", b, e, ctx->n);
+  if (b != 0 || e > ctx->n)
+    return fail(ctx, PBF_ERR_SPAN, "span [%zu, %zu) given; spans are [0, e) with e <= %zu particles", b, e,
+                ctx->n);
   return PBF_OK;
+}
+
+// The constant block of a per-stage call over the span [0, e).
+Dev span_dev(const pbf_ctx* ctx, size_t e) {
+  Dev d = ctx->dev;
+  if (e < ctx->n) {
+    d.span_orig = ctx->origH;
+    d.span_end = (uint32_t)e;
+  }
+  return d;
 }
 
 int need_lists(pbf_ctx* ctx) {
@@ -3111,17 +3147,19 @@ int pbf_download(pbf_ctx* ctx, float* x, float* v, float* rho, float* lambda) {
   const int g = blocks_for(ctx->n);       \
   (void)g;                                \
   const bool X = ctx->params.exact_math != 0; \
-  (void)X;
+  (void)X;                                \
+  const Dev SP = span_dev(ctx, e);        \
+  (void)SP;
 
 int pbf_apply_external_forces(pbf_ctx* ctx, size_t b, size_t e) {
   STAGE_PROLOGUE(b, e);
-  k_external<<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->velH);
+  k_external<<<g, kBlock, 0, ctx->stream>>>(SP, n, ctx->velH);
   return check_launch(ctx, "apply_external_forces");
 }
 
 int pbf_predict_positions(pbf_ctx* ctx, size_t b, size_t e) {
   STAGE_PROLOGUE(b, e);
-  k_predict<<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->posH, ctx->velH, ctx->pstH);
+  k_predict<<<g, kBlock, 0, ctx->stream>>>(SP, n, ctx->posH, ctx->velH, ctx->pstH);
   return check_launch(ctx, "predict_positions");
 }
 
@@ -3130,6 +3168,9 @@ int pbf_find_neighbors(pbf_ctx* ctx, size_t bin_b, size_t bin_e, size_t fill_b, 
   int rc = check_span(ctx, bin_b, bin_e);
   if (rc) return rc;
   if ((rc = check_span(ctx, fill_b, fill_e))) return rc;
+  if (bin_e != ctx->n)
+    return fail(ctx, PBF_ERR_SPAN, "find_neighbors bins every held particle: bin span [0, %zu) given, [0, %zu) held",
+                bin_e, ctx->n);
   if (ctx->n == 0) {
     ctx->lists_valid = true;
     return PBF_OK;
@@ -3151,6 +3192,8 @@ int pbf_find_neighbors(pbf_ctx* ctx, size_t bin_b, size_t bin_e, size_t fill_b, 
   CK(cudaMemcpyAsync(ctx->lamH, ctx->lamS, sizeof(float) * ctx->n, cudaMemcpyDeviceToDevice, s));
   CK(cudaMemcpyAsync(ctx->origH, ctx->origS, sizeof(uint32_t) * ctx->n, cudaMemcpyDeviceToDevice, s));
   launch_fill(ctx, ctx->pstH);
+  if (fill_e < ctx->n)  // particles outside the fill span (halo particles) get empty lists
+    k_clear_outside_span<<<g, kBlock, 0, s>>>(n, ctx->origH, (uint32_t)fill_e, ctx->cnt);
   rc = check_launch(ctx, "find_neighbors");
   if (rc) return rc;
   ctx->lists_valid = true;
@@ -3160,8 +3203,8 @@ int pbf_find_neighbors(pbf_ctx* ctx, size_t bin_b, size_t bin_e, size_t fill_b, 
 int pbf_compute_densities(pbf_ctx* ctx, size_t b, size_t e) {
   STAGE_PROLOGUE(b, e);
   if (int rc = need_lists(ctx)) return rc;
-  if (X) k_density<true><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->pstS);
-  else k_density<false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->pstS);
+  if (X) k_density<true><<<g, kBlock, 0, ctx->stream>>>(SP, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->pstS);
+  else k_density<false><<<g, kBlock, 0, ctx->stream>>>(SP, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->pstS);
   CK(cudaMemcpyAsync(ctx->pstH, ctx->pstS, sizeof(float4) * ctx->n, cudaMemcpyDeviceToDevice, ctx->stream));
   return check_launch(ctx, "compute_densities");
 }
@@ -3169,8 +3212,8 @@ int pbf_compute_densities(pbf_ctx* ctx, size_t b, size_t e) {
 int pbf_compute_pressure_lambdas(pbf_ctx* ctx, size_t b, size_t e) {
   STAGE_PROLOGUE(b, e);
   if (int rc = need_lists(ctx)) return rc;
-  if (X) k_lambda<true><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->lamH);
-  else k_lambda<false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->lamH);
+  if (X) k_lambda<true><<<g, kBlock, 0, ctx->stream>>>(SP, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->lamH);
+  else k_lambda<false><<<g, kBlock, 0, ctx->stream>>>(SP, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->lamH);
   return check_launch(ctx, "compute_pressure_lambdas");
 }
 
@@ -3179,7 +3222,7 @@ int pbf_compute_pressure_dps(pbf_ctx* ctx, size_t b, size_t e, int substep) {
   STAGE_PROLOGUE(b, e);
   if (int rc = need_lists(ctx)) return rc;
   const bool SC = ctx->params.scorr_k > 0.0f;
-  const Dev& P = ctx->dev;
+  const Dev& P = SP;
   if (X && SC) k_dp<true, true><<<g, kBlock, 0, ctx->stream>>>(P, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->lamH, ctx->scrH);
   else if (X) k_dp<true, false><<<g, kBlock, 0, ctx->stream>>>(P, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->lamH, ctx->scrH);
   else if (SC) k_dp<false, true><<<g, kBlock, 0, ctx->stream>>>(P, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->lamH, ctx->scrH);
@@ -3189,13 +3232,13 @@ int pbf_compute_pressure_dps(pbf_ctx* ctx, size_t b, size_t e, int substep) {
 
 int pbf_update_position_stars(pbf_ctx* ctx, size_t b, size_t e) {
   STAGE_PROLOGUE(b, e);
-  k_update_xs<<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->pstH, ctx->scrH);
+  k_update_xs<<<g, kBlock, 0, ctx->stream>>>(SP, n, ctx->pstH, ctx->scrH);
   return check_launch(ctx, "update_position_stars");
 }
 
 int pbf_update_velocities(pbf_ctx* ctx, size_t b, size_t e) {
   STAGE_PROLOGUE(b, e);
-  k_update_v<<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->pstH, ctx->posH, ctx->velH);
+  k_update_v<<<g, kBlock, 0, ctx->stream>>>(SP, n, ctx->pstH, ctx->posH, ctx->velH);
   return check_launch(ctx, "update_velocities");
 }
 
@@ -3204,17 +3247,17 @@ int pbf_apply_surface_tension(pbf_ctx* ctx, size_t cb, size_t ce, size_t sb, siz
   if (int rc = check_span(ctx, sb, se)) return rc;
   STAGE_PROLOGUE(cb, ce);
   if (int rc = need_lists(ctx)) return rc;
-  if (X) k_color<true><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->scrH);
-  else k_color<false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->scrH);
-  k_surface<<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->scrH, ctx->velH);
+  if (X) k_color<true><<<g, kBlock, 0, ctx->stream>>>(SP, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->scrH);
+  else k_color<false><<<g, kBlock, 0, ctx->stream>>>(SP, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->scrH);
+  k_surface<<<g, kBlock, 0, ctx->stream>>>(span_dev(ctx, se), n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->scrH, ctx->velH);
   return check_launch(ctx, "apply_surface_tension");
 }
 
 int pbf_apply_viscosity(pbf_ctx* ctx, size_t b, size_t e) {
   STAGE_PROLOGUE(b, e);
   if (int rc = need_lists(ctx)) return rc;
-  if (X) k_viscosity<true, false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->velT, nullptr, nullptr, nullptr, nullptr);
-  else k_viscosity<false, false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->velT, nullptr, nullptr, nullptr, nullptr);
+  if (X) k_viscosity<true, false><<<g, kBlock, 0, ctx->stream>>>(SP, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->velT, nullptr, nullptr, nullptr, nullptr);
+  else k_viscosity<false, false><<<g, kBlock, 0, ctx->stream>>>(SP, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->velT, nullptr, nullptr, nullptr, nullptr);
   CK(cudaMemcpyAsync(ctx->velH, ctx->velT, sizeof(float4) * ctx->n, cudaMemcpyDeviceToDevice, ctx->stream));
   return check_launch(ctx, "apply_viscosity");
 }
@@ -3222,23 +3265,27 @@ int pbf_apply_viscosity(pbf_ctx* ctx, size_t b, size_t e) {
 int pbf_compute_vorticity(pbf_ctx* ctx, size_t b, size_t e) {
   STAGE_PROLOGUE(b, e);
   if (int rc = need_lists(ctx)) return rc;
-  if (X) k_vorticity<true><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->scrH, nullptr);
-  else k_vorticity<false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->scrH, nullptr);
+  if (X) k_vorticity<true><<<g, kBlock, 0, ctx->stream>>>(SP, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->scrH, nullptr);
+  else k_vorticity<false><<<g, kBlock, 0, ctx->stream>>>(SP, n, ctx->lstride, ctx->nbr, ctx->cnt, ctx->pstH, ctx->velH, ctx->scrH, nullptr);
   return check_launch(ctx, "compute_vorticity");
 }
 
 int pbf_apply_vorticity(pbf_ctx* ctx, size_t b, size_t e) {
   STAGE_PROLOGUE(b, e);
   if (int rc = need_lists(ctx)) return rc;
-  if (X) k_apply_vorticity<true, false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->lstride, ctx->nbr, ctx->cnt, nullptr, ctx->pstH, ctx->scrH, ctx->velH);
-  else k_apply_vorticity<false, false><<<g, kBlock, 0, ctx->stream>>>(ctx->dev, n, ctx->lstride, ctx->nbr, ctx->cnt, nullptr, ctx->pstH, ctx->scrH, ctx->velH);
+  if (X) k_apply_vorticity<true, false><<<g, kBlock, 0, ctx->stream>>>(SP, n, ctx->lstride, ctx->nbr, ctx->cnt, nullptr, ctx->pstH, ctx->scrH, ctx->velH);
+  else k_apply_vorticity<false, false><<<g, kBlock, 0, ctx->stream>>>(SP, n, ctx->lstride, ctx->nbr, ctx->cnt, nullptr, ctx->pstH, ctx->scrH, ctx->velH);
   return check_launch(ctx, "apply_vorticity");
 }
 
 int pbf_update_positions(pbf_ctx* ctx, size_t b, size_t e) {
   STAGE_PROLOGUE(b, e);
-  CK(cudaMemcpyAsync(ctx->posH, ctx->pstH, sizeof(float4) * (size_t)n, cudaMemcpyDeviceToDevice, ctx->stream));
-  return PBF_OK;
+  if (e == ctx->n) {
+    CK(cudaMemcpyAsync(ctx->posH, ctx->pstH, sizeof(float4) * (size_t)n, cudaMemcpyDeviceToDevice, ctx->stream));
+    return PBF_OK;
+  }
+  k_update_positions<<<g, kBlock, 0, ctx->stream>>>(SP, n, ctx->pstH, ctx->posH);
+  return check_launch(ctx, "update_positions");
 }
 
 int pbf_step(pbf_ctx* ctx, int nsteps) {

@@ -46,7 +46,18 @@ struct Dev {
   const Region* scenes;
   const uint32_t* scene_first;
   int nscenes;
+  // span of a per-stage call ([0, span_end) in reference index space, the
+  // multi-rank driver's resident span): a stage updates the particles whose
+  // reference index (span_orig of the slot) is below span_end and leaves the
+  // others (halo particles) as they are; span_end = 0xffffffff is every particle
+  const uint32_t* span_orig;
+  uint32_t span_end;
 };
+
+// Whether the particle in home slot `i` is inside the stage's span.
+__device__ __forceinline__ bool in_span(const Dev& P, int i) {
+  return P.span_end == 0xffffffffu || __ldg(P.span_orig + i) < P.span_end;
+}
 
 // The region of the particle in `slot` (any order the step uses).
 __device__ __forceinline__ Region region_of(const Dev& P, int slot) {

@@ -66,6 +66,32 @@ class Particles:
             v = np.ascontiguousarray(v, dtype=np.float32).reshape(-1, 3)
         self._check(self._lib.pbf_add_particles(self._ctx, _ptr(x), _ptr(v), x.shape[0]), "add_particles")
 
+    def append(self, x: np.ndarray, x_star: np.ndarray, v: np.ndarray) -> None:
+        """Particles::add (particles.h:184-199): append particles with their own
+        x, x* and v (the multi-rank driver's arrivals and halos)."""
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, 3)
+        if x.shape[0] == 0:
+            return
+        n0 = self.local_count()
+        self.add_particles(x, np.ascontiguousarray(v, np.float32).reshape(-1, 3))
+        xs = self.position_stars()
+        xs[n0:] = x_star
+        self.set_array(_abi.ARRAY_POSITION_STARS, xs)
+
+    def remove(self, k: int) -> None:
+        """Particles::remove (particles.h:146-154): drop the last k particles
+        (reference order); x, x* and v of the others are kept (density, lambda
+        and scratch are recomputed by the stages before they are read)."""
+        if k <= 0:
+            return
+        keep = self.local_count() - int(k)
+        if keep < 0:
+            raise RuntimeError("remove: more particles than held")
+        x, xs, v = self.positions()[:keep], self.position_stars()[:keep], self.velocities()[:keep]
+        self.upload(x, v)
+        if keep:
+            self.set_array(_abi.ARRAY_POSITION_STARS, xs)
+
     def construct_fluid(self, fluid_min, fluid_max, velocity=(0.0, 0.0, 0.0)) -> int:
         """Particles::construct_fluid: append the lattice of the box; returns the count added."""
         mn, mx, vel = (C.c_float * 3)(*fluid_min), (C.c_float * 3)(*fluid_max), (C.c_float * 3)(*velocity)

@@ -325,7 +325,9 @@ def test_errors_are_reported_not_faulted():
         g.upload(np.zeros((101, 3), np.float32))
     g.upload(sc.positions()[:100])
     with pytest.raises(RuntimeError, match="span"):
-        g.apply_external_forces((0, 50))
+        g.apply_external_forces((10, 50))   # spans start at 0
+    with pytest.raises(RuntimeError, match="span"):
+        g.apply_external_forces((0, 101))   # past the held particles
     with pytest.raises(RuntimeError, match="neighbor lists"):
         g.compute_densities()
     g.find_neighbors()
