@@ -65,6 +65,9 @@ def parse_args():
     ap.add_argument("--profile-learned", type=int, default=0, metavar="K",
                     help="only run K steps of the learned warm start (eps 1, after its warm-up) and print "
                          "ms/step: the command the learned kernels' ncu summaries are captured from")
+    ap.add_argument("--learned-iterations", type=int, default=10,
+                    help="iteration cap of --profile-learned (1: no conditional loop in the step's graph, "
+                         "which ncu needs to profile the graph's kernels)")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the 16.8M dam, the 200-step trajectory and the s_corr run")
     return ap.parse_args()
@@ -365,11 +368,16 @@ def learned_comparison(scene_name: str, steps: int, warmup: int, target: float =
 # ---------------------------------------------------------------- batched scenes
 def batched_run(steps: int = 200, autotune: bool = True) -> dict:
     """The 64-scene batch (make_batch: counts log-uniform in [4096, 262144])
-    advanced `steps` steps from its initial state by ONE graph launch
-    (pbf_step(ctx, steps); the graph is captured by an untimed run of the same
-    call first), against the same scenes and the same steps as 64
-    single-scene contexts, each replaying its own one-step graph on its own
-    stream (the streams run concurrently)."""
+    advanced `steps` steps from its initial state by ONE graph launch, in two
+    forms, against the same scenes and steps as 64 single-scene contexts each
+    replaying its own one-step graph on its own stream (the streams run
+    concurrently):
+      value        the scene group: one graph launch whose members are the
+                   64 contexts' `steps`-step chains (pbf_group_step), each
+                   scene advancing at its own pace;
+      one_context  one context holding all scenes (pbf_create_batch), every
+                   launch covering every scene (pbf_step(ctx, steps)).
+    Each graph is captured by an untimed run of the same call first."""
     import numpy as np
     import torch
     from pbf_b200 import Particles, make_batch
@@ -428,13 +436,40 @@ def batched_run(steps: int = 200, autotune: bool = True) -> dict:
         for e in ends:
             e.synchronize()
         ts = max(e0.elapsed_time(e) for e in ends) / 1e3
+        out_ind = {"value": b.n * steps / ts, "ms_per_step": 1e3 * ts / steps,
+                   "steps": steps, "graph_launches_per_step": len(b.scenes)}
+        # the same contexts as one scene group: one graph launch of every scene's
+        # `steps`-step chain, each scene at its own pace (pbf_group_step)
+        from pbf_b200 import SceneGroup
+        for c, sc in zip(ctxs, b.scenes):
+            c.upload(sc.positions())
+        with SceneGroup(ctxs) as grp:
+            grp.step(steps)           # captures and instantiates the group's graph (untimed)
+            grp.sync()
+            for c, sc in zip(ctxs, b.scenes):
+                c.upload(sc.positions())
+            torch.cuda.synchronize()
+            gs = torch.cuda.ExternalStream(grp.stream_handle())
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(gs)
+            grp.step(steps)
+            e1.record(gs)
+            e1.synchronize()
+            tg = e0.elapsed_time(e1) / 1e3
+        group_flags = max(c.stats()["error_flags"] for c in ctxs)
     finally:
         for c in ctxs:
             c.close()
-    out["independent_contexts"] = {"value": b.n * steps / ts, "ms_per_step": 1e3 * ts / steps,
-                                   "steps": steps, "graph_launches_per_step": len(b.scenes)}
-    out["speedup_vs_independent"] = out["value"] / out["independent_contexts"]["value"]
-    return out
+    one_context = {k: out[k] for k in ("value", "ms_per_step", "graph_launches", "kernel_launches_per_step",
+                                       "scene_mean_density_error", "error_flags")}
+    one_context["speedup_vs_independent"] = one_context["value"] / out_ind["value"]
+    res = {"workload": out["workload"], "mode": "scene group: one graph launch of every scene's step chain, "
+                                                "each scene at its own pace (pbf_group_step)",
+           "value": b.n * steps / tg, "unit": UNIT, "steps": steps, "ms_per_step": 1e3 * tg / steps,
+           "graph_launches": 1, "tuning": tuning, "error_flags": group_flags,
+           "independent_contexts": out_ind, "speedup_vs_independent": (b.n * steps / tg) / out_ind["value"],
+           "one_context": one_context}
+    return res
 
 
 # ---------------------------------------------------------------- more workloads
@@ -504,7 +539,8 @@ def main():
     if args.profile_learned:
         from pbf_b200.learn import DEFAULT_MODEL, load_model, warm_start_scene
         params, norm, _ = load_model(DEFAULT_MODEL)
-        sc = warm_start_scene(args.scene, seed=4242).with_(solver=1, residual_tol=0.01, max_iterations=10)
+        sc = warm_start_scene(args.scene, seed=4242).with_(solver=1, residual_tol=0.01,
+                                                           max_iterations=args.learned_iterations)
         r = solver_run(sc, args.profile_learned, args.warmup, params, norm, autotune=False)
         print(json.dumps({"learned_ms_per_step": r["ms_per_step"], "iterations": r["mean_iterations"],
                           "kernel_ms_per_step": r["kernel_ms_per_step"]}), flush=True)

@@ -383,6 +383,23 @@ int pbf_mlp_predict(pbf_ctx* ctx, const float* features, size_t n, float* y);
  * (pbf_mlp_init or pbf_mlp_set) and a capacity of at least 278 particles. */
 int pbf_selftest_mlp_wait_timeout(pbf_ctx* ctx, uint32_t* flags);
 
+/* ---- scene groups ----
+ * No counterpart in the reference.  Independent contexts (one scene each)
+ * advanced together by ONE graph launch: the graph holds every member's
+ * nsteps-step chain as a child graph, with no dependency between members, so
+ * each scene advances at its own pace.  Each member's results are its own
+ * pbf_step results, bit for bit.  The launch runs on the group's stream,
+ * after each member's pending work; each member's later work waits for it.
+ * Members must have per-kernel timing off; the graph is cached per nsteps and
+ * rebuilt when a member's particle count or parameters change.  Members stay
+ * owned by the caller and must outlive the group. */
+typedef struct pbf_group pbf_group;
+int pbf_group_create(pbf_ctx* const* ctxs, int n, pbf_group** out);
+int pbf_group_step(pbf_group* g, int nsteps);
+int pbf_group_sync(pbf_group* g);
+int pbf_group_get_stream(pbf_group* g, void** stream_out);
+void pbf_group_destroy(pbf_group* g);
+
 /* ---- neighbor search that allocates nothing ----
  * No counterpart in the reference.  For callers that may not allocate device
  * memory: hosts that own every device allocation (their own pool or a fixed

@@ -1082,7 +1082,10 @@ __global__ void __launch_bounds__(pbf::tc::kThreads, 6) kl_mlp_tc(pbf::MlpDev M,
   __shared__ __align__(1024) uint8_t sB2[pbf::kMlpH * pbf::kMlpH * 2];      // W2 [64 n][64 k]
   __shared__ __align__(1024) uint8_t sA1[T::kRows * pbf::kMlpInPad * 2];    // features [128][16]
   __shared__ __align__(1024) uint8_t sA2[T::kRows * pbf::kMlpH * 2];        // hidden 1 [128][64]
-  __shared__ float sb1[pbf::kMlpH], sb2[pbf::kMlpH], sw3[pbf::kMlpH], half2[T::kRows];
+  __shared__ __align__(16) float sb1[pbf::kMlpH];  // read as float2 pairs
+  __shared__ __align__(16) float sb2[pbf::kMlpH];
+  __shared__ __align__(16) float sw3[pbf::kMlpH];
+  __shared__ float half2[T::kRows];
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tslot;
   __shared__ int fail;
@@ -1160,12 +1163,14 @@ __global__ void __launch_bounds__(pbf::tc::kThreads, 6) kl_mlp_tc(pbf::MlpDev M,
       const int c0 = 32 * h + c;
 #pragma unroll
       for (int j = 0; j < 16; j += 8) {
-        uint4 w;
-        w.x = pbf::pack_bf16x2(pbf::gelu(v[j] + sb1[c0 + j]), pbf::gelu(v[j + 1] + sb1[c0 + j + 1]));
-        w.y = pbf::pack_bf16x2(pbf::gelu(v[j + 2] + sb1[c0 + j + 2]), pbf::gelu(v[j + 3] + sb1[c0 + j + 3]));
-        w.z = pbf::pack_bf16x2(pbf::gelu(v[j + 4] + sb1[c0 + j + 4]), pbf::gelu(v[j + 5] + sb1[c0 + j + 5]));
-        w.w = pbf::pack_bf16x2(pbf::gelu(v[j + 6] + sb1[c0 + j + 6]), pbf::gelu(v[j + 7] + sb1[c0 + j + 7]));
-        *reinterpret_cast<uint4*>(sA2 + T::core_off(row, c0 + j, pbf::kMlpH)) = w;
+        uint32_t wq[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const float2 b = *reinterpret_cast<const float2*>(sb1 + c0 + j + 2 * k);
+          const float2 g = pbf::gelu2(__fadd2_rn(make_float2(v[j + 2 * k], v[j + 2 * k + 1]), b));
+          wq[k] = pbf::pack_bf16x2(g.x, g.y);
+        }
+        *reinterpret_cast<uint4*>(sA2 + T::core_off(row, c0 + j, pbf::kMlpH)) = make_uint4(wq[0], wq[1], wq[2], wq[3]);
       }
     }
     T::fence_proxy_async();
@@ -1186,15 +1191,20 @@ __global__ void __launch_bounds__(pbf::tc::kThreads, 6) kl_mlp_tc(pbf::MlpDev M,
     __syncthreads();
     if (fail) break;
     T::fence_after_sync();
-    float acc = 0.0f;
+    float2 acc2 = make_float2(0.0f, 0.0f);
 #pragma unroll
     for (int c = 0; c < 32; c += 16) {
       float v[16];
       T::tmem_ld16(lanes + (uint32_t)c, v);
       const int c0 = 32 * h + c;
 #pragma unroll
-      for (int q = 0; q < 16; ++q) acc = fmaf(pbf::gelu(v[q] + sb2[c0 + q]), sw3[c0 + q], acc);
+      for (int q = 0; q < 16; q += 2) {
+        const float2 b = *reinterpret_cast<const float2*>(sb2 + c0 + q);
+        const float2 w3 = *reinterpret_cast<const float2*>(sw3 + c0 + q);
+        acc2 = __ffma2_rn(pbf::gelu2(__fadd2_rn(make_float2(v[q], v[q + 1]), b)), w3, acc2);
+      }
     }
+    const float acc = acc2.x + acc2.y;
     if (h == 0) half2[row] = acc;
     T::fence_before_sync();
     __syncthreads();  // the first halves in shared memory; TMEM and operands free for the next tile
@@ -1918,6 +1928,7 @@ struct pbf_ctx {
   uint32_t* d_scene_first = nullptr;
 
   std::map<int, cudaGraphExec_t> graphs;
+  uint64_t graph_epoch = 0;  // counts drop_graphs: a scene group rebuilds when a member's changes
   std::vector<void*> allocations;
 
   bool timing = false;
@@ -2128,6 +2139,7 @@ int dalloc(pbf_ctx* ctx, T** ptr, size_t count) {
 void drop_graphs(pbf_ctx* ctx) {
   for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
   ctx->graphs.clear();
+  ctx->graph_epoch++;
 }
 
 // Stage spans are [0, e) with e <= n: the particles of reference index below
@@ -3288,6 +3300,26 @@ int pbf_update_positions(pbf_ctx* ctx, size_t b, size_t e) {
   return check_launch(ctx, "update_positions");
 }
 
+// nsteps fused steps captured from the context's stream into a graph (not
+// instantiated; the caller owns it).
+static int capture_steps(pbf_ctx* ctx, int nsteps, cudaGraph_t* out) {
+  cudaGraph_t graph = nullptr;
+  ctx->capture_failed = false;
+  CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  for (int i = 0; i < nsteps; ++i) launch_step(ctx);
+  cudaError_t le = cudaGetLastError();
+  cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
+  if (le != cudaSuccess || ce != cudaSuccess || ctx->capture_failed) {
+    if (graph) cudaGraphDestroy(graph);
+    const bool loop = ctx->capture_failed;
+    ctx->capture_failed = false;
+    if (loop) return fail(ctx, PBF_ERR_CUDA, "graph capture of the learned solver's iteration loop failed");
+    return fail(ctx, PBF_ERR_CUDA, "graph capture failed: %s / %s", cudaGetErrorString(le), cudaGetErrorString(ce));
+  }
+  *out = graph;
+  return PBF_OK;
+}
+
 int pbf_step(pbf_ctx* ctx, int nsteps) {
   if (!ctx || nsteps < 0) return PBF_ERR_ARG;
   if (nsteps == 0) return PBF_OK;
@@ -3308,19 +3340,7 @@ int pbf_step(pbf_ctx* ctx, int nsteps) {
   auto it = ctx->graphs.find(nsteps);
   if (it == ctx->graphs.end()) {
     cudaGraph_t graph = nullptr;
-    ctx->capture_failed = false;
-    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    for (int i = 0; i < nsteps; ++i) launch_step(ctx);
-    cudaError_t le = cudaGetLastError();
-    cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
-    if (le != cudaSuccess || ce != cudaSuccess || ctx->capture_failed) {
-      if (graph) cudaGraphDestroy(graph);
-      const bool loop = ctx->capture_failed;
-      ctx->capture_failed = false;
-      if (loop) return fail(ctx, PBF_ERR_CUDA, "graph capture of the learned solver's iteration loop failed");
-      return fail(ctx, PBF_ERR_CUDA, "graph capture failed: %s / %s", cudaGetErrorString(le),
-                  cudaGetErrorString(ce));
-    }
+    if (int rc = capture_steps(ctx, nsteps, &graph)) return rc;
     cudaGraphExec_t exec = nullptr;
     cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
     cudaGraphDestroy(graph);
@@ -3330,6 +3350,139 @@ int pbf_step(pbf_ctx* ctx, int nsteps) {
   CK(cudaGraphLaunch(it->second, ctx->stream));
   ctx->lists_valid = true;
   return PBF_OK;
+}
+
+// ---- scene groups: independent contexts advanced by one graph launch ----
+// The group's graph holds, per member context, its nsteps-step chain as a
+// child graph, with no edge between members: one launch, and every scene
+// advances at its own pace (a light scene's steps run while a crowded one is
+// in its list fill), where the one-context batch ends every step when its
+// slowest scene ends.  Results are each context's own pbf_step results, bit
+// for bit.  The graph is cached per nsteps and rebuilt when a member drops its
+// graphs (a new particle count or new parameters).
+struct pbf_group {
+  std::vector<pbf_ctx*> ctxs;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  std::vector<cudaEvent_t> ready;
+  struct Built {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<uint64_t> epochs;
+  };
+  std::map<int, Built> graphs;
+};
+
+static void group_drop(pbf_group* g) {
+  for (auto& kv : g->graphs) cudaGraphExecDestroy(kv.second.exec);
+  g->graphs.clear();
+}
+
+int pbf_group_create(pbf_ctx* const* ctxs, int n, pbf_group** out) {
+  if (!out || !ctxs || n < 1) return fail(nullptr, PBF_ERR_ARG, "pbf_group_create: no contexts");
+  *out = nullptr;
+  for (int i = 0; i < n; ++i) {
+    if (!ctxs[i]) return fail(nullptr, PBF_ERR_ARG, "pbf_group_create: context %d is NULL", i);
+    for (int j = 0; j < i; ++j)
+      if (ctxs[j] == ctxs[i]) return fail(nullptr, PBF_ERR_ARG, "pbf_group_create: context %d listed twice", i);
+  }
+  auto* g = new pbf_group();
+  g->ctxs.assign(ctxs, ctxs + n);
+  cudaError_t e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->done, cudaEventDisableTiming);
+  g->ready.assign((size_t)n, nullptr);
+  for (int i = 0; i < n && e == cudaSuccess; ++i) e = cudaEventCreateWithFlags(&g->ready[i], cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    pbf_group_destroy(g);
+    return fail(nullptr, PBF_ERR_CUDA, "pbf_group_create: %s", cudaGetErrorString(e));
+  }
+  *out = g;
+  return PBF_OK;
+}
+
+int pbf_group_step(pbf_group* g, int nsteps) {
+  if (!g || nsteps < 0) return fail(nullptr, PBF_ERR_ARG, "pbf_group_step: bad arguments");
+  if (nsteps == 0) return PBF_OK;
+  for (pbf_ctx* c : g->ctxs) {
+    if (c->timing) return fail(nullptr, PBF_ERR_STATE, "pbf_group_step: a member has per-kernel timing on");
+    if (c->params.solver == 1 && !c->mlp_ready)
+      return fail(nullptr, PBF_ERR_STATE, "pbf_group_step: a learned-solver member has no network");
+  }
+  auto it = g->graphs.find(nsteps);
+  if (it != g->graphs.end()) {
+    bool stale = false;
+    for (size_t i = 0; i < g->ctxs.size(); ++i) stale = stale || it->second.epochs[i] != g->ctxs[i]->graph_epoch;
+    if (stale) {
+      cudaGraphExecDestroy(it->second.exec);
+      g->graphs.erase(it);
+      it = g->graphs.end();
+    }
+  }
+  if (it == g->graphs.end()) {
+    cudaGraph_t parent = nullptr;
+    if (cudaGraphCreate(&parent, 0) != cudaSuccess) return fail(nullptr, PBF_ERR_CUDA, "pbf_group_step: graph");
+    pbf_group::Built b;
+    for (pbf_ctx* c : g->ctxs) {
+      b.epochs.push_back(c->graph_epoch);
+      if (c->n == 0) continue;
+      cudaGraph_t child = nullptr;
+      if (int rc = capture_steps(c, nsteps, &child)) {
+        cudaGraphDestroy(parent);
+        return fail(nullptr, rc, "pbf_group_step: capture of a member failed: %s", pbf_last_error(c));
+      }
+      cudaGraphNode_t node = nullptr;
+      const cudaError_t e = cudaGraphAddChildGraphNode(&node, parent, nullptr, 0, child);
+      cudaGraphDestroy(child);  // the node holds its own copy
+      if (e != cudaSuccess) {
+        cudaGraphDestroy(parent);
+        return fail(nullptr, PBF_ERR_CUDA, "pbf_group_step: a member's steps cannot be a child graph (%s)",
+                    cudaGetErrorString(e));
+      }
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&b.exec, parent, 0);
+    cudaGraphDestroy(parent);
+    if (ie != cudaSuccess)
+      return fail(nullptr, PBF_ERR_CUDA, "pbf_group_step: graph instantiate failed: %s", cudaGetErrorString(ie));
+    it = g->graphs.emplace(nsteps, b).first;
+  }
+  // the launch follows each member's pending work, and each member's next work follows the launch
+  cudaError_t e = cudaSuccess;
+  for (size_t i = 0; i < g->ctxs.size() && e == cudaSuccess; ++i) {
+    e = cudaEventRecord(g->ready[i], g->ctxs[i]->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(g->stream, g->ready[i], 0);
+  }
+  if (e == cudaSuccess) e = cudaGraphLaunch(it->second.exec, g->stream);
+  if (e == cudaSuccess) e = cudaEventRecord(g->done, g->stream);
+  for (size_t i = 0; i < g->ctxs.size() && e == cudaSuccess; ++i) e = cudaStreamWaitEvent(g->ctxs[i]->stream, g->done, 0);
+  if (e != cudaSuccess) return fail(nullptr, PBF_ERR_CUDA, "pbf_group_step: launch: %s", cudaGetErrorString(e));
+  for (pbf_ctx* c : g->ctxs) {
+    if (c->n == 0) continue;
+    c->steps_done += (uint64_t)nsteps;
+    c->lists_valid = true;
+  }
+  return PBF_OK;
+}
+
+int pbf_group_sync(pbf_group* g) {
+  if (!g) return PBF_ERR_ARG;
+  const cudaError_t e = cudaStreamSynchronize(g->stream);
+  return e == cudaSuccess ? PBF_OK : fail(nullptr, PBF_ERR_CUDA, "pbf_group_sync: %s", cudaGetErrorString(e));
+}
+
+int pbf_group_get_stream(pbf_group* g, void** stream_out) {
+  if (!g || !stream_out) return PBF_ERR_ARG;
+  *stream_out = g->stream;
+  return PBF_OK;
+}
+
+void pbf_group_destroy(pbf_group* g) {
+  if (!g) return;
+  if (g->stream) cudaStreamSynchronize(g->stream);
+  group_drop(g);
+  for (cudaEvent_t e : g->ready)
+    if (e) cudaEventDestroy(e);
+  if (g->done) cudaEventDestroy(g->done);
+  if (g->stream) cudaStreamDestroy(g->stream);
+  delete g;
 }
 
 int pbf_sync(pbf_ctx* ctx) {

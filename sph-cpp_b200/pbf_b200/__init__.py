@@ -16,7 +16,8 @@ from . import _abi
 from ._abi import PbfParams, PbfStats  # noqa: F401
 from .scenes import SCENES, Batch, Scene, make_batch, make_scene  # noqa: F401
 
-__all__ = ["Particles", "PbfParams", "PbfStats", "Scene", "make_scene", "SCENES", "lib", "params_init"]
+__all__ = ["Particles", "PbfParams", "PbfStats", "Scene", "SceneGroup", "make_scene", "SCENES", "lib",
+           "params_init"]
 
 
 def lib() -> C.CDLL:
@@ -397,3 +398,47 @@ class Particles:
         table = {cand: {f: float(ms[c * nf + i]) for i, f in enumerate(_abi.TUNE_FAMILIES)}
                  for c, cand in enumerate(_abi.TUNE_CANDIDATES)}
         return t.as_dict(), table
+
+
+class SceneGroup:
+    """Independent contexts (one scene each) advanced together by one graph
+    launch (pbf_group_*): every scene's step chain is a child graph of the
+    launch, with no dependency between scenes, so each advances at its own
+    pace; each context's results are its own `step` results, bit for bit."""
+
+    def __init__(self, contexts):
+        self._lib = lib()
+        self.contexts = list(contexts)
+        arr = (C.c_void_p * len(self.contexts))(*[c.ctx.value for c in self.contexts])
+        self._g = C.c_void_p()
+        rc = self._lib.pbf_group_create(arr, len(self.contexts), C.byref(self._g))
+        if rc != 0:
+            raise RuntimeError(f"pbf_group_create failed ({rc}): {self._lib.pbf_last_error(None).decode()}")
+
+    def step(self, nsteps: int = 1) -> None:
+        rc = self._lib.pbf_group_step(self._g, int(nsteps))
+        if rc != 0:
+            raise RuntimeError(f"pbf_group_step failed ({rc}): {self._lib.pbf_last_error(None).decode()}")
+
+    def sync(self) -> None:
+        if self._lib.pbf_group_sync(self._g) != 0:
+            raise RuntimeError(self._lib.pbf_last_error(None).decode())
+
+    def stream_handle(self) -> int:
+        out = C.c_void_p()
+        self._lib.pbf_group_get_stream(self._g, C.byref(out))
+        return out.value or 0
+
+    def close(self) -> None:
+        if self._g:
+            self._lib.pbf_group_destroy(self._g)
+            self._g = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        self.close()

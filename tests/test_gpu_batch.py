@@ -131,3 +131,38 @@ def test_batch_64_scenes_workload():
     for i in (int(np.argmin(b.counts)), int(np.argmax(b.counts))):
         s = run_solo(b.scenes[i], 10)
         assert np.array_equal(g.split(x)[i], s.positions()), i
+
+
+def test_scene_group_equals_each_context_stepping_alone():
+    """A scene group (pbf_group_*) advances its contexts by one graph launch
+    whose members are independent child graphs: every context ends exactly
+    where its own pbf_step would put it (graph cached per step count and
+    rebuilt after a member changes its particle count)."""
+    from pbf_b200 import SceneGroup
+    b = small_batch()
+    ctxs = []
+    for sc in b.scenes:
+        c = Particles(sc.params(), sc.n)
+        c.upload(sc.positions())
+        ctxs.append(c)
+    with SceneGroup(ctxs) as grp:
+        grp.step(5)
+        grp.step(5)     # the cached 5-step graph again
+        grp.step(2)
+        grp.sync()
+        for sc, c in zip(b.scenes, ctxs):
+            s = run_solo(sc, 12)
+            for w in ARRAYS:
+                assert np.array_equal(c.get_array(w), s.get_array(w)), (sc.name, w)
+            assert c.step_count() == 12
+        # a member with a new particle count: the group rebuilds its graph
+        sc0 = b.scenes[0]
+        ctxs[0].upload(sc0.positions()[: sc0.n // 2])
+        grp.step(5)
+        s = Particles(sc0.params(), sc0.n)
+        s.upload(sc0.positions()[: sc0.n // 2])
+        s.step(5)
+        assert np.array_equal(ctxs[0].get_array(_abi.ARRAY_POSITIONS), s.get_array(_abi.ARRAY_POSITIONS))
+    for c in ctxs:
+        assert c.stats()["error_flags"] == 0
+        c.close()

@@ -77,6 +77,14 @@ def test_resident_spans_match_the_reference(resident):
         # halo particles: x and x* unchanged by the resident-span stages
         assert np.array_equal(g.get_array(POS)[resident:], x0[resident:])
         assert np.array_equal(g.get_array(PST)[resident:], x0[resident:])
+        # the driver refreshes the halo densities before XSPH divides by them
+        # (main.adios); here both engines get the same stand-in values
+        if resident < n:
+            rho0 = float(sc.params().rest_density)
+            for eng in (g, ref):
+                r = eng.get_array(RHO)
+                r[resident:] = rho0
+                eng.set_array(RHO, r)
         _both(g, ref, "apply_viscosity", res)
         _both(g, ref, "compute_vorticity", res)
         _both(g, ref, "apply_vorticity", res)
