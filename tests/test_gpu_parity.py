@@ -245,6 +245,16 @@ def test_65k_100_steps_fast_statistics(eps):
     assert g.stats()["error_flags"] == 0
 
 
+# Against the reference's OpenMP build, whose in-place XSPH and density nudge
+# race (every run differs, more so with more host threads): the max clamped
+# density error at eps = 600, set by how many particles pile into a wall
+# corner, is a discrete chaotic count.  Averaged over steps 81-100 the
+# reference's runs have differed from each other by up to 2.2% and from this
+# GPU path by up to 4.4% on the boxes of this build; its bar here is 10%.  The
+# deterministic oracle keeps the 4.4% bar (test_65k_100_steps_fast_statistics).
+REF_BUILD_BARS = dict(STAT_BARS[600.0], max_density_error=0.10)
+
+
 def test_65k_100_steps_fast_vs_reference_build():
     """The same averaged statistics against the reference's own OpenMP build."""
     if not ref_available():
@@ -256,7 +266,7 @@ def test_65k_100_steps_fast_vs_reference_build():
     g.upload(x)
     r = RefSim(p, sc.n)
     r.set_state(x)
-    check_bars(averaged_stats(g, g.stats), averaged_stats(r, lambda: r.stats(p)), STAT_BARS[600.0])
+    check_bars(averaged_stats(g, g.stats), averaged_stats(r, lambda: r.stats(p)), REF_BUILD_BARS)
 
 
 # ---------------------------------------------------------------- variants
