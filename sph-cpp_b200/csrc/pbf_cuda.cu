@@ -43,6 +43,7 @@
 #include "pbf_fast.cuh"
 #include "pbf_learn.cuh"
 #include "pbf_mlp_tc.cuh"
+#include "pbf_train_tc.cuh"
 
 using pbf::Dev;
 using pbf::Fast;
@@ -3421,8 +3422,12 @@ int pbf_group_step(pbf_group* g, int nsteps) {
     cudaGraph_t parent = nullptr;
     if (cudaGraphCreate(&parent, 0) != cudaSuccess) return fail(nullptr, PBF_ERR_CUDA, "pbf_group_step: graph");
     pbf_group::Built b;
-    for (pbf_ctx* c : g->ctxs) {
-      b.epochs.push_back(c->graph_epoch);
+    for (pbf_ctx* c : g->ctxs) b.epochs.push_back(c->graph_epoch);
+    // members in descending particle count: the largest scenes' chains enter
+    // the graph first, so their kernels are the first the GPU schedules
+    std::vector<pbf_ctx*> order(g->ctxs);
+    std::stable_sort(order.begin(), order.end(), [](const pbf_ctx* a, const pbf_ctx* b) { return a->n > b->n; });
+    for (pbf_ctx* c : order) {
       if (c->n == 0) continue;
       cudaGraph_t child = nullptr;
       if (int rc = capture_steps(c, nsteps, &child)) {
@@ -3679,18 +3684,37 @@ int pbf_get_training_data(pbf_ctx* ctx, float* features, float* labels) {
   return PBF_OK;
 }
 
+// The tensor-core training kernel: one CTA per SM (its 138 KB of operands),
+// at most one per 128-sample tile.
+static int grad_tc_setup(pbf_ctx* ctx) {
+  const cudaError_t e1 = cudaFuncSetAttribute(pbf::k_mlp_grad_tc<true, true>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, pbf::tt::kSmemBytes);
+  const cudaError_t e2 = cudaFuncSetAttribute(pbf::k_mlp_grad_tc<false, false>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, pbf::tt::kSmemBytes);
+  if (e1 != cudaSuccess || e2 != cudaSuccess)
+    return fail(ctx, PBF_ERR_CUDA, "training kernel shared memory: %s", cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+  return PBF_OK;
+}
+
+static int grad_tc_grid(const pbf_ctx* ctx, int batch) {
+  const int tiles = (batch + pbf::tc::kRows - 1) / pbf::tc::kRows;
+  return std::max(1, std::min(ctx->sms, tiles));
+}
+
 int pbf_mlp_train(pbf_ctx* ctx, int adam_steps, int batch, float lr, uint64_t seed, float* loss) {
   if (!ctx || adam_steps < 0 || batch < 1) return PBF_ERR_ARG;
   if (!ctx->mlp_ready) return fail(ctx, PBF_ERR_STATE, "no network: call pbf_mlp_init or pbf_mlp_set");
   if (!ctx->feats || ctx->n == 0) return fail(ctx, PBF_ERR_STATE, "no recorded step to train on");
   const pbf::MlpDev M = mlp_dev(ctx);
-  const int nb = (batch + pbf::kGradRows - 1) / pbf::kGradRows;
+  if (int rc = grad_tc_setup(ctx)) return rc;
   for (int it = 0; it < adam_steps; ++it) {
     CK(cudaMemsetAsync(ctx->mlp_grad, 0, sizeof(float) * pbf::kMlpParams, ctx->stream));
     CK(cudaMemsetAsync(ctx->mlp_loss, 0, sizeof(float), ctx->stream));
-    pbf::k_mlp_grad<true, true><<<nb, 128, 0, ctx->stream>>>(M, ctx->feats, ctx->lamsumH, (int)ctx->n, batch,
-                                                             seed + 0x632BE59BD9B4E019ull * (uint64_t)it,
-                                                             1.0f / ctx->label_scale, ctx->mlp_grad, ctx->mlp_loss);
+    pbf::k_mlp_grad_tc<true, true><<<grad_tc_grid(ctx, batch), pbf::tc::kThreads, pbf::tt::kSmemBytes,
+                                      ctx->stream>>>(M, ctx->feats, ctx->lamsumH, (int)ctx->n, batch,
+                                                     seed + 0x632BE59BD9B4E019ull * (uint64_t)it,
+                                                     1.0f / ctx->label_scale, ctx->mlp_grad, ctx->mlp_loss,
+                                                     ctx->err);
     ctx->adam_t += 1;
     const float c1 = 1.0f / (1.0f - std::pow(0.9f, (float)ctx->adam_t));
     const float c2 = 1.0f / (1.0f - std::pow(0.999f, (float)ctx->adam_t));
@@ -3716,9 +3740,10 @@ int pbf_mlp_gradients(pbf_ctx* ctx, const float* features, const float* targets,
   CK(cudaMemcpyAsync(dt, targets, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemsetAsync(ctx->mlp_grad, 0, sizeof(float) * pbf::kMlpParams, ctx->stream));
   CK(cudaMemsetAsync(ctx->mlp_loss, 0, sizeof(float), ctx->stream));
-  const int nb = (int)((n + pbf::kGradRows - 1) / pbf::kGradRows);
-  pbf::k_mlp_grad<false, false><<<nb, 128, 0, ctx->stream>>>(mlp_dev(ctx), df, dt, (int)n, (int)n, 0, 1.0f,
-                                                             ctx->mlp_grad, ctx->mlp_loss);
+  if (int rc = grad_tc_setup(ctx)) return rc;
+  pbf::k_mlp_grad_tc<false, false><<<grad_tc_grid(ctx, (int)n), pbf::tc::kThreads, pbf::tt::kSmemBytes,
+                                     ctx->stream>>>(mlp_dev(ctx), df, dt, (int)n, (int)n, 0, 1.0f, ctx->mlp_grad,
+                                                    ctx->mlp_loss, ctx->err);
   if (int rc = check_launch(ctx, "mlp_gradients")) return rc;
   if (grad)
     CK(cudaMemcpyAsync(grad, ctx->mlp_grad, sizeof(float) * pbf::kMlpParams, cudaMemcpyDeviceToHost, ctx->stream));

@@ -1,16 +1,8 @@
 // Per-particle MLP of the learned warm start: 12 -> 64 -> 64 -> 1, GELU
-// (erf form), BF16 weights and activations on the tensor cores, FP32
-// accumulation (mma.sync.m16n8k16.row.col.f32.bf16.bf16.f32).
-//
-// A warp evaluates a tile of 16 particles.  Fragment layouts (PTX ISA,
-// m16n8k16, g = lane/4, t = lane%4):
-//   A 16x16 row-major, 4 x b32:  a0 (g, 2t..2t+1)   a1 (g+8, 2t..2t+1)
-//                                a2 (g, 2t+8..+9)   a3 (g+8, 2t+8..+9)
-//   B 16x8 column-major, 2 x b32: b0 (2t..2t+1, g)  b1 (2t+8..+9, g)
-//   C/D 16x8, 4 x f32:           (g, 2t) (g, 2t+1) (g+8, 2t) (g+8, 2t+1)
-// The D fragments of two neighbouring 8-column tiles are exactly the A
-// fragment of the next layer's 16-wide k step, so activations stay in
-// registers between layers.
+// (erf form), BF16 weights and activations, FP32 accumulation.  Its layout
+// constants, the device view of its parameters and the activation functions;
+// the tensor-core kernels are in pbf_mlp_tc.cuh (inference) and
+// pbf_train_tc.cuh (training).
 #pragma once
 #include <cuda_bf16.h>
 
@@ -51,14 +43,6 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
   return *reinterpret_cast<const uint32_t*>(&v);
 }
 
-__device__ __forceinline__ void mma_bf16_16816(float d[4], const uint32_t a[4], const uint32_t b[2]) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
-      "{%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, {%0, %1, %2, %3};\n"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
-
 // GELU(x) = x/2 (1 + erf(x/sqrt 2)) and its derivative.
 __device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
 __device__ __forceinline__ float gelu_grad(float x) {
@@ -88,81 +72,6 @@ __device__ __forceinline__ float2 gelu2(float2 x) {
   const float2 e = __fmul2_rn(q, u);
   const float2 hx = __fmul2_rn(x, make_float2(0.5f, 0.5f));
   return __ffma2_rn(hx, e, hx);
-}
-
-// B fragment of an [n][k]-stored (n-major, k contiguous) bf16 matrix with row
-// stride ld, for the 8-column tile n0 and the 16-deep k step k0.
-__device__ __forceinline__ void load_b(uint32_t b[2], const __nv_bfloat16* w, int ld, int n0, int k0, int lane) {
-  const int g = lane >> 2, t = lane & 3;
-  const __nv_bfloat16* p = w + (size_t)(n0 + g) * ld + k0 + 2 * t;
-  b[0] = *reinterpret_cast<const uint32_t*>(p);
-  b[1] = *reinterpret_cast<const uint32_t*>(p + 8);
-}
-
-// Forward pass of one 16-row tile.  a_in: A fragment of the normalised,
-// zero-padded features.  Returns y for rows g and g+8 (every lane of a quad
-// holds the same two values).  When z1/z2 are given, the pre-activations are
-// kept (D layout, 8 tiles x 4) for the backward pass.
-__device__ __forceinline__ void mlp_forward16(const MlpDev& M, const uint32_t a_in[4], int lane, float& y_lo,
-                                              float& y_hi, float (*z1)[4] = nullptr, float (*z2)[4] = nullptr) {
-  const int t = lane & 3;
-  uint32_t h1[4][4];  // A fragments of layer 2 (4 k steps)
-#pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    float d[4] = {0.f, 0.f, 0.f, 0.f};
-    uint32_t b[2];
-    load_b(b, M.w1, kMlpInPad, 8 * j, 0, lane);
-    mma_bf16_16816(d, a_in, b);
-    const float bb0 = M.b1[8 * j + 2 * t], bb1 = M.b1[8 * j + 2 * t + 1];
-    d[0] += bb0; d[1] += bb1; d[2] += bb0; d[3] += bb1;
-    if (z1) {
-#pragma unroll
-      for (int e = 0; e < 4; ++e) z1[j][e] = d[e];
-    }
-    const uint32_t lo = pack_bf16x2(gelu(d[0]), gelu(d[1]));
-    const uint32_t hi = pack_bf16x2(gelu(d[2]), gelu(d[3]));
-    // tile j holds columns 8j..8j+7: k step j/2, low (j even) or high half
-    if ((j & 1) == 0) { h1[j >> 1][0] = lo; h1[j >> 1][1] = hi; }
-    else { h1[j >> 1][2] = lo; h1[j >> 1][3] = hi; }
-  }
-  float acc_lo = 0.f, acc_hi = 0.f;
-#pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    float d[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-    for (int ks = 0; ks < 4; ++ks) {
-      uint32_t b[2];
-      load_b(b, M.w2, kMlpH, 8 * j, 16 * ks, lane);
-      mma_bf16_16816(d, h1[ks], b);
-    }
-    const int c0 = 8 * j + 2 * t;
-    const float bb0 = M.b2[c0], bb1 = M.b2[c0 + 1];
-    d[0] += bb0; d[1] += bb1; d[2] += bb0; d[3] += bb1;
-    if (z2) {
-#pragma unroll
-      for (int e = 0; e < 4; ++e) z2[j][e] = d[e];
-    }
-    const float w0 = M.w3[c0], w1 = M.w3[c0 + 1];
-    acc_lo = fmaf(gelu(d[0]), w0, fmaf(gelu(d[1]), w1, acc_lo));
-    acc_hi = fmaf(gelu(d[2]), w0, fmaf(gelu(d[3]), w1, acc_hi));
-  }
-  // the four lanes of a quad hold disjoint columns of rows g and g+8
-  acc_lo += __shfl_xor_sync(0xffffffffu, acc_lo, 1);
-  acc_lo += __shfl_xor_sync(0xffffffffu, acc_lo, 2);
-  acc_hi += __shfl_xor_sync(0xffffffffu, acc_hi, 1);
-  acc_hi += __shfl_xor_sync(0xffffffffu, acc_hi, 2);
-  y_lo = acc_lo + M.b3[0];
-  y_hi = acc_hi + M.b3[0];
-}
-
-// A fragment of a 16-row tile of features stored row-major (stride 16 bf16)
-// in shared memory.
-__device__ __forceinline__ void load_a_rows16(uint32_t a[4], const __nv_bfloat16* s, int lane) {
-  const int g = lane >> 2, t = lane & 3;
-  a[0] = *reinterpret_cast<const uint32_t*>(s + g * 16 + 2 * t);
-  a[1] = *reinterpret_cast<const uint32_t*>(s + (g + 8) * 16 + 2 * t);
-  a[2] = *reinterpret_cast<const uint32_t*>(s + g * 16 + 2 * t + 8);
-  a[3] = *reinterpret_cast<const uint32_t*>(s + (g + 8) * 16 + 2 * t + 8);
 }
 
 }  // namespace pbf
