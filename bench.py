@@ -65,6 +65,10 @@ def parse_args():
     ap.add_argument("--profile-learned", type=int, default=0, metavar="K",
                     help="only run K steps of the learned warm start (eps 1, after its warm-up) and print "
                          "ms/step: the command the learned kernels' ncu summaries are captured from")
+    ap.add_argument("--profile-training", type=int, default=0, metavar="K",
+                    help="only record one 1M-dam step and run K Adam updates of the warm-start network "
+                         "(batch 65,536) and print ms/update: the command the training kernel's ncu "
+                         "summary is captured from")
     ap.add_argument("--learned-iterations", type=int, default=10,
                     help="iteration cap of --profile-learned (1: no conditional loop in the step's graph, "
                          "which ncu needs to profile the graph's kernels)")
@@ -536,6 +540,32 @@ def main():
     args = parse_args()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.profile_training:
+        import ctypes as C
+        import torch
+        from pbf_b200 import Particles
+        from pbf_b200.learn import normalization, warm_start_scene
+        sc = warm_start_scene(args.scene)
+        with Particles(sc.params(), sc.n) as g:
+            g.mlp_init(7)
+            g.upload(sc.positions())
+            g.step(3)
+            g.set_recording(True)
+            g.step(1)
+            g.set_recording(False)
+            f, lab = g.training_data()
+            params, _ = g.mlp_get()
+            g.mlp_set(params, normalization(f, lab))
+            loss = C.c_float()
+            for _ in range(2):  # the second call is timed
+                g.sync()
+                t0 = time.perf_counter()
+                rc = g._lib.pbf_mlp_train(g.ctx, args.profile_training, 65536, C.c_float(1e-3), 5, C.byref(loss))
+                dt = time.perf_counter() - t0
+                assert rc == 0, g._lib.pbf_last_error(g.ctx)
+        print(json.dumps({"ms_per_adam_update": 1e3 * dt / args.profile_training, "batch": 65536,
+                          "loss": loss.value}), flush=True)
+        return 0
     if args.profile_learned:
         from pbf_b200.learn import DEFAULT_MODEL, load_model, warm_start_scene
         params, norm, _ = load_model(DEFAULT_MODEL)
