@@ -3361,6 +3361,8 @@ int pbf_step(pbf_ctx* ctx, int nsteps) {
 // slowest scene ends.  Results are each context's own pbf_step results, bit
 // for bit.  The graph is cached per nsteps and rebuilt when a member drops its
 // graphs (a new particle count or new parameters).
+constexpr bool kGroupPriorities = true;  // members' kernels prioritised by scene size
+
 struct pbf_group {
   std::vector<pbf_ctx*> ctxs;
   cudaStream_t stream = nullptr;
@@ -3424,15 +3426,37 @@ int pbf_group_step(pbf_group* g, int nsteps) {
     pbf_group::Built b;
     for (pbf_ctx* c : g->ctxs) b.epochs.push_back(c->graph_epoch);
     // members in descending particle count: the largest scenes' chains enter
-    // the graph first, so their kernels are the first the GPU schedules
+    // the graph first, and their kernels run at the higher stream priorities
+    // (the graph is instantiated with node priorities), so the longest chains
+    // start first and the small scenes fill the GPU around them
     std::vector<pbf_ctx*> order(g->ctxs);
     std::stable_sort(order.begin(), order.end(), [](const pbf_ctx* a, const pbf_ctx* b) { return a->n > b->n; });
-    for (pbf_ctx* c : order) {
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    const int levels = least - greatest + 1;  // e.g. 0 (lowest) .. -5 (highest)
+    for (size_t rank = 0; rank < order.size(); ++rank) {
+      pbf_ctx* c = order[rank];
       if (c->n == 0) continue;
       cudaGraph_t child = nullptr;
       if (int rc = capture_steps(c, nsteps, &child)) {
         cudaGraphDestroy(parent);
         return fail(nullptr, rc, "pbf_group_step: capture of a member failed: %s", pbf_last_error(c));
+      }
+      if (kGroupPriorities && levels > 1) {
+        const int prio = greatest + (int)((rank * (size_t)levels) / order.size());
+        size_t nn = 0;
+        cudaGraphGetNodes(child, nullptr, &nn);
+        std::vector<cudaGraphNode_t> nodes(nn);
+        if (nn && cudaGraphGetNodes(child, nodes.data(), &nn) == cudaSuccess) {
+          cudaLaunchAttributeValue v = {};
+          v.priority = prio;
+          for (cudaGraphNode_t node : nodes) {
+            cudaGraphNodeType type;
+            if (cudaGraphNodeGetType(node, &type) == cudaSuccess && type == cudaGraphNodeTypeKernel)
+              cudaGraphKernelNodeSetAttribute(node, cudaLaunchAttributePriority, &v);
+          }
+        }
+        cudaGetLastError();  // a priority that does not apply leaves the default
       }
       cudaGraphNode_t node = nullptr;
       const cudaError_t e = cudaGraphAddChildGraphNode(&node, parent, nullptr, 0, child);
@@ -3443,7 +3467,8 @@ int pbf_group_step(pbf_group* g, int nsteps) {
                     cudaGetErrorString(e));
       }
     }
-    const cudaError_t ie = cudaGraphInstantiate(&b.exec, parent, 0);
+    const cudaError_t ie =
+        cudaGraphInstantiate(&b.exec, parent, kGroupPriorities ? cudaGraphInstantiateFlagUseNodePriority : 0);
     cudaGraphDestroy(parent);
     if (ie != cudaSuccess)
       return fail(nullptr, PBF_ERR_CUDA, "pbf_group_step: graph instantiate failed: %s", cudaGetErrorString(ie));
