@@ -498,7 +498,7 @@ __device__ __noinline__ int fill_runs(float px, float py, float pz, float s2, in
       for (uint32_t r = q; r < qe && count < cap; ++r) {
         if (r == self) continue;
         if (row16) row16[count] = (uint16_t)((int)r + off);
-        row[count++] = (int32_t)r;
+        row[pbf::list_off(count++)] = (int32_t)r;
       }
       if (count >= cap) break;
     }
@@ -510,8 +510,8 @@ __device__ __noinline__ int fill_runs(float px, float py, float pz, float s2, in
 // fill_neighbors (neighbors.h:197-230) over slots in sorted order: the 27
 // bins in the reference's order (x offset outer, z inner, float re-hash of
 // coord + i*s), candidates of a bin in ascending reference index, strict
-// d^2 < s^2, self skipped, the first `cap` kept.  Lists are row-major
-// ([slot][cap]): each thread fills its own contiguous run.  A neighbour bin whose every point is provably
+// d^2 < s^2, self skipped, the first `cap` kept.  Each thread fills its own
+// list in the warp-tiled layout (pbf::list_off).  A neighbour bin whose every point is provably
 // farther than s from the particle is skipped: the per-axis distance from the
 // particle to the bin's face, less a margin of many ulps of the coordinate
 // (P.skip_eps), squared and summed, exceeds s^2.  Only bins equal to the
@@ -551,7 +551,7 @@ __global__ void __launch_bounds__(kFillBlock) k_fill2(Dev P, int n, size_t strid
   const int cap = P.cap;
   const float s = P.s;
   const pbf::Region R = pbf::region_of(P, bb);
-  int32_t* row = nbr + (size_t)b * stride;
+  int32_t* row = nbr + pbf::list_base(b, stride);
   // calculate_neighbor_indices (neighbors.h:172-185): the bin of coord + i*s
   // per axis for i = -1, 0, 1, in the reference's float operations.  The 27
   // bins combine these per-axis values, so 9 float hashes cover all of them.
@@ -654,7 +654,7 @@ __global__ void __launch_bounds__(kFillBlock) k_fill2(Dev P, int n, size_t strid
             const float d2 = pbf::mag2<true>(pbf::xsub(xp.x, xq.x), pbf::xsub(xp.y, xq.y), pbf::xsub(xp.z, xq.z));
             if (d2 < P.s2 && q != (uint32_t)b && count < cap) {
               if (STAGE && staged) row16[count] = (uint16_t)((int)q + off);
-              row[count++] = (int32_t)q;
+              row[pbf::list_off(count++)] = (int32_t)q;
             }
           }
         }
@@ -689,7 +689,7 @@ __global__ void __launch_bounds__(kBlock) k_density(Dev P, int n, size_t stride,
   float rho = pbf::M<X>(P.m, P.W0);
   bool nudged = false;
   for (int k = 0; k < c; ++k) {
-    const int q = nbr[(size_t)b * stride + k];
+    const int q = nbr[pbf::list_at(b, stride, k)];
     const float4 xq = pst[q];
     float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
     float rm = pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz));
@@ -741,7 +741,7 @@ __global__ void __launch_bounds__(kBlock) k_lambda(Dev P, int n, size_t stride, 
   float3 sg = make_float3(0.f, 0.f, 0.f);
   float sumC = 0.0f;
   for (int k = 0; k < c; ++k) {
-    const float4 xq = pst[nbr[(size_t)b * stride + k]];
+    const float4 xq = pst[nbr[pbf::list_at(b, stride, k)]];
     const float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
     lambda_terms<X>(P, rx, ry, rz, pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz)), sg, sumC);
   }
@@ -766,7 +766,7 @@ __device__ __forceinline__ void density_lambda_one(const Dev& P, int b, size_t s
   float sumC = 0.0f;
   bool nudged = false;
   for (int k = 0; k < c; ++k) {
-    const float4 xq = pst[nbr[(size_t)b * stride + k]];
+    const float4 xq = pst[nbr[pbf::list_at(b, stride, k)]];
     float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
     float rm = pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz));
     if ((double)rm < 0.00000001) {
@@ -878,7 +878,7 @@ __device__ __forceinline__ void density_lambda_tile(int tile, const Dev& P, cons
   const float4 xp = pst[b];
   const int c = G.live ? cnt[b] : 0;
   const DensitySums S = density_sums<GL, MODE == kDlRecord, STAGED>(
-      F, G, nbr + (size_t)b * stride, STAGED ? nbr16 + (size_t)b * stride : nullptr, c, STAGED ? staged : n,
+      F, G, nbr + pbf::list_base(b, stride), STAGED ? nbr16 + (size_t)b * stride : nullptr, c, STAGED ? staged : n,
       STAGED ? stage : pst, xp);
   const float rho = fmaf(F.m_poly, S.sw, F.m_w0);
   if (MODE == kDlCheck && G.live && G.lane == 0) err += fmaxf(fmaf(rho, F.inv_rho0, -1.0f), 0.0f);
@@ -1026,7 +1026,7 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) kl_features(Dev P, F
   const int b = G.b;
   const float4 xp = pst[b];
   const int c = G.live ? cnt[b] : 0;
-  const DensitySums S = density_sums<GL, true>(F, G, nbr + (size_t)b * stride, nullptr, c, n, pst, xp);
+  const DensitySums S = density_sums<GL, true>(F, G, nbr + pbf::list_base(b, stride), nullptr, c, n, pst, xp);
   if (!G.live || G.lane != 0) return;
   const float rho = fmaf(F.m_poly, S.sw, F.m_w0);
   const float L2 = F.lam_grad * F.lam_grad;
@@ -1247,7 +1247,7 @@ __global__ void __launch_bounds__(kBlock) k_lambda_fixup(Dev P, int n, size_t st
   float3 sg = make_float3(0.f, 0.f, 0.f);
   float sumC = 0.0f;
   for (int k = 0; k < c; ++k) {
-    const float4 xq = xl[nbr[(size_t)b * stride + k]];
+    const float4 xq = xl[nbr[pbf::list_at(b, stride, k)]];
     const float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
     lambda_terms<X>(P, rx, ry, rz, pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz)), sg, sumC);
   }
@@ -1281,7 +1281,7 @@ __global__ void __launch_bounds__(kBlock) k_dp(Dev P, int n, size_t stride, cons
   const int c = cnt[b];
   float3 dp = make_float3(0.f, 0.f, 0.f);
   for (int k = 0; k < c; ++k) {
-    const int q = nbr[(size_t)b * stride + k];
+    const int q = nbr[pbf::list_at(b, stride, k)];
     const float4 xq = pst[q];
     const float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
     dp_term<X, SCORR>(P, lp, lam[q], rx, ry, rz, pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz)), dp);
@@ -1344,14 +1344,14 @@ __global__ void __launch_bounds__(kBlock) k_dp_update(Dev P, int n, size_t strid
   float3 dp = make_float3(0.f, 0.f, 0.f);
   if (*nudge == 0u) {
     for (int k = 0; k < c; ++k) {
-      const float4 xq = xl[nbr[(size_t)b * stride + k]];
+      const float4 xq = xl[nbr[pbf::list_at(b, stride, k)]];
       const float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
       dp_term<X, SCORR>(P, xp.w, xq.w, rx, ry, rz, pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz)), dp);
     }
   } else {  // lambdas were recomputed by k_lambda_fixup
     const float lp = lam[b];
     for (int k = 0; k < c; ++k) {
-      const int q = nbr[(size_t)b * stride + k];
+      const int q = nbr[pbf::list_at(b, stride, k)];
       const float4 xq = xl[q];
       const float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
       dp_term<X, SCORR>(P, lp, lam[q], rx, ry, rz, pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz)), dp);
@@ -1379,7 +1379,7 @@ __global__ void __launch_bounds__(kBlock) k_color(Dev P, int n, size_t stride, c
   const int c = cnt[b];
   float3 col = make_float3(0.f, 0.f, 0.f);
   for (int k = 0; k < c; ++k) {
-    const int q = nbr[(size_t)b * stride + k];
+    const int q = nbr[pbf::list_at(b, stride, k)];
     const float4 xq = pst[q];
     const float rq = vel[q].w;
     const float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
@@ -1403,7 +1403,7 @@ __global__ void __launch_bounds__(kBlock) k_surface(Dev P, int n, size_t stride,
   const float ng = -P.gamma;
   float3 f = make_float3(0.f, 0.f, 0.f);
   for (int k = 0; k < c; ++k) {
-    const int q = nbr[(size_t)b * stride + k];
+    const int q = nbr[pbf::list_at(b, stride, k)];
     const float4 xq = pst[q], sq = scr[q];
     const float rq = vel[q].w;
     const float rx = pbf::xsub(xp.x, xq.x), ry = pbf::xsub(xp.y, xq.y), rz = pbf::xsub(xp.z, xq.z);
@@ -1441,7 +1441,7 @@ __global__ void __launch_bounds__(kBlock) k_viscosity(Dev P, int n, size_t strid
   const int c = cnt[b];
   float3 dv = make_float3(0.f, 0.f, 0.f);
   for (int k = 0; k < c; ++k) {
-    const int q = nbr[(size_t)b * stride + k];
+    const int q = nbr[pbf::list_at(b, stride, k)];
     const float4 xq = pst[q], vq = vin[q];
     const float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
     const float w = pbf::poly6<X>(P, pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz)));
@@ -1477,7 +1477,7 @@ __global__ void __launch_bounds__(kBlock) k_vorticity(Dev P, int n, size_t strid
   const int c = cnt[b];
   float3 w = make_float3(0.f, 0.f, 0.f);
   for (int k = 0; k < c; ++k) {
-    const int q = nbr[(size_t)b * stride + k];
+    const int q = nbr[pbf::list_at(b, stride, k)];
     const float4 xq = pst[q], vq = vel[q];
     const float rx = pbf::S<X>(xp.x, xq.x), ry = pbf::S<X>(xp.y, xq.y), rz = pbf::S<X>(xp.z, xq.z);
     const float3 d = pbf::del_spikey<X>(P, rx, ry, rz, pbf::SQ<X>(pbf::mag2<X>(rx, ry, rz)));
@@ -1507,7 +1507,7 @@ __global__ void __launch_bounds__(kBlock) k_apply_vorticity(Dev P, int n, size_t
   const int c = cnt[b];
   float3 eta = make_float3(0.f, 0.f, 0.f);
   for (int k = 0; k < c; ++k) {
-    const int q = nbr[(size_t)b * stride + k];
+    const int q = nbr[pbf::list_at(b, stride, k)];
     float4 xq;
     float vm;
     if (PACKED) {
@@ -1561,7 +1561,7 @@ __device__ __forceinline__ void dp_update_tile(int tile, const Dev& P, const Fas
   const int c = G.live ? cnt[b] : 0;
   float ax = 0.f, ay = 0.f, az = 0.f;
   const float lp = xp.w;
-  pbf::walk1<GL, STAGED, true>(nbr + (size_t)b * stride, STAGED ? src.nbr16 + (size_t)b * stride : nullptr, c,
+  pbf::walk1<GL, STAGED>(nbr + pbf::list_base(b, stride), STAGED ? src.nbr16 + (size_t)b * stride : nullptr, c,
                          STAGED ? src.dummy : n, G.lane, STAGED ? src.a : xl, [&](int, float4 xq) {
     const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
     const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
@@ -1636,7 +1636,7 @@ __device__ __forceinline__ void viscosity_tile(int tile, const Fast& F, int n, s
   const float4 xp = pst[b], vp = vin[b];
   const int c = G.live ? cnt[b] : 0;
   float ax = 0.f, ay = 0.f, az = 0.f;
-  pbf::walk2<GL, STAGED, FINAL>(nbr + (size_t)b * stride, STAGED ? src.nbr16 + (size_t)b * stride : nullptr, c,
+  pbf::walk2<GL, STAGED, FINAL>(nbr + pbf::list_base(b, stride), STAGED ? src.nbr16 + (size_t)b * stride : nullptr, c,
                          STAGED ? src.dummy : n, G.lane, STAGED ? src.a : pst, STAGED ? src.b : vin,
                          [&](int, float4 xq, float4 vq) {
     const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
@@ -1697,7 +1697,7 @@ __device__ __forceinline__ void vorticity_tile(int tile, const Fast& F, int n, s
   const float4 xp = pst[b], vp = vel[b];
   const int c = G.live ? cnt[b] : 0;
   float wx = 0.f, wy = 0.f, wz = 0.f;
-  pbf::walk2<GL, STAGED>(nbr + (size_t)b * stride, STAGED ? src.nbr16 + (size_t)b * stride : nullptr, c,
+  pbf::walk2<GL, STAGED>(nbr + pbf::list_base(b, stride), STAGED ? src.nbr16 + (size_t)b * stride : nullptr, c,
                          STAGED ? src.dummy : n, G.lane, STAGED ? src.a : pst, STAGED ? src.b : vel,
                          [&](int, float4 xq, float4 vq) {
     const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
@@ -1752,7 +1752,7 @@ __device__ __forceinline__ void apply_vorticity_tile(int tile, const Fast& F, in
   const float4 xp = xl[b];
   const int c = G.live ? cnt[b] : 0;
   float ex = 0.f, ey = 0.f, ez = 0.f;
-  pbf::walk1<GL, STAGED>(nbr + (size_t)b * stride, STAGED ? src.nbr16 + (size_t)b * stride : nullptr, c,
+  pbf::walk1<GL, STAGED>(nbr + pbf::list_base(b, stride), STAGED ? src.nbr16 + (size_t)b * stride : nullptr, c,
                          STAGED ? src.dummy : n, G.lane, STAGED ? src.a : xl, [&](int, float4 xq) {
     const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
     const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
@@ -1820,7 +1820,7 @@ __global__ void __launch_bounds__(kBlock) k_stats(Dev P, int b0, int b1, size_t 
     const int c = cnt[b];
     float d = pbf::xmul(P.m, P.W0);
     for (int k = 0; k < c; ++k) {
-      const float4 xq = pst[nbr[(size_t)b * stride + k]];
+      const float4 xq = pst[nbr[pbf::list_at(b, stride, k)]];
       const float rx = pbf::xsub(xp.x, xq.x), ry = pbf::xsub(xp.y, xq.y), rz = pbf::xsub(xp.z, xq.z);
       d = pbf::xadd(d, pbf::xmul(P.m, pbf::poly6<true>(P, __fsqrt_rn(pbf::mag2<true>(rx, ry, rz)))));
     }
@@ -1852,7 +1852,7 @@ __global__ void k_export_neighbors(int n, size_t stride, int cap, const int32_t*
   if (cnt_out) cnt_out[o] = c;
   if (idx_out)
     for (int k = 0; k < cap; ++k)
-      idx_out[o * cap + k] = k < c ? (int32_t)orig[nbr[(size_t)b * stride + k]] : -1;
+      idx_out[o * cap + k] = k < c ? (int32_t)orig[nbr[pbf::list_at(b, stride, k)]] : -1;
 }
 
 }  // namespace
@@ -2782,7 +2782,7 @@ static int create_ctx(const pbf_params* p, size_t capacity, const pbf_scene* sce
       (rc = dalloc(ctx, &ctx->cell_start, (size_t)ctx->nbins + 1)) ||
       (rc = dalloc(ctx, &ctx->scan_part, (size_t)ctx->nscan_parts)) || (rc = dalloc(ctx, &ctx->err, 1)) ||
       (rc = dalloc(ctx, &ctx->nudge, 1)) ||
-      (rc = dalloc(ctx, &ctx->pairs, C)) || (rc = dalloc(ctx, &ctx->pairs_sorted, C)) || (rc = dalloc(ctx, &ctx->nbr, C * cap)) ||
+      (rc = dalloc(ctx, &ctx->pairs, C)) || (rc = dalloc(ctx, &ctx->pairs_sorted, C)) || (rc = dalloc(ctx, &ctx->nbr, pbf::list_entries(C, cap))) ||
       (rc = dalloc(ctx, &ctx->cnt, C)) || (rc = dalloc(ctx, &ctx->stage, 6 * C)) ||
       (rc = dalloc(ctx, &ctx->stage_i, C * cap + C)) || (rc = dalloc(ctx, &ctx->acc, 8)) ||
       (rc = dalloc(ctx, &ctx->maxerr, 1)) || (rc = dalloc(ctx, &ctx->hits, 1)) ||

@@ -10,7 +10,7 @@
 //    h < r < s, which stay in the lists because x* moves during the iterations;
 //  - kernel constants (norms, 1/rho0, mass) folded on the host;
 //  - GL = 2, 4 or 8 lanes per particle (the launch shape the autotuner picks)
-//    walk its row-major, padded list together (see Group, gwalk1) and
+//    walk its warp-tiled, padded list together (see Group, gwalk1) and
 //    combine their partial sums with shuffles.
 // A particle sitting exactly on a neighbour (d^2 < 1e-16, the reference's
 // nudge condition |r| < 1e-8, particles.h:303-305) falls back to the
@@ -50,10 +50,10 @@ inline Fast make_fast(const Dev& d) {
 
 // Lane groups: GL consecutive threads share one particle (GL = 2, 4 or 8, the
 // launch shape the autotuner picks per kernel family; kGL is the default).
-// Lane l walks entries l, l + GL, ... of the particle's row-major list, so one
-// warp-wide load touches GL consecutive entries of each of 32/GL lists, and
-// the neighbours those entries name are mostly consecutive slots of one bin
-// (coalesced gathers).  Partial sums are combined with shuffles.
+// Lane l walks its share of every batch of the particle's list (gwalk1,
+// gwalk2); a warp-wide index load reads the same chunk row of 32/GL
+// consecutive particles' lists, contiguous in the warp-tiled layout.  Partial
+// sums are combined with shuffles.
 constexpr int kGL = 8;
 
 struct Group {
@@ -108,34 +108,58 @@ __device__ __forceinline__ float gmin(float v) {
   return v;
 }
 
-// Walk a list row: lane l of the group takes entries 4l..4l+3 of every
-// 4*GL-entry batch, one 16-byte index load, then its four neighbour records
+// Vector v of a particle's list (entries 4v..4v+3, or 2v, 2v+1 for the 8-byte
+// vectors) in the warp-tiled layout (list_base, list_off): the row pointer is
+// the particle's first entry, its 8-entry chunks 128 entries apart.
+__device__ __forceinline__ int vec4_at(int v) { return (v >> 1) * (kListTile * kListChunk / 4) + (v & 1); }
+__device__ __forceinline__ int vec2_at(int v) { return (v >> 2) * (kListTile * kListChunk / 2) + (v & 3); }
+// A batch of a walk covers whole chunks when GL is even (4*GL entries per
+// batch) or a multiple of 4 (2*GL entries): batch t starts t * 16 * GL
+// vectors in (its 4*GL or 2*GL entries span GL/2 or GL/4 chunk rows), and
+// lane l's vector sits at vec4_at(l) / vec2_at(l) from there.
+constexpr int kBatchVecs = kListTile * kListChunk / 8;  // x GL: vectors per batch
+
+// The last batch: entries of vector v (entries 4v..4v+3, or 2v, 2v+1) at or
+// past the count c name `dummy`.
+__device__ __forceinline__ int4 tail4(int4 q, int v, int c, int dummy) {
+  const int e = 4 * v;
+  q.x = e < c ? q.x : dummy;
+  q.y = e + 1 < c ? q.y : dummy;
+  q.z = e + 2 < c ? q.z : dummy;
+  q.w = e + 3 < c ? q.w : dummy;
+  return q;
+}
+__device__ __forceinline__ int2 tail2(int2 q, int v, int c, int dummy) {
+  const int e = 2 * v;
+  q.x = e < c ? q.x : dummy;
+  q.y = e + 1 < c ? q.y : dummy;
+  return q;
+}
+
+// Walk a list row: lane l of the group takes four entries of every 4*GL-entry
+// batch (the 16-byte vector vec4_at), one index load, then its four neighbour records
 // (four independent loads in flight), then the four bodies.  Rows are padded
 // to a multiple of 32 entries, so every batch reads whole vectors inside the
 // row; entries of the last batch past the count are replaced by `dummy`, a
 // slot whose every term is zero.  PF: the next batch's index vector is loaded
 // before this batch's records (the lists stream from DRAM; the prefetch takes
 // one DRAM round trip per batch off the index -> record chain).  It is set
-// where it measured faster (Δp, the final XSPH pass); elsewhere it measured
-// slower.
+// where it measured faster (the final XSPH pass); elsewhere it measured
+// slower (Δp too, since the warp-tiled lists).
 template <int GL = kGL, bool PF = false, class Body>
 __device__ __forceinline__ void gwalk1(const int32_t* __restrict__ row, int c, int dummy, int lane,
                                        const float4* __restrict__ a, Body&& body) {
+  static_assert(GL % 2 == 0, "a batch covers whole chunks");
   const int4* r4 = reinterpret_cast<const int4*>(row);
+  const int l0 = vec4_at(lane);
   if constexpr (PF) {
     const int batches = (c + 4 * GL - 1) / (4 * GL);
     if (batches == 0) return;
-    int4 next = __ldg(r4 + lane);
+    int4 next = __ldg(r4 + l0);
     for (int t = 0; t < batches; ++t) {
       int4 q = next;
-      if (t + 1 < batches) next = __ldg(r4 + (t + 1) * GL + lane);
-      if (t + 1 == batches) {
-        const int e = t * 4 * GL + 4 * lane;
-        q.x = e < c ? q.x : dummy;
-        q.y = e + 1 < c ? q.y : dummy;
-        q.z = e + 2 < c ? q.z : dummy;
-        q.w = e + 3 < c ? q.w : dummy;
-      }
+      if (t + 1 < batches) next = __ldg(r4 + (l0 + (t + 1) * kBatchVecs * GL));
+      if (t + 1 == batches) q = tail4(q, t * GL + lane, c, dummy);
       const float4 v0 = __ldg(a + q.x), v1 = __ldg(a + q.y), v2 = __ldg(a + q.z), v3 = __ldg(a + q.w);
       body(q.x, v0);
       body(q.y, v1);
@@ -146,7 +170,7 @@ __device__ __forceinline__ void gwalk1(const int32_t* __restrict__ row, int c, i
     const int full = c / (4 * GL);
     int t = 0;
     for (; t < full; ++t) {
-      const int4 q = __ldg(r4 + t * GL + lane);
+      const int4 q = __ldg(r4 + (l0 + t * kBatchVecs * GL));
       const float4 v0 = __ldg(a + q.x), v1 = __ldg(a + q.y), v2 = __ldg(a + q.z), v3 = __ldg(a + q.w);
       body(q.x, v0);
       body(q.y, v1);
@@ -154,12 +178,7 @@ __device__ __forceinline__ void gwalk1(const int32_t* __restrict__ row, int c, i
       body(q.w, v3);
     }
     if (t * 4 * GL < c) {
-      int4 q = __ldg(r4 + t * GL + lane);
-      const int e = t * 4 * GL + 4 * lane;
-      q.x = e < c ? q.x : dummy;
-      q.y = e + 1 < c ? q.y : dummy;
-      q.z = e + 2 < c ? q.z : dummy;
-      q.w = e + 3 < c ? q.w : dummy;
+      const int4 q = tail4(__ldg(r4 + (l0 + t * kBatchVecs * GL)), t * GL + lane, c, dummy);
       const float4 v0 = __ldg(a + q.x), v1 = __ldg(a + q.y), v2 = __ldg(a + q.z), v3 = __ldg(a + q.w);
       body(q.x, v0);
       body(q.y, v1);
@@ -177,18 +196,16 @@ __device__ __forceinline__ void gwalk2(const int32_t* __restrict__ row, int c, i
                                        const float4* __restrict__ a, const float4* __restrict__ bsrc,
                                        Body&& body) {
   const int2* r2 = reinterpret_cast<const int2*>(row);
+  // vector of batch t (whole chunk rows when GL is a multiple of 4)
+  auto at = [&](int t) { return GL % 4 == 0 ? t * kBatchVecs * GL + vec2_at(lane) : vec2_at(t * GL + lane); };
   if constexpr (PF) {
     const int batches = (c + 2 * GL - 1) / (2 * GL);
     if (batches == 0) return;
-    int2 next = __ldg(r2 + lane);
+    int2 next = __ldg(r2 + at(0));
     for (int t = 0; t < batches; ++t) {
       int2 q = next;
-      if (t + 1 < batches) next = __ldg(r2 + (t + 1) * GL + lane);
-      if (t + 1 == batches) {
-        const int e = t * 2 * GL + 2 * lane;
-        q.x = e < c ? q.x : dummy;
-        q.y = e + 1 < c ? q.y : dummy;
-      }
+      if (t + 1 < batches) next = __ldg(r2 + at(t + 1));
+      if (t + 1 == batches) q = tail2(q, t * GL + lane, c, dummy);
       const float4 a0 = __ldg(a + q.x), b0 = __ldg(bsrc + q.x), a1 = __ldg(a + q.y), b1 = __ldg(bsrc + q.y);
       body(q.x, a0, b0);
       body(q.y, a1, b1);
@@ -197,16 +214,13 @@ __device__ __forceinline__ void gwalk2(const int32_t* __restrict__ row, int c, i
     const int full = c / (2 * GL);
     int t = 0;
     for (; t < full; ++t) {
-      const int2 q = __ldg(r2 + t * GL + lane);
+      const int2 q = __ldg(r2 + at(t));
       const float4 a0 = __ldg(a + q.x), b0 = __ldg(bsrc + q.x), a1 = __ldg(a + q.y), b1 = __ldg(bsrc + q.y);
       body(q.x, a0, b0);
       body(q.y, a1, b1);
     }
     if (t * 2 * GL < c) {
-      int2 q = __ldg(r2 + t * GL + lane);
-      const int e = t * 2 * GL + 2 * lane;
-      q.x = e < c ? q.x : dummy;
-      q.y = e + 1 < c ? q.y : dummy;
+      const int2 q = tail2(__ldg(r2 + at(t)), t * GL + lane, c, dummy);
       const float4 a0 = __ldg(a + q.x), b0 = __ldg(bsrc + q.x), a1 = __ldg(a + q.y), b1 = __ldg(bsrc + q.y);
       body(q.x, a0, b0);
       body(q.y, a1, b1);

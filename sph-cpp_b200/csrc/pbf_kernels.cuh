@@ -15,6 +15,28 @@
 
 namespace pbf {
 
+// Neighbour lists in warp tiles.  The lists of kListTile consecutive sorted
+// slots interleave in chunks of kListChunk entries: entry j of slot b is at
+//   (b / 16) * 16 * stride + (j / 8) * 128 + (b % 16) * 8 + j % 8
+// (stride = the row length, a multiple of 32 entries).  A particle's chunk is
+// one 32-byte sector, and the same chunk of 16 consecutive particles is 512
+// contiguous bytes, so a warp of a gather that reads one chunk row of its
+// particles' lists touches 4 cache lines, where row-major lists put each
+// particle's chunk on a line of its own (one L1 wavefront per line).  The
+// list buffer holds whole tiles: capacity rounded up to kListTile slots.
+constexpr int kListTile = 16, kListChunk = 8;  // list_off's shift is log2(kListChunk)
+
+__host__ __device__ inline size_t list_base(size_t b, size_t stride) {
+  return (b / kListTile) * kListTile * stride + (b % kListTile) * kListChunk;
+}
+__host__ __device__ inline int list_off(int j) {
+  return (j >> 3) * (kListTile * kListChunk) + (j & (kListChunk - 1));
+}
+__host__ __device__ inline size_t list_at(size_t b, size_t stride, int j) { return list_base(b, stride) + list_off(j); }
+__host__ __device__ inline size_t list_entries(size_t capacity, size_t stride) {
+  return (capacity + kListTile - 1) / kListTile * kListTile * stride;
+}
+
 // Box and bin grid of one scene.  A context advances one scene (the box and
 // grid of Dev itself) or a batch of independent scenes, each with its own box
 // and grid; the bin keys of a batch's scene i start at key0, so the sort by
