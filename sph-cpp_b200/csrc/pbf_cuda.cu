@@ -648,11 +648,20 @@ __global__ void __launch_bounds__(kFillBlock) k_fill2(Dev P, int n, size_t strid
         if (q1 - q0 > kRunBin) {
           count = fill_runs(xp.x, xp.y, xp.z, P.s2, cap, (uint32_t)b, q0, q1, pst, run_end, row,
                             STAGE && staged ? row16 : nullptr, off, count);
-        } else {
+        } else if (q0 <= (uint32_t)b && (uint32_t)b < q1) {  // the particle's own bin: skip itself
           for (uint32_t q = q0; q < q1; ++q) {
             const float4 xq = pst[q];
             const float d2 = pbf::mag2<true>(pbf::xsub(xp.x, xq.x), pbf::xsub(xp.y, xq.y), pbf::xsub(xp.z, xq.z));
             if (d2 < P.s2 && q != (uint32_t)b && count < cap) {
+              if (STAGE && staged) row16[count] = (uint16_t)((int)q + off);
+              row[pbf::list_off(count++)] = (int32_t)q;
+            }
+          }
+        } else {  // another bin (all but one of the 27, at the same offset for every lane)
+          for (uint32_t q = q0; q < q1; ++q) {
+            const float4 xq = pst[q];
+            const float d2 = pbf::mag2<true>(pbf::xsub(xp.x, xq.x), pbf::xsub(xp.y, xq.y), pbf::xsub(xp.z, xq.z));
+            if (d2 < P.s2 && count < cap) {
               if (STAGE && staged) row16[count] = (uint16_t)((int)q + off);
               row[pbf::list_off(count++)] = (int32_t)q;
             }
@@ -912,7 +921,8 @@ __device__ __forceinline__ void density_lambda_tile(int tile, const Dev& P, cons
 
 // The residual check runs on a persistent grid walking the tiles, so that
 // once the step has converged the launch costs a few hundred empty blocks.
-template <int MODE, int GL>
+// LOOP: a check inside the graph's conditional loop (pbf::decide_if_last).
+template <int MODE, int GL, bool LOOP = false>
 __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) kf_density_lambda(Dev P, Fast F, int n, size_t stride,
                                                             const int32_t* __restrict__ nbr,
                                                             const int32_t* __restrict__ cnt,
@@ -920,7 +930,8 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) kf_density_lambda(De
                                                             float* lam, uint32_t* nudge, LearnIO io) {
   if (MODE == kDlCheck && io.state->done) {
     // a check after the step converged: it ends the loop it runs in
-    if (io.loop.use && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(io.loop.cond, 0u);
+    if constexpr (LOOP)
+      if (io.loop.use && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(io.loop.cond, 0u);
     return;
   }
   const int tiles = pbf::tiles_of<GL>(n);
@@ -929,7 +940,7 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) kf_density_lambda(De
     density_lambda_tile<MODE, GL>(tile, P, F, n, stride, nbr, cnt, pst, xl, vel, lam, nudge, io, err);
   if (MODE == kDlCheck) {
     pbf::block_partial<kBlock>(err, io.partials + blockIdx.x);
-    pbf::decide_if_last<kBlock>(io.state, io.partials, n, io.tol, io.final_check, io.loop);
+    pbf::decide_if_last<kBlock, LOOP>(io.state, io.partials, n, io.tol, io.final_check, io.loop);
   }
 }
 
@@ -969,7 +980,7 @@ __device__ __forceinline__ int stage_tile(const TileIO& T, int tile, const float
   return nr > 0 ? total : -1;
 }
 
-template <int MODE>
+template <int MODE, bool LOOP = false>
 __global__ void __launch_bounds__(kStageThreads) ks_density_lambda(Dev P, Fast F, int n, size_t stride,
                                                                   const int32_t* __restrict__ nbr,
                                                                   const int32_t* __restrict__ cnt,
@@ -978,7 +989,8 @@ __global__ void __launch_bounds__(kStageThreads) ks_density_lambda(Dev P, Fast F
                                                                   TileIO T) {
   __shared__ float4 stage[kStageMax + 1];
   if (MODE == kDlCheck && io.state->done) {
-    if (io.loop.use && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(io.loop.cond, 0u);
+    if constexpr (LOOP)
+      if (io.loop.use && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(io.loop.cond, 0u);
     return;
   }
   const int tiles = (n + kTile - 1) / kTile;
@@ -994,7 +1006,7 @@ __global__ void __launch_bounds__(kStageThreads) ks_density_lambda(Dev P, Fast F
   }
   if (MODE == kDlCheck) {
     pbf::block_partial<kStageThreads>(err, io.partials + blockIdx.x);
-    pbf::decide_if_last<kStageThreads>(io.state, io.partials, n, io.tol, io.final_check, io.loop);
+    pbf::decide_if_last<kStageThreads, LOOP>(io.state, io.partials, n, io.tol, io.final_check, io.loop);
   }
 }
 
@@ -2219,11 +2231,13 @@ int update_shapes(pbf_ctx* ctx) {
   };
   const pbf_tuning& t = ctx->tune;
   if (t.staged[PBF_TUNE_DENSITY])
-    ctx->pgrid_check = resident((const void*)ks_density_lambda<kDlCheck>, kStageThreads);
+    ctx->pgrid_check = std::min(resident((const void*)ks_density_lambda<kDlCheck, false>, kStageThreads),
+                                resident((const void*)ks_density_lambda<kDlCheck, true>, kStageThreads));
   else
     with_lanes(t.lanes[PBF_TUNE_DENSITY], [&](auto gl) {
-      ctx->pgrid_check = resident((const void*)kf_density_lambda<kDlCheck, decltype(gl)::value>,
-                                  t.block[PBF_TUNE_DENSITY]);
+      constexpr int GL = decltype(gl)::value;
+      ctx->pgrid_check = std::min(resident((const void*)kf_density_lambda<kDlCheck, GL, false>, t.block[PBF_TUNE_DENSITY]),
+                                  resident((const void*)kf_density_lambda<kDlCheck, GL, true>, t.block[PBF_TUNE_DENSITY]));
     });
   if (t.staged[PBF_TUNE_DELTA_P])
     ctx->pgrid_dp = resident((const void*)ks_dp_update<false, false, true>, kStageThreads);
@@ -2421,13 +2435,22 @@ void launch_learned_solve(pbf_ctx* ctx) {
   auto check = [&](cudaStream_t cs, const LearnIO& cio) {
     if (T.staged[PBF_TUNE_DENSITY]) {
       Launch L(ctx, "residual_check");
-      ks_density_lambda<kDlCheck><<<gpc, kStageThreads, 0, cs>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS,
-                                                                 ctx->xl, ctx->velS, ctx->lamH, ctx->nudge, cio, tio);
+      if (cio.loop.use)
+        ks_density_lambda<kDlCheck, true><<<gpc, kStageThreads, 0, cs>>>(
+            P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl, ctx->velS, ctx->lamH, ctx->nudge, cio, tio);
+      else
+        ks_density_lambda<kDlCheck, false><<<gpc, kStageThreads, 0, cs>>>(
+            P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl, ctx->velS, ctx->lamH, ctx->nudge, cio, tio);
     } else {
       with_lanes(T.lanes[PBF_TUNE_DENSITY], [&](auto gl) {
+        constexpr int GL = decltype(gl)::value;
         Launch L(ctx, "residual_check");
-        kf_density_lambda<kDlCheck, decltype(gl)::value><<<gpc, bd, 0, cs>>>(
-            P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl, ctx->velS, ctx->lamH, ctx->nudge, cio);
+        if (cio.loop.use)
+          kf_density_lambda<kDlCheck, GL, true><<<gpc, bd, 0, cs>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS,
+                                                                    ctx->xl, ctx->velS, ctx->lamH, ctx->nudge, cio);
+        else
+          kf_density_lambda<kDlCheck, GL, false><<<gpc, bd, 0, cs>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS,
+                                                                     ctx->xl, ctx->velS, ctx->lamH, ctx->nudge, cio);
       });
     }
   };

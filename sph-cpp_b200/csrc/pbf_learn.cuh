@@ -129,7 +129,10 @@ __device__ __forceinline__ void block_partial(float v, double* out) {
 // fixed order (so the decision is the same on every run) and either stops the
 // step's iterations (mean error at or below tol) or allows one more (the final
 // check of a step only records the residual).
-template <int THREADS>
+// LOOP: the check sits in the graph's conditional loop and sets its handle;
+// a check outside the loop is compiled without the call (a kernel that can
+// set a conditional handle is one ncu cannot profile).
+template <int THREADS, bool LOOP>
 __device__ __forceinline__ void decide_if_last(SolveState* st, const double* partials, int n, float tol,
                                                int final_check, SolveLoop loop) {
   __shared__ unsigned last;
@@ -155,13 +158,15 @@ __device__ __forceinline__ void decide_if_last(SolveState* st, const double* par
   st->ticket = 0u;
   if (mean <= (double)tol) st->done = 1u;
   else if (!final_check) st->iterations += 1u;
-  if (loop.use) {
-    // One more pass of the loop only while the step is not done and another
-    // plain iteration is allowed; `loops` bounds the loop whatever the
-    // residuals do.
-    st->loops += 1u;
-    const bool more = !st->done && st->iterations + 1u < (uint32_t)loop.iters && st->loops < (uint32_t)loop.iters;
-    cudaGraphSetConditional(loop.cond, more ? 1u : 0u);
+  if constexpr (LOOP) {
+    if (loop.use) {
+      // One more pass of the loop only while the step is not done and another
+      // plain iteration is allowed; `loops` bounds the loop whatever the
+      // residuals do.
+      st->loops += 1u;
+      const bool more = !st->done && st->iterations + 1u < (uint32_t)loop.iters && st->loops < (uint32_t)loop.iters;
+      cudaGraphSetConditional(loop.cond, more ? 1u : 0u);
+    }
   }
 }
 
