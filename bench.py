@@ -200,6 +200,8 @@ def kernel_bytes(name: str, n: int, nbar: float, K: int, nbins: int) -> float:
         "apply_vorticity": 16 + 16 + 16 + L + 16,
         "viscosity_final": 16 + 16 + L + 16 + 16 + 16 + 4 + 4,
         "update_velocities": 16 + 16 + 16,
+        # every gather pass of the step in one launch (pbf_set_persistent)
+        "persistent_step": K * ((40 + L) + (32 + L)) + 32 + (48 + L) + (64 + L) + (64 + L) + (96 + L),
         "color_field": 16 + 16 + L + 16,
         "surface_tension": 16 + 16 + 16 + L + 16,
     }
@@ -380,7 +382,9 @@ def batched_run(steps: int = 200, autotune: bool = True) -> dict:
                    64 contexts' `steps`-step chains (pbf_group_step), each
                    scene advancing at its own pace;
       one_context  one context holding all scenes (pbf_create_batch), every
-                   launch covering every scene (pbf_step(ctx, steps)).
+                   launch covering every scene (pbf_step(ctx, steps)), and
+                   (persistent_step) the same with each step's gather
+                   passes in one persistent launch (pbf_set_persistent).
     Each graph is captured by an untimed run of the same call first."""
     import numpy as np
     import torch
@@ -407,6 +411,22 @@ def batched_run(steps: int = 200, autotune: bool = True) -> dict:
         errs = [g.scene_stats(i)["mean_density_error"] for i in range(len(b.scenes))]
         flags = g.stats()["error_flags"]
         launches = g.launches_per_step()
+        # the same context with the persistent step: the list fill and every
+        # gather pass of a step in one launch, each scene at its own pace
+        # through the passes (pbf_set_persistent; its fixed launch shapes)
+        g.set_persistent(True)
+        g.upload(x0)
+        g.step(steps)          # captures the steps-step graph (untimed)
+        g.upload(x0)
+        g.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        g.step(steps)
+        e1.record(stream)
+        e1.synchronize()
+        tp = e0.elapsed_time(e1) / 1e3
+        persistent = {"value": b.n * steps / tp, "ms_per_step": 1e3 * tp / steps, "graph_launches": 1,
+                      "kernel_launches_per_step": g.launches_per_step(), "error_flags": g.stats()["error_flags"]}
     out.update({"value": b.n * steps / t, "unit": UNIT, "steps": steps, "ms_per_step": 1e3 * t / steps,
                 "graph_launches": 1, "kernel_launches_per_step": launches, "tuning": tuning,
                 "scene_mean_density_error": {"min": float(np.min(errs)), "max": float(np.max(errs))},
@@ -467,6 +487,8 @@ def batched_run(steps: int = 200, autotune: bool = True) -> dict:
     one_context = {k: out[k] for k in ("value", "ms_per_step", "graph_launches", "kernel_launches_per_step",
                                        "scene_mean_density_error", "error_flags")}
     one_context["speedup_vs_independent"] = one_context["value"] / out_ind["value"]
+    persistent["speedup_vs_independent"] = persistent["value"] / out_ind["value"]
+    one_context["persistent_step"] = persistent
     res = {"workload": out["workload"], "mode": "scene group: one graph launch of every scene's step chain, "
                                                 "each scene at its own pace (pbf_group_step)",
            "value": b.n * steps / tg, "unit": UNIT, "steps": steps, "ms_per_step": 1e3 * tg / steps,

@@ -54,7 +54,7 @@ extern "C" {
 /* Device-side error flag bits (pbf_stats_t.error_flags). */
 #define PBF_FLAG_KEY_RANGE 1u     /* a bin id fell outside the grid; clamped */
 #define PBF_FLAG_NONFINITE 2u     /* a non-finite position was hashed */
-#define PBF_FLAG_WAIT_TIMEOUT 4u  /* a kernel gave up a bounded wait on the tensor cores; that launch's results are invalid */
+#define PBF_FLAG_WAIT_TIMEOUT 4u  /* a kernel gave up a bounded wait (tensor cores, persistent step); that launch's results are invalid */
 
 /*
  * Parameter block.  Field meaning follows the reference's public
@@ -382,6 +382,32 @@ int pbf_mlp_predict(pbf_ctx* ctx, const float* features, size_t n, float* y);
  * tensor memory and returns; the context stays usable.  Needs a network
  * (pbf_mlp_init or pbf_mlp_set) and a capacity of at least 278 particles. */
 int pbf_selftest_mlp_wait_timeout(pbf_ctx* ctx, uint32_t* flags);
+
+/* ---- persistent step (batches of scenes) ----
+ * No counterpart in the reference.  With enable = 1, each step of a batch
+ * context (pbf_create_batch) runs all its gather passes (the K Jacobi
+ * iterations of density/lambda and delta-p, both XSPH passes, vorticity and
+ * its application) as ONE persistent launch after the list fill, instead of
+ * one launch per pass: blocks take (pass, tile) tasks from a queue, and a tile
+ * waits only until the previous pass has finished in the scenes it covers, so
+ * each scene goes through the passes at its own pace within the step.  The
+ * gathers run at fixed shapes (2 lanes per particle, 4 for vorticity, 128
+ * threads); the results are those of the launch-per-pass step at the same
+ * shapes, bit for bit.  Every wait is bounded (2 s); a launch that gives one
+ * up raises PBF_FLAG_WAIT_TIMEOUT (pbf_stats) and its step's results are
+ * invalid.  Applies to fast math, the plain solver with 1..16 iterations, no
+ * surface tension and no s_corr: PBF_ERR_PARAMS otherwise, PBF_ERR_STATE on a
+ * one-scene context; a later pbf_set_params outside these runs the
+ * launch-per-pass step until it is back inside.  enable = 0 turns it off.
+ * Drops captured graphs. */
+int pbf_set_persistent(pbf_ctx* ctx, int enable);
+/* Self-test of the persistent step's failure path; no counterpart in the
+ * reference.  Runs the persistent kernel's scheduler alone (no particle data
+ * is read or written) on two 4-tile passes whose dependency is never met,
+ * with a 2 ms bound: every waiting block gives up, raises
+ * PBF_FLAG_WAIT_TIMEOUT in *flags (its own status word, not the context's
+ * error flags) and returns; the context stays usable. */
+int pbf_selftest_persistent_wait_timeout(pbf_ctx* ctx, uint32_t* flags);
 
 /* ---- scene groups ----
  * No counterpart in the reference.  Independent contexts (one scene each)

@@ -537,12 +537,13 @@ struct TileIO {
   uint16_t* nbr16;  // [slot][stride] staging index of every list entry
 };
 
+// The list of slot b (a thread's share of k_fill2; the persistent step calls
+// it too, STAGE = false).
 template <bool STAGE>
-__global__ void __launch_bounds__(kFillBlock) k_fill2(Dev P, int n, size_t stride, const float4* __restrict__ pst,
-                                                      const uint32_t* __restrict__ cell_start,
-                                                      const uint32_t* __restrict__ run_end, int32_t* nbr,
-                                                      int32_t* cnt, uint32_t* err, TileIO T) {
-  const int b = blockIdx.x * kFillBlock + threadIdx.x;
+__device__ __forceinline__ void fill_thread(int b, const Dev& P, int n, size_t stride, const float4* __restrict__ pst,
+                                            const uint32_t* __restrict__ cell_start,
+                                            const uint32_t* __restrict__ run_end, int32_t* nbr, int32_t* cnt,
+                                            uint32_t* err, const TileIO& T) {
   if (!STAGE && b >= n) return;
   if (STAGE && (b & ~(kTile - 1)) >= n) return;  // a whole warp past the end: no tile (warp-uniform)
   const bool live = b < n;
@@ -675,6 +676,14 @@ done:
   cnt[b] = count;
   // a bin outside the tile's box (float re-hash at a bin face): the tile walks the int32 lists
   if (STAGE && stray) T.nruns[tile] = 0;
+}
+
+template <bool STAGE>
+__global__ void __launch_bounds__(kFillBlock) k_fill2(Dev P, int n, size_t stride, const float4* __restrict__ pst,
+                                                      const uint32_t* __restrict__ cell_start,
+                                                      const uint32_t* __restrict__ run_end, int32_t* nbr,
+                                                      int32_t* cnt, uint32_t* err, TileIO T) {
+  fill_thread<STAGE>(blockIdx.x * kFillBlock + threadIdx.x, P, n, stride, pst, cell_start, run_end, nbr, cnt, err, T);
 }
 
 // ---- density (particles.h:292-313) ----
@@ -843,7 +852,7 @@ struct DensitySums {
 // STAGED: the neighbour records come from the tile's staging area `src` in
 // shared memory through the 16-bit list row16; else from `src` in global
 // memory through the int32 list row.  `dummy` names the zero record.
-template <int GL, bool NH, bool STAGED = false>
+template <int GL, bool NH, bool STAGED = false, bool COH = false>
 __device__ __forceinline__ DensitySums density_sums(const Fast& F, const pbf::Group& G, const int32_t* row,
                                                     const uint16_t* row16, int c, int dummy, const float4* src,
                                                     float4 xp) {
@@ -864,7 +873,7 @@ __device__ __forceinline__ DensitySums density_sums(const Fast& F, const pbf::Gr
   if (STAGED)
     pbf::swalk1<GL>(row16, c, dummy, G.lane, src, body);
   else
-    pbf::gwalk1<GL>(row, c, dummy, G.lane, src, body);
+    pbf::gwalk1<GL, false, COH>(row, c, dummy, G.lane, src, body);
   S.sw = pbf::gsum<GL>(S.sw);
   S.s1x = pbf::gsum<GL>(S.s1x);
   S.s1y = pbf::gsum<GL>(S.s1y);
@@ -875,7 +884,8 @@ __device__ __forceinline__ DensitySums density_sums(const Fast& F, const pbf::Gr
   return S;
 }
 
-template <int MODE, int GL, bool STAGED = false>
+// COH: inside the persistent step (pbf::ldw).
+template <int MODE, int GL, bool STAGED = false, bool COH = false>
 __device__ __forceinline__ void density_lambda_tile(int tile, const Dev& P, const Fast& F, int n, size_t stride,
                                                     const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
                                                     const float4* __restrict__ pst, float4* xl, float4* vel,
@@ -886,7 +896,7 @@ __device__ __forceinline__ void density_lambda_tile(int tile, const Dev& P, cons
   const int b = G.b;
   const float4 xp = pst[b];
   const int c = G.live ? cnt[b] : 0;
-  const DensitySums S = density_sums<GL, MODE == kDlRecord, STAGED>(
+  const DensitySums S = density_sums<GL, MODE == kDlRecord, STAGED, COH>(
       F, G, nbr + pbf::list_base(b, stride), STAGED ? nbr16 + (size_t)b * stride : nullptr, c, STAGED ? staged : n,
       STAGED ? stage : pst, xp);
   const float rho = fmaf(F.m_poly, S.sw, F.m_w0);
@@ -1561,7 +1571,7 @@ struct Src {
   int dummy;              // index of the zero record
 };
 
-template <bool SCORR, bool LAST, int GL, bool STAGED = false>
+template <bool SCORR, bool LAST, int GL, bool STAGED = false, bool COH = false>
 __device__ __forceinline__ void dp_update_tile(int tile, const Dev& P, const Fast& F, int n, size_t stride,
                                                const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
                                                const float4* __restrict__ xl, float4* pst,
@@ -1573,8 +1583,9 @@ __device__ __forceinline__ void dp_update_tile(int tile, const Dev& P, const Fas
   const int c = G.live ? cnt[b] : 0;
   float ax = 0.f, ay = 0.f, az = 0.f;
   const float lp = xp.w;
-  pbf::walk1<GL, STAGED>(nbr + pbf::list_base(b, stride), STAGED ? src.nbr16 + (size_t)b * stride : nullptr, c,
-                         STAGED ? src.dummy : n, G.lane, STAGED ? src.a : xl, [&](int, float4 xq) {
+  pbf::walk1<GL, STAGED, false, COH>(nbr + pbf::list_base(b, stride),
+                                     STAGED ? src.nbr16 + (size_t)b * stride : nullptr, c, STAGED ? src.dummy : n,
+                                     G.lane, STAGED ? src.a : xl, [&](int, float4 xq) {
     const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
     const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
     float l = lp + xq.w;
@@ -1636,7 +1647,7 @@ __global__ void __launch_bounds__(kStageThreads) ks_dp_update(Dev P, Fast F, int
   }
 }
 
-template <bool FINAL, int GL, bool STAGED = false>
+template <bool FINAL, int GL, bool STAGED = false, bool COH = false>
 __device__ __forceinline__ void viscosity_tile(int tile, const Fast& F, int n, size_t stride,
                                                const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
                                                const float4* __restrict__ pst, const float4* __restrict__ vin,
@@ -1648,9 +1659,10 @@ __device__ __forceinline__ void viscosity_tile(int tile, const Fast& F, int n, s
   const float4 xp = pst[b], vp = vin[b];
   const int c = G.live ? cnt[b] : 0;
   float ax = 0.f, ay = 0.f, az = 0.f;
-  pbf::walk2<GL, STAGED, FINAL>(nbr + pbf::list_base(b, stride), STAGED ? src.nbr16 + (size_t)b * stride : nullptr, c,
-                         STAGED ? src.dummy : n, G.lane, STAGED ? src.a : pst, STAGED ? src.b : vin,
-                         [&](int, float4 xq, float4 vq) {
+  pbf::walk2<GL, STAGED, FINAL, COH>(nbr + pbf::list_base(b, stride),
+                                     STAGED ? src.nbr16 + (size_t)b * stride : nullptr, c, STAGED ? src.dummy : n,
+                                     G.lane, STAGED ? src.a : pst, STAGED ? src.b : vin,
+                                     [&](int, float4 xq, float4 vq) {
     const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
     const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
     const float wr = __fdividef(pbf::poly_cube(F, d2), vq.w);
@@ -1699,7 +1711,7 @@ __global__ void __launch_bounds__(kStageThreads) ks_viscosity(Dev P, Fast F, int
     viscosity_tile<FINAL, 4>(tile, F, n, stride, nbr, cnt, pst, vin, vout, posH, pstH, origS, origH);
 }
 
-template <int GL, bool STAGED = false>
+template <int GL, bool STAGED = false, bool COH = false>
 __device__ __forceinline__ void vorticity_tile(int tile, const Fast& F, int n, size_t stride,
                                                const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
                                                const float4* __restrict__ pst, const float4* __restrict__ vel,
@@ -1709,8 +1721,9 @@ __device__ __forceinline__ void vorticity_tile(int tile, const Fast& F, int n, s
   const float4 xp = pst[b], vp = vel[b];
   const int c = G.live ? cnt[b] : 0;
   float wx = 0.f, wy = 0.f, wz = 0.f;
-  pbf::walk2<GL, STAGED>(nbr + pbf::list_base(b, stride), STAGED ? src.nbr16 + (size_t)b * stride : nullptr, c,
-                         STAGED ? src.dummy : n, G.lane, STAGED ? src.a : pst, STAGED ? src.b : vel,
+  pbf::walk2<GL, STAGED, false, COH>(nbr + pbf::list_base(b, stride),
+                                     STAGED ? src.nbr16 + (size_t)b * stride : nullptr, c, STAGED ? src.dummy : n,
+                                     G.lane, STAGED ? src.a : pst, STAGED ? src.b : vel,
                          [&](int, float4 xq, float4 vq) {
     const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
     const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
@@ -1753,7 +1766,7 @@ __global__ void __launch_bounds__(kStageThreads) ks_vorticity(Dev P, Fast F, int
     vorticity_tile<4>(tile, F, n, stride, nbr, cnt, pst, vel, scr, xl);
 }
 
-template <int GL, bool STAGED = false>
+template <int GL, bool STAGED = false, bool COH = false>
 __device__ __forceinline__ void apply_vorticity_tile(int tile, const Fast& F, int n, size_t stride,
                                                      const int32_t* __restrict__ nbr,
                                                      const int32_t* __restrict__ cnt,
@@ -1764,8 +1777,9 @@ __device__ __forceinline__ void apply_vorticity_tile(int tile, const Fast& F, in
   const float4 xp = xl[b];
   const int c = G.live ? cnt[b] : 0;
   float ex = 0.f, ey = 0.f, ez = 0.f;
-  pbf::walk1<GL, STAGED>(nbr + pbf::list_base(b, stride), STAGED ? src.nbr16 + (size_t)b * stride : nullptr, c,
-                         STAGED ? src.dummy : n, G.lane, STAGED ? src.a : xl, [&](int, float4 xq) {
+  pbf::walk1<GL, STAGED, false, COH>(nbr + pbf::list_base(b, stride),
+                                     STAGED ? src.nbr16 + (size_t)b * stride : nullptr, c, STAGED ? src.dummy : n,
+                                     G.lane, STAGED ? src.a : xl, [&](int, float4 xq) {
     const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
     const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
     const float t = xq.w * pbf::spikey_over_r(F, d2);
@@ -1809,6 +1823,198 @@ __global__ void __launch_bounds__(kStageThreads) ks_apply_vorticity(Dev P, Fast 
     apply_vorticity_tile<4, true>(tile, F, n, stride, nbr, cnt, xl, scr, vel, Src{T.nbr16, stage, nullptr, staged});
   else
     apply_vorticity_tile<4>(tile, F, n, stride, nbr, cnt, xl, scr, vel);
+}
+
+// ---- the persistent step (batches of scenes) ----
+// Every gather pass of a fast-math plain step (K Jacobi iterations of
+// density/lambda and delta-p, both XSPH passes, vorticity and its
+// application) as ONE launch, after the list fill's.  Work is a queue of tasks, pass-major: task
+// (pass, tile) is one tile of that pass, tiles over the batch's sorted slots.
+// Blocks take tasks in queue order (an atomic counter) until it is empty.  A
+// tile of pass p reads what pass p-1 wrote in the scenes it covers (a list
+// never leaves its scene), so it waits only until every tile of pass p-1 that
+// covers those scenes has finished: per (pass, scene) counters, each finished
+// tile adding one to the counter of every scene it covers.  A scene whose
+// pass is done goes on to its next pass while a crowded scene of the batch is
+// still in an earlier pass; the launch-per-pass step makes every scene wait
+// for the slowest at every pass.
+//  - No deadlock: a block waits only on tasks earlier in the queue, which
+//    blocks already running have taken; the earliest unfinished task waits on
+//    none.  Any grid size works; a persistent one (SMs x resident blocks) is
+//    used.
+//  - Visibility: a finished tile's writes are fenced (GPU scope) before its
+//    counters are raised; a waiting block reads the counters with acquire
+//    loads before any of its threads reads the data, and the walks read with
+//    plain loads (pbf::ldw<true>), not the read-only path.
+//  - Each block fetches its next task while the current one runs, and a
+//    block that has found pass p-1 finished in some scenes does not wait for
+//    it again for later tiles of pass p in those scenes.
+//  - 12 resident blocks per SM (40 registers, a few spilled): measured the
+//    fastest of 56, 48 and 40 registers on the 64-scene batch.
+//  - Every wait is bounded in time (limit_ns, %globaltimer).  A block that
+//    gives up raises PBF_FLAG_WAIT_TIMEOUT and the abort word, and every block
+//    then returns at its next task or wait: the launch ends, the step's
+//    results are invalid and flagged.
+enum PersistKind { kPDensity = 0, kPDp, kPDpLast, kPVisc, kPVort, kPApply, kPViscFinal };
+constexpr int kPersistThreads = 128;
+constexpr int kPersistTilesPerTask = 1;  // consecutive tiles of one pass per task
+constexpr int kPersistMaxK = 16;
+constexpr int kPersistMaxPasses = 2 * kPersistMaxK + 4;
+// lanes per particle of each gather pass (a tile is kPersistThreads / GL particles)
+constexpr int kPGLDensity = 2, kPGLDp = 2, kPGLVisc = 2, kPGLVort = 4, kPGLApply = 2;
+
+struct PersistPass {
+  int kind, size, first_task, tiles;  // PersistKind, slots per tile, its first task, its tiles
+};
+// (tasks of a pass: ceil(tiles / kPersistTilesPerTask))
+struct PersistPlan {
+  PersistPass pass[kPersistMaxPasses];
+  int npass, tasks, nscenes;
+  int stall_pass;                // -1, or a pass whose dependency is never met (the wait self-test)
+  unsigned long long limit_ns;   // bound of every wait
+  uint32_t* words;               // [0] next task, [1] abort
+  uint32_t* done;                // [npass][nscenes] finished tiles
+  uint32_t* flags;               // PBF_FLAG_WAIT_TIMEOUT is raised here
+  const uint32_t* first;         // [nscenes + 1] first slot of every scene, then the slot count
+};
+struct PersistArrays {
+  float4 *pst, *xl, *vel, *velT, *pos, *scr, *velH, *posH, *pstH;
+  float* lam;
+  uint32_t *nudge, *err, *origH;
+  const uint32_t *cell_start, *run_end, *origS;
+  int32_t *nbr, *cnt;
+};
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// The last scene whose first slot is <= slot.
+__device__ __forceinline__ int persist_scene(const PersistPlan& S, uint32_t slot) {
+  int lo = 0, hi = S.nscenes - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (S.first[mid] <= slot) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Thread 0 of a block: wait until pass p-1 has finished in scenes sa..sb.
+// False when this or another block gave up.
+__device__ bool persist_wait(const PersistPlan& S, int p, int sa, int sb) {
+  const PersistPass q = S.pass[p - 1];
+  const unsigned long long t0 = globaltimer_ns();
+  for (int s = sa; s <= sb; ++s) {
+    const uint32_t f = S.first[s], e = S.first[s + 1];
+    if (e == f) continue;  // an empty scene has no tiles
+    uint32_t need = (e - 1) / (uint32_t)q.size - f / (uint32_t)q.size + 1u;
+    if (p == S.stall_pass) need += 1u;  // one tile more than exist: the self-test's wait
+    const uint32_t* c = S.done + (size_t)(p - 1) * S.nscenes + s;
+    unsigned sleep = 128;  // polls back off, so that waiting blocks leave the counters' L2 slice alone
+    while (ld_acquire_gpu(c) < need) {
+      if (ld_acquire_gpu(S.words + 1) != 0u) return false;
+      if (globaltimer_ns() - t0 > S.limit_ns) {
+        atomicOr(S.flags, PBF_FLAG_WAIT_TIMEOUT);
+        atomicExch(S.words + 1, 1u);
+        return false;
+      }
+      __nanosleep(sleep);
+      sleep = min(2u * sleep, 8192u);
+    }
+  }
+  return true;
+}
+
+// DRY: the scheduler and its waits only, no tile work (the wait self-test).
+template <bool DRY>
+__global__ void __launch_bounds__(kPersistThreads, 12)
+    k_persist(Dev P, Fast F, int n, size_t stride, PersistPlan S, PersistArrays A) {
+  __shared__ int s_task, s_ok;
+  // thread 0: the task after the current one (fetched while the current one
+  // runs) and the last (pass, scenes) it found finished, which later tasks of
+  // the same pass in those scenes need not wait for again
+  int next = 0, cp = -1, csa = 0, csb = -1;
+  if (threadIdx.x == 0) s_task = (int)atomicAdd(S.words, 1u);
+  __syncthreads();
+  for (;;) {
+    const int task = s_task;
+    if (task >= S.tasks) return;
+    if (threadIdx.x == 0) next = (int)atomicAdd(S.words, 1u);
+    int p = 0;
+    while (p + 1 < S.npass && task >= S.pass[p + 1].first_task) ++p;
+    const int kind = S.pass[p].kind, size = S.pass[p].size;
+    const int t0 = (task - S.pass[p].first_task) * kPersistTilesPerTask;
+    const int t1 = min(t0 + kPersistTilesPerTask, S.pass[p].tiles);
+    const uint32_t a = (uint32_t)t0 * (uint32_t)size;
+    const uint32_t z = min((uint32_t)t1 * (uint32_t)size, (uint32_t)n) - 1u;
+    const int sa = persist_scene(S, a), sb = persist_scene(S, z);
+    if (threadIdx.x == 0) {
+      bool ok = true;
+      if (p > 0 && !(p == cp && sa >= csa && sb <= csb)) {
+        ok = persist_wait(S, p, sa, sb);
+        __threadfence();
+        cp = p;
+        csa = sa;
+        csb = sb;
+      }
+      s_ok = ok;
+    }
+    __syncthreads();
+    if (!s_ok) return;
+    for (int tile = t0; !DRY && tile < t1; ++tile) {
+      switch (kind) {
+        case kPDensity: {
+          float err = 0.0f;
+          const LearnIO io{};
+          density_lambda_tile<kDlPlain, kPGLDensity, false, true>(tile, P, F, n, stride, A.nbr, A.cnt, A.pst, A.xl,
+                                                                  A.vel, A.lam, A.nudge, io, err);
+          break;
+        }
+        case kPDp:
+          dp_update_tile<false, false, kPGLDp, false, true>(tile, P, F, n, stride, A.nbr, A.cnt, A.xl, A.pst, A.pos,
+                                                            A.vel, nullptr);
+          break;
+        case kPDpLast:
+          dp_update_tile<false, true, kPGLDp, false, true>(tile, P, F, n, stride, A.nbr, A.cnt, A.xl, A.pst, A.pos,
+                                                           A.vel, nullptr);
+          break;
+        case kPVisc:
+          viscosity_tile<false, kPGLVisc, false, true>(tile, F, n, stride, A.nbr, A.cnt, A.pst, A.vel, A.velT,
+                                                       nullptr, nullptr, nullptr, nullptr);
+          break;
+        case kPVort:
+          vorticity_tile<kPGLVort, false, true>(tile, F, n, stride, A.nbr, A.cnt, A.pst, A.velT, A.scr, A.xl);
+          break;
+        case kPApply:
+          apply_vorticity_tile<kPGLApply, false, true>(tile, F, n, stride, A.nbr, A.cnt, A.xl, A.scr, A.velT);
+          break;
+        default:
+          viscosity_tile<true, kPGLVisc, false, true>(tile, F, n, stride, A.nbr, A.cnt, A.pst, A.velT, A.velH,
+                                                      A.posH, A.pstH, A.origS, A.origH);
+          break;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();  // the tiles' writes before their counters
+      for (int tile = t0; tile < t1; ++tile) {
+        const uint32_t ta = (uint32_t)tile * (uint32_t)size;
+        const uint32_t tz = min(ta + (uint32_t)size, (uint32_t)n) - 1u;
+        const int ua = persist_scene(S, ta), ub = persist_scene(S, tz);
+        for (int s = ua; s <= ub; ++s) atomicAdd(S.done + (size_t)p * S.nscenes + s, 1u);
+      }
+      s_task = *(volatile const uint32_t*)(S.words + 1) ? S.tasks : next;  // another block gave up: stop
+    }
+    __syncthreads();
+  }
 }
 
 // Residual statistics (no state change): density over the current lists,
@@ -1939,6 +2145,12 @@ struct pbf_ctx {
   std::vector<uint32_t> scene_first;
   pbf::Region* d_regions = nullptr;
   uint32_t* d_scene_first = nullptr;
+
+  // persistent step (pbf_set_persistent): its task counter and abort word,
+  // the [pass][scene] tile counters, the grid
+  bool persistent = false;
+  uint32_t *persist_words = nullptr, *persist_done = nullptr;
+  int persist_grid = 0;
 
   std::map<int, cudaGraphExec_t> graphs;
   uint64_t graph_epoch = 0;  // counts drop_graphs: a scene group rebuilds when a member's changes
@@ -2155,6 +2367,48 @@ void drop_graphs(pbf_ctx* ctx) {
   ctx->graph_epoch++;
 }
 
+// The configurations the persistent step runs: a batch of scenes, fast math,
+// the plain solver with 1..kPersistMaxK iterations, no surface tension, no
+// s_corr.  Any other runs the launch-per-pass step.
+bool persist_supported(const pbf_ctx* ctx) {
+  const pbf_params& p = ctx->params;
+  return !ctx->scenes.empty() && !p.exact_math && p.solver == 0 && p.gamma == 0.0f && !(p.scorr_k > 0.0f) &&
+         p.solve_steps >= 1 && p.solve_steps <= kPersistMaxK;
+}
+bool persist_on(const pbf_ctx* ctx) { return ctx->persistent && persist_supported(ctx) && ctx->n > 0; }
+
+// The task queue of one persistent step over the context's n slots.
+PersistPlan persist_plan(const pbf_ctx* ctx) {
+  PersistPlan S{};
+  const int n = (int)ctx->n;
+  int np = 0, task = 0;
+  auto add = [&](int kind, int size) {
+    const int tiles = (n + size - 1) / size;
+    S.pass[np++] = PersistPass{kind, size, task, tiles};
+    task += (tiles + kPersistTilesPerTask - 1) / kPersistTilesPerTask;
+  };
+  const int K = ctx->params.solve_steps;
+  for (int it = 0; it < K; ++it) {
+    add(kPDensity, kPersistThreads / kPGLDensity);
+    add(it == K - 1 ? kPDpLast : kPDp, kPersistThreads / kPGLDp);
+  }
+  add(kPVisc, kPersistThreads / kPGLVisc);
+  add(kPVort, kPersistThreads / kPGLVort);
+  add(kPApply, kPersistThreads / kPGLApply);
+  add(kPViscFinal, kPersistThreads / kPGLVisc);
+  S.npass = np;
+  S.tasks = task;
+  S.nscenes = (int)ctx->scenes.size();
+  S.stall_pass = -1;
+  S.limit_ns = 2000000000ull;  // 2 s: far above any tile's work, short of a watchdog
+  S.words = ctx->persist_words;
+  S.done = ctx->persist_done;
+  S.flags = ctx->err;
+  S.first = ctx->d_scene_first;
+  return S;
+}
+
+
 // Stage spans are [0, e) with e <= n: the particles of reference index below
 // e (a multi-rank driver's resident particles, Simulation/Source/main.adios);
 // the others are halo particles the stage reads but leaves as they are.
@@ -2363,6 +2617,37 @@ void launch_fill(pbf_ctx* ctx, const float4* pst) {
         tile_io(ctx));
 }
 
+// The list fill, then every gather pass of the step in one launch.
+void launch_persistent(pbf_ctx* ctx) {
+  cudaStream_t s = ctx->stream;
+  const int n = (int)ctx->n;
+  launch_fill(ctx, ctx->pstS);
+  const PersistPlan S = persist_plan(ctx);
+  cudaMemsetAsync(ctx->persist_words, 0, 2 * sizeof(uint32_t), s);
+  cudaMemsetAsync(ctx->persist_done, 0, (size_t)S.npass * S.nscenes * sizeof(uint32_t), s);
+  PersistArrays A{};
+  A.pst = ctx->pstS;
+  A.xl = ctx->xl;
+  A.vel = ctx->velS;
+  A.velT = ctx->velT;
+  A.pos = ctx->posS;
+  A.scr = ctx->scrH;
+  A.velH = ctx->velH;
+  A.posH = ctx->posH;
+  A.pstH = ctx->pstH;
+  A.lam = ctx->lamH;
+  A.nudge = ctx->nudge;
+  A.err = ctx->err;
+  A.origH = ctx->origH;
+  A.cell_start = ctx->cell_start;
+  A.run_end = ctx->run_end;
+  A.origS = ctx->origS;
+  A.nbr = ctx->nbr;
+  A.cnt = ctx->cnt;
+  Launch L(ctx, "persistent_step");
+  k_persist<false><<<ctx->persist_grid, kPersistThreads, 0, s>>>(ctx->dev, ctx->fast, n, ctx->lstride, S, A);
+}
+
 // ---- the fused step (graph-capturable: fixed pointers, no host sync) ----
 pbf::MlpDev mlp_dev(const pbf_ctx* ctx) {
   pbf::MlpDev M;
@@ -2542,6 +2827,10 @@ void launch_step_t(pbf_ctx* ctx) {
                                           keep ? ctx->lamsumH : nullptr, ctx->posS, ctx->pstS, ctx->velS, nullptr,
                                           keep ? ctx->lamprevS : nullptr, ctx->origS, ctx->keyH);
   }
+  if (!X && !SCORR && persist_on(ctx)) {
+    launch_persistent(ctx);
+    return;
+  }
   launch_fill(ctx, ctx->pstS);
   const int K = ctx->params.solve_steps;
   const Fast& F = ctx->fast;
@@ -2719,6 +3008,7 @@ int launches_per_step(const pbf_ctx* ctx) {
   // (density/lambda, [exact: lambda fix-up], delta-p) + (K==0: velocity)
   // + 2 if gamma + 4 (visc, vort, apply, visc)
   const int sort = 5 * ctx->radix_passes;
+  if (persist_on(ctx)) return 1 + 3 + sort + 1 + 2 + 1;  // ... reorder, runs, fill, the persistent step
   const int K = ctx->params.solve_steps;
   const int tail = (ctx->params.gamma != 0.0f ? 2 : 0) + 4;
   if (ctx->params.solver == 1 && !ctx->params.exact_math) {
@@ -3836,6 +4126,63 @@ int pbf_selftest_mlp_wait_timeout(pbf_ctx* ctx, uint32_t* flags) {
                                                                    nullptr, dy, status);
   if (int rc = check_launch(ctx, "selftest_mlp_wait_timeout")) return rc;
   CK(cudaMemcpyAsync(flags, status, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PBF_OK;
+}
+
+int pbf_set_persistent(pbf_ctx* ctx, int enable) {
+  if (!ctx) return PBF_ERR_ARG;
+  if (!enable) {
+    if (ctx->persistent) drop_graphs(ctx);
+    ctx->persistent = false;
+    return PBF_OK;
+  }
+  if (ctx->scenes.empty())
+    return fail(ctx, PBF_ERR_STATE, "the persistent step runs batches of scenes (pbf_create_batch)");
+  if (!persist_supported(ctx))
+    return fail(ctx, PBF_ERR_PARAMS, "the persistent step runs fast math, the plain solver with 1..%d iterations, "
+                                     "no surface tension and no s_corr", kPersistMaxK);
+  if (!ctx->persist_words) {
+    int rc;
+    if ((rc = dalloc(ctx, &ctx->persist_words, 2)) ||
+        (rc = dalloc(ctx, &ctx->persist_done, (size_t)kPersistMaxPasses * ctx->scenes.size())))
+      return rc;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persist<false>, kPersistThreads, 0) != cudaSuccess ||
+        per_sm <= 0)
+      per_sm = 1;
+    ctx->persist_grid = ctx->sms * per_sm;
+  }
+  if (!ctx->persistent) drop_graphs(ctx);
+  ctx->persistent = true;
+  return PBF_OK;
+}
+
+int pbf_selftest_persistent_wait_timeout(pbf_ctx* ctx, uint32_t* flags) {
+  if (!ctx || !flags) return PBF_ERR_ARG;
+  if (6 * ctx->capacity < 8)
+    return fail(ctx, PBF_ERR_CAPACITY, "the self-test needs a context of at least 2 particles");
+  // scratch in the staging area: words[2], done[2], flags, first[2]
+  uint32_t* w = reinterpret_cast<uint32_t*>(ctx->stage);
+  const uint32_t host[7] = {0u, 0u, 0u, 0u, 0u, 0u, 4u * kPersistThreads};
+  CK(cudaMemcpyAsync(w, host, sizeof(host), cudaMemcpyHostToDevice, ctx->stream));
+  PersistPlan S{};
+  const int tasks = (4 + kPersistTilesPerTask - 1) / kPersistTilesPerTask;  // per pass
+  S.pass[0] = PersistPass{kPDensity, kPersistThreads, 0, 4};
+  S.pass[1] = PersistPass{kPDp, kPersistThreads, tasks, 4};
+  S.npass = 2;
+  S.tasks = 2 * tasks;
+  S.nscenes = 1;
+  S.stall_pass = 1;
+  S.limit_ns = 2000000ull;  // 2 ms
+  S.words = w;
+  S.done = w + 2;
+  S.flags = w + 4;
+  S.first = w + 5;
+  k_persist<true><<<8, kPersistThreads, 0, ctx->stream>>>(ctx->dev, ctx->fast, 4 * kPersistThreads, ctx->lstride, S,
+                                                         PersistArrays{});
+  if (int rc = check_launch(ctx, "selftest_persistent_wait_timeout")) return rc;
+  CK(cudaMemcpyAsync(flags, S.flags, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   return PBF_OK;
 }

@@ -119,6 +119,20 @@ __device__ __forceinline__ int vec2_at(int v) { return (v >> 2) * (kListTile * k
 // lane l's vector sits at vec4_at(l) / vec2_at(l) from there.
 constexpr int kBatchVecs = kListTile * kListChunk / 8;  // x GL: vectors per batch
 
+// Loads of the walks.  The read-only path (__ldg, ld.global.nc) for arrays
+// no thread writes during the launch; COH: plain loads (ld.global, cached in
+// L1), for the persistent step, one launch whose passes write what later
+// passes read.  A pass there reads only after an acquire at GPU scope, which
+// drops the SM's L1 lines that other SMs have written since; the read-only
+// path promises no such thing.
+template <bool COH, class T>
+__device__ __forceinline__ T ldw(const T* p) {
+  if constexpr (COH)
+    return *p;
+  else
+    return __ldg(p);
+}
+
 // The last batch: entries of vector v (entries 4v..4v+3, or 2v, 2v+1) at or
 // past the count c name `dummy`.
 __device__ __forceinline__ int4 tail4(int4 q, int v, int c, int dummy) {
@@ -146,7 +160,7 @@ __device__ __forceinline__ int2 tail2(int2 q, int v, int c, int dummy) {
 // one DRAM round trip per batch off the index -> record chain).  It is set
 // where it measured faster (the final XSPH pass); elsewhere it measured
 // slower (Δp too, since the warp-tiled lists).
-template <int GL = kGL, bool PF = false, class Body>
+template <int GL = kGL, bool PF = false, bool COH = false, class Body>
 __device__ __forceinline__ void gwalk1(const int32_t* __restrict__ row, int c, int dummy, int lane,
                                        const float4* __restrict__ a, Body&& body) {
   static_assert(GL % 2 == 0, "a batch covers whole chunks");
@@ -155,12 +169,13 @@ __device__ __forceinline__ void gwalk1(const int32_t* __restrict__ row, int c, i
   if constexpr (PF) {
     const int batches = (c + 4 * GL - 1) / (4 * GL);
     if (batches == 0) return;
-    int4 next = __ldg(r4 + l0);
+    int4 next = ldw<COH>(r4 + l0);
     for (int t = 0; t < batches; ++t) {
       int4 q = next;
-      if (t + 1 < batches) next = __ldg(r4 + (l0 + (t + 1) * kBatchVecs * GL));
+      if (t + 1 < batches) next = ldw<COH>(r4 + (l0 + (t + 1) * kBatchVecs * GL));
       if (t + 1 == batches) q = tail4(q, t * GL + lane, c, dummy);
-      const float4 v0 = __ldg(a + q.x), v1 = __ldg(a + q.y), v2 = __ldg(a + q.z), v3 = __ldg(a + q.w);
+      const float4 v0 = ldw<COH>(a + q.x), v1 = ldw<COH>(a + q.y);
+      const float4 v2 = ldw<COH>(a + q.z), v3 = ldw<COH>(a + q.w);
       body(q.x, v0);
       body(q.y, v1);
       body(q.z, v2);
@@ -170,16 +185,18 @@ __device__ __forceinline__ void gwalk1(const int32_t* __restrict__ row, int c, i
     const int full = c / (4 * GL);
     int t = 0;
     for (; t < full; ++t) {
-      const int4 q = __ldg(r4 + (l0 + t * kBatchVecs * GL));
-      const float4 v0 = __ldg(a + q.x), v1 = __ldg(a + q.y), v2 = __ldg(a + q.z), v3 = __ldg(a + q.w);
+      const int4 q = ldw<COH>(r4 + (l0 + t * kBatchVecs * GL));
+      const float4 v0 = ldw<COH>(a + q.x), v1 = ldw<COH>(a + q.y);
+      const float4 v2 = ldw<COH>(a + q.z), v3 = ldw<COH>(a + q.w);
       body(q.x, v0);
       body(q.y, v1);
       body(q.z, v2);
       body(q.w, v3);
     }
     if (t * 4 * GL < c) {
-      const int4 q = tail4(__ldg(r4 + (l0 + t * kBatchVecs * GL)), t * GL + lane, c, dummy);
-      const float4 v0 = __ldg(a + q.x), v1 = __ldg(a + q.y), v2 = __ldg(a + q.z), v3 = __ldg(a + q.w);
+      const int4 q = tail4(ldw<COH>(r4 + (l0 + t * kBatchVecs * GL)), t * GL + lane, c, dummy);
+      const float4 v0 = ldw<COH>(a + q.x), v1 = ldw<COH>(a + q.y);
+      const float4 v2 = ldw<COH>(a + q.z), v3 = ldw<COH>(a + q.w);
       body(q.x, v0);
       body(q.y, v1);
       body(q.z, v2);
@@ -191,7 +208,7 @@ __device__ __forceinline__ void gwalk1(const int32_t* __restrict__ row, int c, i
 // Two records per neighbour: entries 2l, 2l+1 of every 2*GL-entry batch (an
 // 8-byte index load), so that four records are in flight per lane, as in the
 // one-record walk; PF as there.
-template <int GL = kGL, bool PF = false, class Body>
+template <int GL = kGL, bool PF = false, bool COH = false, class Body>
 __device__ __forceinline__ void gwalk2(const int32_t* __restrict__ row, int c, int dummy, int lane,
                                        const float4* __restrict__ a, const float4* __restrict__ bsrc,
                                        Body&& body) {
@@ -201,12 +218,13 @@ __device__ __forceinline__ void gwalk2(const int32_t* __restrict__ row, int c, i
   if constexpr (PF) {
     const int batches = (c + 2 * GL - 1) / (2 * GL);
     if (batches == 0) return;
-    int2 next = __ldg(r2 + at(0));
+    int2 next = ldw<COH>(r2 + at(0));
     for (int t = 0; t < batches; ++t) {
       int2 q = next;
-      if (t + 1 < batches) next = __ldg(r2 + at(t + 1));
+      if (t + 1 < batches) next = ldw<COH>(r2 + at(t + 1));
       if (t + 1 == batches) q = tail2(q, t * GL + lane, c, dummy);
-      const float4 a0 = __ldg(a + q.x), b0 = __ldg(bsrc + q.x), a1 = __ldg(a + q.y), b1 = __ldg(bsrc + q.y);
+      const float4 a0 = ldw<COH>(a + q.x), b0 = ldw<COH>(bsrc + q.x);
+      const float4 a1 = ldw<COH>(a + q.y), b1 = ldw<COH>(bsrc + q.y);
       body(q.x, a0, b0);
       body(q.y, a1, b1);
     }
@@ -214,14 +232,16 @@ __device__ __forceinline__ void gwalk2(const int32_t* __restrict__ row, int c, i
     const int full = c / (2 * GL);
     int t = 0;
     for (; t < full; ++t) {
-      const int2 q = __ldg(r2 + at(t));
-      const float4 a0 = __ldg(a + q.x), b0 = __ldg(bsrc + q.x), a1 = __ldg(a + q.y), b1 = __ldg(bsrc + q.y);
+      const int2 q = ldw<COH>(r2 + at(t));
+      const float4 a0 = ldw<COH>(a + q.x), b0 = ldw<COH>(bsrc + q.x);
+      const float4 a1 = ldw<COH>(a + q.y), b1 = ldw<COH>(bsrc + q.y);
       body(q.x, a0, b0);
       body(q.y, a1, b1);
     }
     if (t * 2 * GL < c) {
-      const int2 q = tail2(__ldg(r2 + at(t)), t * GL + lane, c, dummy);
-      const float4 a0 = __ldg(a + q.x), b0 = __ldg(bsrc + q.x), a1 = __ldg(a + q.y), b1 = __ldg(bsrc + q.y);
+      const int2 q = tail2(ldw<COH>(r2 + at(t)), t * GL + lane, c, dummy);
+      const float4 a0 = ldw<COH>(a + q.x), b0 = ldw<COH>(bsrc + q.x);
+      const float4 a1 = ldw<COH>(a + q.y), b1 = ldw<COH>(bsrc + q.y);
       body(q.x, a0, b0);
       body(q.y, a1, b1);
     }
@@ -294,22 +314,22 @@ __device__ __forceinline__ void swalk2(const uint16_t* __restrict__ row16, int c
 }
 
 // One walk for both sources: staged (shared memory, 16-bit list) or direct.
-template <int GL, bool STAGED, bool PF = false, class Body>
+template <int GL, bool STAGED, bool PF = false, bool COH = false, class Body>
 __device__ __forceinline__ void walk1(const int32_t* row, const uint16_t* row16, int c, int dummy, int lane,
                                       const float4* src, Body&& body) {
   if (STAGED)
     swalk1<GL>(row16, c, dummy, lane, src, body);
   else
-    gwalk1<GL, PF>(row, c, dummy, lane, src, body);
+    gwalk1<GL, PF, COH>(row, c, dummy, lane, src, body);
 }
 
-template <int GL, bool STAGED, bool PF = false, class Body>
+template <int GL, bool STAGED, bool PF = false, bool COH = false, class Body>
 __device__ __forceinline__ void walk2(const int32_t* row, const uint16_t* row16, int c, int dummy, int lane,
                                       const float4* sa, const float4* sb, Body&& body) {
   if (STAGED)
     swalk2<GL>(row16, c, dummy, lane, sa, sb, body);
   else
-    gwalk2<GL, PF>(row, c, dummy, lane, sa, sb, body);
+    gwalk2<GL, PF, COH>(row, c, dummy, lane, sa, sb, body);
 }
 
 // (h - r)^2 / r for r < h, else 0 (the Del_Spikey magnitude over r, no norm).

@@ -351,6 +351,19 @@ class Particles:
         self._check(self._lib.pbf_selftest_mlp_wait_timeout(self._ctx, C.byref(out)), "selftest_mlp_wait_timeout")
         return int(out.value)
 
+    def set_persistent(self, enable: bool = True) -> None:
+        """Run each step's list fill and gather passes as one persistent
+        launch, each scene of the batch at its own pace (pbf_set_persistent)."""
+        self._check(self._lib.pbf_set_persistent(self._ctx, int(enable)), "set_persistent")
+
+    def selftest_persistent_wait_timeout(self) -> int:
+        """Run the persistent step's scheduler on a dependency that is never
+        met (pbf_selftest_persistent_wait_timeout); returns the flags it raised."""
+        out = C.c_uint32(0)
+        self._check(self._lib.pbf_selftest_persistent_wait_timeout(self._ctx, C.byref(out)),
+                    "selftest_persistent_wait_timeout")
+        return int(out.value)
+
     # -- instrumentation --
     def set_timing(self, on: bool) -> None:
         self._check(self._lib.pbf_set_timing(self._ctx, int(on)), "set_timing")

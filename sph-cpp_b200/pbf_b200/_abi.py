@@ -195,6 +195,8 @@ SIGNATURES = {
     "pbf_mlp_gradients": (_i, [_vp, _vp, _vp, _sz, _vp, _P(C.c_float)]),
     "pbf_mlp_predict": (_i, [_vp, _vp, _sz, _vp]),
     "pbf_selftest_mlp_wait_timeout": (_i, [_vp, _vp]),
+    "pbf_set_persistent": (_i, [_vp, _i]),
+    "pbf_selftest_persistent_wait_timeout": (_i, [_vp, _vp]),
     "pbf_group_create": (_i, [_vp, _i, _P(_vp)]),
     "pbf_group_step": (_i, [_vp, _i]),
     "pbf_group_sync": (_i, [_vp]),
