@@ -348,7 +348,9 @@ def learned_comparison(scene_name: str, steps: int, warmup: int, target: float =
     """Plain PBF against the learned warm start at equal mean density error
     <= target (1% of rest density): plain runs with the smallest K in 3..12
     that keeps its mean error over the window at or below the target; the
-    learned solver iterates per step until its error is at or below it."""
+    learned solver iterates per step until its error is at or below it
+    (`learned`, residual checks), and, by plain's protocol, with the smallest
+    fixed count that keeps its mean error at or below it (`learned_fixed`)."""
     from pbf_b200.learn import DEFAULT_MODEL, load_model, warm_start_scene
     if not DEFAULT_MODEL.exists():
         return {"unavailable": f"no trained network at {DEFAULT_MODEL.relative_to(ROOT)}"}
@@ -364,10 +366,24 @@ def learned_comparison(scene_name: str, steps: int, warmup: int, target: float =
             break
     learned = solver_run(base.with_(solver=1, residual_tol=target, max_iterations=K), steps, warmup, params, norm,
                          autotune=autotune)
+    # the same protocol as plain's: the smallest fixed count (network + plain
+    # iterations, no residual checks) that keeps the mean error at or below it
+    fixed, tried_fixed = None, {}
+    for m in range(1, K + 1):
+        fixed = solver_run(base.with_(solver=1, residual_tol=0.0, max_iterations=m), steps, warmup, params, norm,
+                           autotune=autotune)
+        tried_fixed[m] = fixed["mean_density_error"]
+        if fixed["mean_density_error"] <= target:
+            fixed = dict(fixed, iterations=m)
+            break
+    else:
+        fixed = None
     return {"workload": f"{base.name}, relaxation epsilon {base.lambda_epsilon}, steps {warmup}..{warmup + steps}",
             "target_mean_density_error": target, "plain_errors_by_K": tried,
             "plain": dict(plain, iterations=K), "learned": dict(learned, residual_tol=target, max_iterations=K),
             "speedup": learned["value"] / plain["value"],
+            "learned_fixed_errors_by_count": tried_fixed, "learned_fixed": fixed,
+            "speedup_fixed": None if fixed is None else fixed["value"] / plain["value"],
             "network": {k: meta.get(k) for k in ("trajectories", "steps", "batch", "lr", "final_loss")}}
 
 

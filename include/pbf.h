@@ -96,7 +96,9 @@ typedef struct pbf_params {
   /* Solver: 0 = the reference's K plain Jacobi iterations; 1 = learned warm
    * start: iteration 1 takes lambda from the per-particle MLP (pbf_mlp_*),
    * then plain iterations run while the mean clamped density error exceeds
-   * residual_tol, at most max_iterations in all (fast math only). */
+   * residual_tol, at most max_iterations in all (fast math only).  With
+   * residual_tol <= 0 the count is fixed: exactly max_iterations, the
+   * network's and max_iterations - 1 plain ones, with no residual checks. */
   int32_t solver;
   float residual_tol;
   int32_t max_iterations;

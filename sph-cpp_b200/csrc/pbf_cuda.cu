@@ -2715,6 +2715,40 @@ void launch_learned_solve(pbf_ctx* ctx) {
           P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS, ctx->posS, ctx->velS, ctx->state, nullptr);
     });
   }
+  if (!(tol > 0.0f)) {
+    // A fixed count (residual_tol <= 0): max_iterations - 1 plain iterations
+    // after the network's, no residual checks.  Each is the plain step's
+    // density/lambda and delta-p pass; the latter adds its lambda to the
+    // step's sum (the next step's feature).
+    for (int r = 1; r < iters; ++r) {
+      if (T.staged[PBF_TUNE_DENSITY]) {
+        Launch L(ctx, "density_lambda");
+        ks_density_lambda<kDlPlain><<<grid_of(ctx, PBF_TUNE_DENSITY), kStageThreads, 0, s>>>(
+            P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl, ctx->velS, ctx->lamH, ctx->nudge, io, tio);
+      } else {
+        with_lanes(T.lanes[PBF_TUNE_DENSITY], [&](auto gl) {
+          Launch L(ctx, "density_lambda");
+          kf_density_lambda<kDlPlain, decltype(gl)::value><<<grid_of(ctx, PBF_TUNE_DENSITY), bd, 0, s>>>(
+              P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl, ctx->velS, ctx->lamH, ctx->nudge, io);
+        });
+      }
+      if (T.staged[PBF_TUNE_DELTA_P]) {
+        Launch L(ctx, "dp_update");
+        ks_dp_update<SCORR, false, false><<<grid_of(ctx, PBF_TUNE_DELTA_P), kStageThreads, 0, s>>>(
+            P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS, ctx->posS, ctx->velS, ctx->state, ctx->lamsumH,
+            tio);
+      } else {
+        with_lanes(T.lanes[PBF_TUNE_DELTA_P], [&](auto gl) {
+          Launch L(ctx, "dp_update");
+          kf_dp_update<SCORR, false, false, decltype(gl)::value><<<grid_of(ctx, PBF_TUNE_DELTA_P), bp, 0, s>>>(
+              P, F, n, st, ctx->nbr, ctx->cnt, ctx->xl, ctx->pstS, ctx->posS, ctx->velS, ctx->state, ctx->lamsumH);
+        });
+      }
+    }
+    Launch L(ctx, "update_velocities");
+    k_update_v<<<g, kBlock, 0, s>>>(P, n, ctx->pstS, ctx->posS, ctx->velS);
+    return;
+  }
   // a residual check (final: the step's last, which only records) and a
   // plain position update, each skipping itself once the step is done
   auto check = [&](cudaStream_t cs, const LearnIO& cio) {
@@ -3011,6 +3045,12 @@ int launches_per_step(const pbf_ctx* ctx) {
   if (persist_on(ctx)) return 1 + 3 + sort + 1 + 2 + 1;  // ... reorder, runs, fill, the persistent step
   const int K = ctx->params.solve_steps;
   const int tail = (ctx->params.gamma != 0.0f ? 2 : 0) + 4;
+  if (ctx->params.solver == 1 && !ctx->params.exact_math && !(ctx->params.residual_tol > 0.0f)) {
+    // learned, a fixed count: warm iteration (features, network, delta-p) + (iters-1) x (density, delta-p)
+    // + velocity
+    const int it = ctx->params.max_iterations > 0 ? ctx->params.max_iterations : 1;
+    return 1 + 3 + sort + 1 + 2 + 3 + 2 * (it - 1) + 1 + tail;
+  }
   if (ctx->params.solver == 1 && !ctx->params.exact_math) {
     // learned: warm iteration (features, network, delta-p) + (iters-1) x (check, delta-p)
     // + final check + velocity
@@ -3906,7 +3946,10 @@ static int stats_range(pbf_ctx* ctx, size_t b0, size_t b1, bool clear_flags, pbf
   out->mean_neighbors = acc[5] / n;
   out->cap_hits = hits;
   out->error_flags = err;
-  if (ctx->params.solver == 1) {
+  if (ctx->params.solver == 1 && !(ctx->params.residual_tol > 0.0f)) {  // a fixed count, no checks
+    out->solver_iterations = (uint32_t)std::max(ctx->params.max_iterations, 1);
+    out->solver_residual = -1.0;
+  } else if (ctx->params.solver == 1) {
     pbf::SolveState stt;
     CK(cudaMemcpy(&stt, ctx->state, sizeof(stt), cudaMemcpyDeviceToHost));
     out->solver_iterations = 1u + stt.iterations;

@@ -188,6 +188,42 @@ def test_captured_iteration_loop_matches_eager_launches(tol):
         assert runs[mode][2] == its, (mode, runs[mode][2], its)
 
 
+def test_fixed_count_runs_the_checked_iterations_without_the_checks():
+    """residual_tol <= 0 fixes the count at max_iterations with no residual
+    checks.  From the same state, one step moves every particle exactly as the
+    checked loop does when its tolerance is never met (each check's
+    density/lambda pass is the plain one); the velocities differ only through
+    the density XSPH divides by, which the fixed count takes from its last
+    density pass, as the plain solver does (particles.h:436-447 after the last
+    iteration), and the checked loop from its final check."""
+    from pbf_b200.learn import DEFAULT_MODEL, load_model
+    params, norm, _ = load_model(DEFAULT_MODEL)
+    base = warm_start_scene("dam_8k", solver=1, residual_tol=1e-30, max_iterations=3)
+    with Particles(base.params(), base.n) as w:
+        w.mlp_set(params, norm)
+        w.upload(base.positions())
+        w.step(30)
+        d = w.download()
+    out = {}
+    for tol in (1e-30, 0.0):
+        sc = base.with_(residual_tol=tol)
+        with Particles(sc.params(), sc.n) as g:
+            g.mlp_set(params, norm)
+            g.upload(d["x"], d["v"])
+            g.set_timing(True)
+            g.step(1)
+            kt = g.kernel_times()
+            g.set_timing(False)
+            st = g.stats()
+            assert st["error_flags"] == 0 and st["solver_iterations"] == 3
+            assert sum(v["launches"] for v in kt.values()) == g.launches_per_step()
+            out[tol] = (g.positions(), g.velocities(), kt)
+    assert np.array_equal(out[0.0][0], out[1e-30][0])
+    v0, v1 = out[0.0][1], out[1e-30][1]
+    assert np.abs(v0 - v1).max() <= 1e-3 * np.abs(v1).max()
+    assert "residual_check" not in out[0.0][2] and out[0.0][2]["density_lambda"]["launches"] == 2
+
+
 def test_timing_counts_every_learned_kernel():
     """Eager learned steps (per-kernel timing on) launch exactly what
     launches_per_step reports: the features and the network, then
