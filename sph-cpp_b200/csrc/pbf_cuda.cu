@@ -1647,29 +1647,46 @@ __global__ void __launch_bounds__(kStageThreads) ks_dp_update(Dev P, Fast F, int
   }
 }
 
+// wvis (fast, direct walks): the weights W(r)/rho_q per list entry, written
+// by the first pass and read by the final one (pbf::gwalk2w, pbf::gwalkw).
 template <bool FINAL, int GL, bool STAGED = false, bool COH = false>
 __device__ __forceinline__ void viscosity_tile(int tile, const Fast& F, int n, size_t stride,
                                                const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
                                                const float4* __restrict__ pst, const float4* __restrict__ vin,
                                                float4* vout, float4* posH, float4* pstH,
-                                               const uint32_t* __restrict__ origS, uint32_t* origH,
+                                               const uint32_t* __restrict__ origS, uint32_t* origH, float* wvis,
                                                Src src = Src{nullptr, nullptr, nullptr, 0}) {
   const pbf::Group G = pbf::group_at<GL>(n, tile);
   const int b = G.b;
   const float4 xp = pst[b], vp = vin[b];
   const int c = G.live ? cnt[b] : 0;
   float ax = 0.f, ay = 0.f, az = 0.f;
-  pbf::walk2<GL, STAGED, FINAL, COH>(nbr + pbf::list_base(b, stride),
-                                     STAGED ? src.nbr16 + (size_t)b * stride : nullptr, c, STAGED ? src.dummy : n,
-                                     G.lane, STAGED ? src.a : pst, STAGED ? src.b : vin,
-                                     [&](int, float4 xq, float4 vq) {
+  auto weight = [&](float4 xq, float4 vq) {
     const float dx = xp.x - xq.x, dy = xp.y - xq.y, dz = xp.z - xq.z;
     const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-    const float wr = __fdividef(pbf::poly_cube(F, d2), vq.w);
+    return __fdividef(pbf::poly_cube(F, d2), vq.w);
+  };
+  auto add = [&](float wr, float4 vq) {
     ax = fmaf(vq.x - vp.x, wr, ax);
     ay = fmaf(vq.y - vp.y, wr, ay);
     az = fmaf(vq.z - vp.z, wr, az);
-  });
+  };
+  const int32_t* row = nbr + pbf::list_base(b, stride);
+  if (!STAGED && wvis != nullptr) {
+    float* wrow = wvis + pbf::list_base(b, stride);
+    if (FINAL)
+      pbf::gwalkw<GL, false, COH>(row, wrow, c, n, G.lane, vin, [&](int, float wr, float4 vq) { add(wr, vq); });
+    else
+      pbf::gwalk2w<GL, COH>(row, wrow, c, n, G.lane, pst, vin, [&](int, float4 xq, float4 vq) {
+        const float wr = weight(xq, vq);
+        add(wr, vq);
+        return wr;
+      });
+  } else {
+    pbf::walk2<GL, STAGED, FINAL, COH>(row, STAGED ? src.nbr16 + (size_t)b * stride : nullptr, c,
+                                       STAGED ? src.dummy : n, G.lane, STAGED ? src.a : pst, STAGED ? src.b : vin,
+                                       [&](int, float4 xq, float4 vq) { add(weight(xq, vq), vq); });
+  }
   ax = pbf::gsum<GL>(ax);
   ay = pbf::gsum<GL>(ay);
   az = pbf::gsum<GL>(az);
@@ -1688,8 +1705,9 @@ __global__ void __launch_bounds__(kBlock) kf_viscosity(Dev P, Fast F, int n, siz
                                                        const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
                                                        const float4* __restrict__ pst, const float4* __restrict__ vin,
                                                        float4* vout, float4* posH, float4* pstH,
-                                                       const uint32_t* __restrict__ origS, uint32_t* origH) {
-  viscosity_tile<FINAL, GL>(blockIdx.x, F, n, stride, nbr, cnt, pst, vin, vout, posH, pstH, origS, origH);
+                                                       const uint32_t* __restrict__ origS, uint32_t* origH,
+                                                       float* wvis) {
+  viscosity_tile<FINAL, GL>(blockIdx.x, F, n, stride, nbr, cnt, pst, vin, vout, posH, pstH, origS, origH, wvis);
 }
 
 template <bool FINAL>
@@ -1705,10 +1723,10 @@ __global__ void __launch_bounds__(kStageThreads) ks_viscosity(Dev P, Fast F, int
   const int tile = blockIdx.x;
   const int staged = stage_tile<true>(T, tile, pst, sa, vin, sb);
   if (staged >= 0)
-    viscosity_tile<FINAL, 4, true>(tile, F, n, stride, nbr, cnt, pst, vin, vout, posH, pstH, origS, origH,
+    viscosity_tile<FINAL, 4, true>(tile, F, n, stride, nbr, cnt, pst, vin, vout, posH, pstH, origS, origH, nullptr,
                                    Src{T.nbr16, sa, sb, staged});
   else
-    viscosity_tile<FINAL, 4>(tile, F, n, stride, nbr, cnt, pst, vin, vout, posH, pstH, origS, origH);
+    viscosity_tile<FINAL, 4>(tile, F, n, stride, nbr, cnt, pst, vin, vout, posH, pstH, origS, origH, nullptr);
 }
 
 template <int GL, bool STAGED = false, bool COH = false>
@@ -1879,7 +1897,7 @@ struct PersistPlan {
 };
 struct PersistArrays {
   float4 *pst, *xl, *vel, *velT, *pos, *scr, *velH, *posH, *pstH;
-  float* lam;
+  float *lam, *wvis;
   uint32_t *nudge, *err, *origH;
   const uint32_t *cell_start, *run_end, *origS;
   int32_t *nbr, *cnt;
@@ -1988,7 +2006,7 @@ __global__ void __launch_bounds__(kPersistThreads, 12)
           break;
         case kPVisc:
           viscosity_tile<false, kPGLVisc, false, true>(tile, F, n, stride, A.nbr, A.cnt, A.pst, A.vel, A.velT,
-                                                       nullptr, nullptr, nullptr, nullptr);
+                                                       nullptr, nullptr, nullptr, nullptr, A.wvis);
           break;
         case kPVort:
           vorticity_tile<kPGLVort, false, true>(tile, F, n, stride, A.nbr, A.cnt, A.pst, A.velT, A.scr, A.xl);
@@ -1998,7 +2016,7 @@ __global__ void __launch_bounds__(kPersistThreads, 12)
           break;
         default:
           viscosity_tile<true, kPGLVisc, false, true>(tile, F, n, stride, A.nbr, A.cnt, A.pst, A.velT, A.velH,
-                                                      A.posH, A.pstH, A.origS, A.origH);
+                                                      A.posH, A.pstH, A.origS, A.origH, A.wvis);
           break;
       }
     }
@@ -2109,8 +2127,11 @@ struct pbf_ctx {
   uint32_t *cell_count = nullptr, *cell_start = nullptr, *scan_part = nullptr, *err = nullptr, *nudge = nullptr;
   unsigned long long *pairs = nullptr, *pairs_sorted = nullptr;
   int32_t *nbr = nullptr, *cnt = nullptr;
+  float* wvis = nullptr;  // XSPH weights per list entry (the list's layout), in stage_i's memory
   float* stage = nullptr;  // 6*C floats: two AoS float3 staging areas
-  int32_t* stage_i = nullptr;  // neighbor export staging (C*cap + C)
+  // neighbor export staging (C*cap + C); within a step, the XSPH weights
+  // (wvis: written by the first viscosity pass, read by the final one)
+  int32_t* stage_i = nullptr;
   double* acc = nullptr;
   unsigned long long *maxerr = nullptr, *hits = nullptr;
 
@@ -2636,6 +2657,7 @@ void launch_persistent(pbf_ctx* ctx) {
   A.posH = ctx->posH;
   A.pstH = ctx->pstH;
   A.lam = ctx->lamH;
+  A.wvis = ctx->wvis;
   A.nudge = ctx->nudge;
   A.err = ctx->err;
   A.origH = ctx->origH;
@@ -2983,7 +3005,7 @@ void launch_step_t(pbf_ctx* ctx) {
         Launch L(ctx, "viscosity");
         kf_viscosity<false, decltype(gl)::value><<<gv, bv, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS,
                                                                    ctx->velS, ctx->velT, nullptr, nullptr, nullptr,
-                                                                   nullptr);
+                                                                   nullptr, ctx->wvis);
       });
     }
     if (T.staged[PBF_TUNE_VORTICITY]) {
@@ -3019,7 +3041,7 @@ void launch_step_t(pbf_ctx* ctx) {
         Launch L(ctx, "viscosity_final");
         kf_viscosity<true, decltype(gl)::value><<<gv, bv, 0, s>>>(P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS,
                                                                   ctx->velT, ctx->velH, ctx->posH, ctx->pstH,
-                                                                  ctx->origS, ctx->origH);
+                                                                  ctx->origS, ctx->origH, ctx->wvis);
       });
     }
   }
@@ -3136,8 +3158,9 @@ static int create_ctx(const pbf_params* p, size_t capacity, const pbf_scene* sce
       (rc = dalloc(ctx, &ctx->scan_part, (size_t)ctx->nscan_parts)) || (rc = dalloc(ctx, &ctx->err, 1)) ||
       (rc = dalloc(ctx, &ctx->nudge, 1)) ||
       (rc = dalloc(ctx, &ctx->pairs, C)) || (rc = dalloc(ctx, &ctx->pairs_sorted, C)) || (rc = dalloc(ctx, &ctx->nbr, pbf::list_entries(C, cap))) ||
-      (rc = dalloc(ctx, &ctx->cnt, C)) || (rc = dalloc(ctx, &ctx->stage, 6 * C)) ||
-      (rc = dalloc(ctx, &ctx->stage_i, C * cap + C)) || (rc = dalloc(ctx, &ctx->acc, 8)) ||
+            (rc = dalloc(ctx, &ctx->cnt, C)) || (rc = dalloc(ctx, &ctx->stage, 6 * C)) ||
+      (rc = dalloc(ctx, &ctx->stage_i, std::max(C * cap + C, pbf::list_entries(C, cap)))) ||
+      (rc = dalloc(ctx, &ctx->acc, 8)) ||
       (rc = dalloc(ctx, &ctx->maxerr, 1)) || (rc = dalloc(ctx, &ctx->hits, 1)) ||
       (rc = dalloc(ctx, &ctx->lamsumH, C)) || (rc = dalloc(ctx, &ctx->lamprevS, C)) ||
       (rc = dalloc(ctx, &ctx->featb, C * pbf::kMlpInPad)) ||
@@ -3152,6 +3175,7 @@ static int create_ctx(const pbf_params* p, size_t capacity, const pbf_scene* sce
       (rc = dalloc(ctx, &ctx->mlp_loss, 1)) || (rc = dalloc(ctx, &ctx->w1b, pbf::kMlpH * pbf::kMlpInPad)) ||
       (rc = dalloc(ctx, &ctx->w2b, pbf::kMlpH * pbf::kMlpH)) || (rc = dalloc(ctx, &ctx->w2tb, pbf::kMlpH * pbf::kMlpH)))
     return bail(rc);
+  ctx->wvis = reinterpret_cast<float*>(ctx->stage_i);
   if (!ctx->scenes.empty() &&
       ((rc = dalloc(ctx, &ctx->d_regions, ctx->regions.size())) ||
        (rc = dalloc(ctx, &ctx->d_scene_first, ctx->scene_first.size())) || (rc = upload_scenes(ctx))))

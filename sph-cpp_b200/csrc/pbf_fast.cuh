@@ -248,6 +248,78 @@ __device__ __forceinline__ void gwalk2(const int32_t* __restrict__ row, int c, i
   }
 }
 
+// The XSPH passes' weights W(r)/rho_q per list entry: both viscosity passes
+// weigh a neighbour's velocity by the same value (x* and the densities do not
+// change between them), so the first stores it beside its list entry (the
+// same warp-tiled layout, `wrow` = the weight row of the particle's list row)
+// and the final pass reads it as a coalesced stream instead of gathering the
+// neighbour's x* (one scattered record per entry instead of two).
+// gwalk2 that also stores body's return value per entry:
+template <int GL = kGL, bool COH = false, class Body>
+__device__ __forceinline__ void gwalk2w(const int32_t* __restrict__ row, float* wrow, int c, int dummy, int lane,
+                                        const float4* __restrict__ a, const float4* __restrict__ bsrc, Body&& body) {
+  const int2* r2 = reinterpret_cast<const int2*>(row);
+  float2* w2 = reinterpret_cast<float2*>(wrow);
+  auto at = [&](int t) { return GL % 4 == 0 ? t * kBatchVecs * GL + vec2_at(lane) : vec2_at(t * GL + lane); };
+  auto two = [&](int t, int2 q) {
+    const float4 a0 = ldw<COH>(a + q.x), b0 = ldw<COH>(bsrc + q.x);
+    const float4 a1 = ldw<COH>(a + q.y), b1 = ldw<COH>(bsrc + q.y);
+    const float w0 = body(q.x, a0, b0);
+    const float w1 = body(q.y, a1, b1);
+    w2[at(t)] = make_float2(w0, w1);
+  };
+  const int full = c / (2 * GL);
+  int t = 0;
+  for (; t < full; ++t) two(t, ldw<COH>(r2 + at(t)));
+  if (t * 2 * GL < c) two(t, tail2(ldw<COH>(r2 + at(t)), t * GL + lane, c, dummy));
+}
+
+// The final pass's walk: entry q with its stored weight w and one record
+// (entries past the count: the dummy record, weight 0); PF as gwalk1.
+template <int GL = kGL, bool PF = false, bool COH = false, class Body>
+__device__ __forceinline__ void gwalkw(const int32_t* __restrict__ row, const float* __restrict__ wrow, int c,
+                                       int dummy, int lane, const float4* __restrict__ bsrc, Body&& body) {
+  const int2* r2 = reinterpret_cast<const int2*>(row);
+  const float2* w2 = reinterpret_cast<const float2*>(wrow);
+  auto at = [&](int t) { return GL % 4 == 0 ? t * kBatchVecs * GL + vec2_at(lane) : vec2_at(t * GL + lane); };
+  auto two = [&](int2 q, float2 w) {
+    const float4 b0 = ldw<COH>(bsrc + q.x), b1 = ldw<COH>(bsrc + q.y);
+    body(q.x, w.x, b0);
+    body(q.y, w.y, b1);
+  };
+  auto tail = [&](int t, int2& q, float2& w) {
+    const int e = 2 * (t * GL + lane);
+    if (e >= c) { q.x = dummy; w.x = 0.0f; }
+    if (e + 1 >= c) { q.y = dummy; w.y = 0.0f; }
+  };
+  if constexpr (PF) {
+    const int batches = (c + 2 * GL - 1) / (2 * GL);
+    if (batches == 0) return;
+    int2 next = ldw<COH>(r2 + at(0));
+    float2 wnext = ldw<COH>(w2 + at(0));
+    for (int t = 0; t < batches; ++t) {
+      int2 q = next;
+      float2 w = wnext;
+      if (t + 1 < batches) {
+        next = ldw<COH>(r2 + at(t + 1));
+        wnext = ldw<COH>(w2 + at(t + 1));
+      }
+      if (t + 1 == batches) tail(t, q, w);
+      two(q, w);
+    }
+  } else {
+    const int full = c / (2 * GL);
+    int t = 0;
+    for (; t < full; ++t) two(ldw<COH>(r2 + at(t)), ldw<COH>(w2 + at(t)));
+    if (t * 2 * GL < c) {
+      int2 q = ldw<COH>(r2 + at(t));
+      float2 w = ldw<COH>(w2 + at(t));
+      tail(t, q, w);
+      two(q, w);
+    }
+  }
+}
+
 // ---- staged walks: the tile's neighbour records in shared memory ----
 // The list fill writes, beside each int32 list, a 16-bit list of indices into
 // the tile's staging area (the neighbour bins of a 32-particle tile, copied to
