@@ -102,6 +102,12 @@ typedef struct pbf_params {
   int32_t solver;
   float residual_tol;
   int32_t max_iterations;
+  /* Learned solver's residual checks: 1 (or less) = the mean over every
+   * particle, each check the next iteration's density/lambda pass as well;
+   * S > 1 = the mean over every S-th run of 32 consecutive sorted slots (an
+   * estimate from a spatially spread sample), and the full density/lambda
+   * pass runs only when another iteration follows. */
+  int32_t residual_sample;
 } pbf_params;
 
 /* Physics statistics of the current state (a residual density pass over the

@@ -932,12 +932,15 @@ __device__ __forceinline__ void density_lambda_tile(int tile, const Dev& P, cons
 // The residual check runs on a persistent grid walking the tiles, so that
 // once the step has converged the launch costs a few hundred empty blocks.
 // LOOP: a check inside the graph's conditional loop (pbf::decide_if_last).
-template <int MODE, int GL, bool LOOP = false>
+// COND: a plain pass of the learned solver's sampled checks, skipped once the
+// step has converged.
+template <int MODE, int GL, bool LOOP = false, bool COND = false>
 __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) kf_density_lambda(Dev P, Fast F, int n, size_t stride,
                                                             const int32_t* __restrict__ nbr,
                                                             const int32_t* __restrict__ cnt,
                                                             const float4* __restrict__ pst, float4* xl, float4* vel,
                                                             float* lam, uint32_t* nudge, LearnIO io) {
+  if (COND && io.state->done) return;
   if (MODE == kDlCheck && io.state->done) {
     // a check after the step converged: it ends the loop it runs in
     if constexpr (LOOP)
@@ -952,6 +955,48 @@ __global__ void __launch_bounds__(kBlock, kGatherMinBlocks) kf_density_lambda(De
     pbf::block_partial<kBlock>(err, io.partials + blockIdx.x);
     pbf::decide_if_last<kBlock, LOOP>(io.state, io.partials, n, io.tol, io.final_check, io.loop);
   }
+}
+
+// The learned solver's sampled residual check (residual_sample = S > 1): the
+// density of every S-th run of kProbeRun consecutive sorted slots over its
+// list (runs keep the gathers' neighbour records shared, as in the full pass),
+// the mean clamped error of those particles decided as kDlCheck does
+// (pbf::decide_if_last over the samples); nothing else is written.  The nudge
+// of a coincident neighbour is left out of the estimate.
+constexpr int kProbeRun = 32;
+
+template <int GL, bool LOOP>
+__global__ void __launch_bounds__(kBlock, kGatherMinBlocks) kl_residual_probe(Dev P, Fast F, int n, int stride_s,
+                                                                              size_t stride,
+                                                                              const int32_t* __restrict__ nbr,
+                                                                              const int32_t* __restrict__ cnt,
+                                                                              const float4* __restrict__ pst,
+                                                                              LearnIO io) {
+  if (io.state->done) {
+    if constexpr (LOOP)
+      if (io.loop.use && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(io.loop.cond, 0u);
+    return;
+  }
+  const int span = kProbeRun * stride_s;  // one run sampled per span of slots
+  const int runs = (n + span - 1) / span;
+  const int ns = runs * kProbeRun;        // sample k: slot (k / run) * span + k % run, live below n
+  const int last = n - (runs - 1) * span;
+  const int live = (runs - 1) * kProbeRun + (last < kProbeRun ? last : kProbeRun);
+  const int tiles = pbf::tiles_of<GL>(ns);
+  float err = 0.0f;
+  for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    pbf::Group G = pbf::group_at<GL>(ns, tile);
+    const int slot = (G.b / kProbeRun) * span + G.b % kProbeRun;
+    G.live = G.live && slot < n;
+    G.b = G.live ? slot : 0;
+    const int b = G.b;
+    const float4 xp = pst[b];
+    const int c = G.live ? cnt[b] : 0;
+    const DensitySums S = density_sums<GL, false>(F, G, nbr + pbf::list_base(b, stride), nullptr, c, n, pst, xp);
+    if (G.live && G.lane == 0) err += fmaxf(fmaf(fmaf(F.m_poly, S.sw, F.m_w0), F.inv_rho0, -1.0f), 0.0f);
+  }
+  pbf::block_partial<kBlock>(err, io.partials + blockIdx.x);
+  pbf::decide_if_last<kBlock, LOOP>(io.state, io.partials, live, io.tol, io.final_check, io.loop);
 }
 
 // ---- staged gathers: one 32-particle tile per block of kStageThreads ----
@@ -2772,8 +2817,24 @@ void launch_learned_solve(pbf_ctx* ctx) {
     return;
   }
   // a residual check (final: the step's last, which only records) and a
-  // plain position update, each skipping itself once the step is done
+  // plain position update, each skipping itself once the step is done.
+  // Sampled checks (residual_sample > 1, direct density shapes): the check
+  // estimates the residual from every S-th slot, and a plain density/lambda
+  // pass, skipped once the step is done, precedes each position update.
+  const int sample = ctx->params.residual_sample;
+  const bool sampled = sample > 1 && !T.staged[PBF_TUNE_DENSITY];
   auto check = [&](cudaStream_t cs, const LearnIO& cio) {
+    if (sampled) {
+      with_lanes(T.lanes[PBF_TUNE_DENSITY], [&](auto gl) {
+        constexpr int GL = decltype(gl)::value;
+        Launch L(ctx, "residual_check");
+        if (cio.loop.use)
+          kl_residual_probe<GL, true><<<gpc, bd, 0, cs>>>(P, F, n, sample, st, ctx->nbr, ctx->cnt, ctx->pstS, cio);
+        else
+          kl_residual_probe<GL, false><<<gpc, bd, 0, cs>>>(P, F, n, sample, st, ctx->nbr, ctx->cnt, ctx->pstS, cio);
+      });
+      return;
+    }
     if (T.staged[PBF_TUNE_DENSITY]) {
       Launch L(ctx, "residual_check");
       if (cio.loop.use)
@@ -2796,6 +2857,13 @@ void launch_learned_solve(pbf_ctx* ctx) {
     }
   };
   auto update = [&](cudaStream_t cs) {
+    if (sampled) {  // lambda of the iteration, skipped once the step is done
+      with_lanes(T.lanes[PBF_TUNE_DENSITY], [&](auto gl) {
+        Launch L(ctx, "density_lambda");
+        kf_density_lambda<kDlPlain, decltype(gl)::value, false, true><<<gpc, bd, 0, cs>>>(
+            P, F, n, st, ctx->nbr, ctx->cnt, ctx->pstS, ctx->xl, ctx->velS, ctx->lamH, ctx->nudge, io);
+      });
+    }
     if (T.staged[PBF_TUNE_DELTA_P]) {
       Launch L(ctx, "dp_update");
       ks_dp_update<SCORR, false, true><<<gpd, kStageThreads, 0, cs>>>(
@@ -3074,10 +3142,11 @@ int launches_per_step(const pbf_ctx* ctx) {
     return 1 + 3 + sort + 1 + 2 + 3 + 2 * (it - 1) + 1 + tail;
   }
   if (ctx->params.solver == 1 && !ctx->params.exact_math) {
-    // learned: warm iteration (features, network, delta-p) + (iters-1) x (check, delta-p)
-    // + final check + velocity
+    // learned: warm iteration (features, network, delta-p) + (iters-1) x (check, [sampled checks:
+    // density/lambda,] delta-p) + final check + velocity
     const int it = ctx->params.max_iterations > 0 ? ctx->params.max_iterations : 1;
-    return 1 + 3 + sort + 1 + 2 + 3 + 2 * (it - 1) + 1 + 1 + tail;
+    const bool sampled = ctx->params.residual_sample > 1 && !ctx->tune.staged[PBF_TUNE_DENSITY];
+    return 1 + 3 + sort + 1 + 2 + 3 + (sampled ? 3 : 2) * (it - 1) + 1 + 1 + tail;
   }
   const int per_iter = ctx->params.exact_math ? 3 : 2;
   return 1 + 3 + sort + 1 + 2 + per_iter * K + (K == 0 ? 1 : 0) + tail;

@@ -73,6 +73,7 @@ void pbf_params_init(pbf_params* p) {
   p->solver = 0;
   p->residual_tol = 0.01f;
   p->max_iterations = 8;
+  p->residual_sample = 1;
 }
 
 // parameters.h:123-148

@@ -70,6 +70,7 @@ class PbfParams(C.Structure):
         ("solver", C.c_int32),
         ("residual_tol", C.c_float),
         ("max_iterations", C.c_int32),
+        ("residual_sample", C.c_int32),
     ]
 
     def as_dict(self) -> dict:

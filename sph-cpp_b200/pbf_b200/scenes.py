@@ -50,6 +50,7 @@ class Scene:
     solver: int = 0                        # 0 plain K iterations, 1 learned warm start
     residual_tol: float = 0.01             # learned solver: mean clamped density error target
     max_iterations: int = 8                # learned solver: iterations per step at most
+    residual_sample: int = 1               # learned solver: residual over every S-th run of 32 slots
 
     @property
     def n(self) -> int:
@@ -87,6 +88,7 @@ class Scene:
         p.solver = self.solver
         p.residual_tol = self.residual_tol
         p.max_iterations = self.max_iterations
+        p.residual_sample = self.residual_sample
         rc = lib.pbf_params_derive(C.byref(p), self.spacing, -1.0)
         if rc:
             raise RuntimeError(f"pbf_params_derive failed ({rc})")

@@ -150,8 +150,9 @@ def test_network_kernel_gives_up_a_wait_and_the_context_stays_usable():
         g2.selftest_mlp_wait_timeout()
 
 
+@pytest.mark.parametrize("sample", [1, 8])
 @pytest.mark.parametrize("tol", [1e-4, 0.005])
-def test_captured_iteration_loop_matches_eager_launches(tol):
+def test_captured_iteration_loop_matches_eager_launches(tol, sample):
     """In a captured step the learned solver's plain iterations are a WHILE
     node of the graph that the residual check ends; eager launches (per-kernel
     timing on) run the same iterations as a loop of launches that skip
@@ -162,7 +163,7 @@ def test_captured_iteration_loop_matches_eager_launches(tol):
     the loop ends it."""
     from pbf_b200.learn import DEFAULT_MODEL, load_model
     params, norm, _ = load_model(DEFAULT_MODEL)
-    sc = warm_start_scene("dam_8k", solver=1, residual_tol=tol, max_iterations=4)
+    sc = warm_start_scene("dam_8k", solver=1, residual_tol=tol, max_iterations=4, residual_sample=sample)
     runs = {}
     for mode in ("eager", "graph1", "graph4"):
         g = Particles(sc.params(), sc.n)
@@ -222,6 +223,32 @@ def test_fixed_count_runs_the_checked_iterations_without_the_checks():
     v0, v1 = out[0.0][1], out[1e-30][1]
     assert np.abs(v0 - v1).max() <= 1e-3 * np.abs(v1).max()
     assert "residual_check" not in out[0.0][2] and out[0.0][2]["density_lambda"]["launches"] == 2
+
+
+def test_sampled_checks_keep_the_error_at_the_tolerance(trained_8k):
+    """residual_sample = 8: each check estimates the mean clamped density
+    error from every 8th run of 32 slots, and the plain density/lambda pass runs only
+    when another iteration follows.  A step that stops before the cap has an
+    estimate at or below the tolerance, and the true mean error over the window
+    stays within a few per cent of it."""
+    sc, params, norm, _ = trained_8k
+    held = sc.with_(seed=98)
+    plain3 = run_solver(held.with_(solve_steps=3), 40, warmup=20)
+    tol = float(plain3["residual"].mean())
+    p = held.with_(solver=1, max_iterations=6, residual_tol=tol, residual_sample=8).params()
+    errs = []
+    with Particles(p, held.n) as g:
+        g.mlp_set(params, norm)
+        g.upload(held.positions())
+        g.step(20)
+        for _ in range(40):
+            g.step(1)
+            st = g.stats()
+            assert st["error_flags"] == 0
+            if st["solver_iterations"] < 6:
+                assert st["solver_residual"] <= tol
+            errs.append(st["mean_density_error"])
+    assert np.mean(errs) <= tol * 1.05 + 1e-6, (np.mean(errs), tol)
 
 
 def test_timing_counts_every_learned_kernel():
