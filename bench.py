@@ -69,6 +69,8 @@ def parse_args():
                     help="only record one 1M-dam step and run K Adam updates of the warm-start network "
                          "(batch 65,536) and print ms/update: the command the training kernel's ncu "
                          "summary is captured from")
+    ap.add_argument("--residual-sample", type=int, default=1,
+                    help="residual_sample of --profile-learned (1: full residual checks)")
     ap.add_argument("--learned-iterations", type=int, default=10,
                     help="iteration cap of --profile-learned (1: no conditional loop in the step's graph, "
                          "which ncu needs to profile the graph's kernels)")
@@ -619,7 +621,8 @@ def main():
         from pbf_b200.learn import DEFAULT_MODEL, load_model, warm_start_scene
         params, norm, _ = load_model(DEFAULT_MODEL)
         sc = warm_start_scene(args.scene, seed=4242).with_(solver=1, residual_tol=0.01,
-                                                           max_iterations=args.learned_iterations)
+                                                           max_iterations=args.learned_iterations,
+                                                           residual_sample=args.residual_sample)
         r = solver_run(sc, args.profile_learned, args.warmup, params, norm, autotune=False)
         print(json.dumps({"learned_ms_per_step": r["ms_per_step"], "iterations": r["mean_iterations"],
                           "kernel_ms_per_step": r["kernel_ms_per_step"]}), flush=True)
