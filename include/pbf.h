@@ -320,7 +320,9 @@ int pbf_scene_stats(pbf_ctx* ctx, int scene, pbf_stats_t* out);
  * lists of staging indices the list fill writes beside the int32 lists.  The
  * shape changes only the order of floating-point sums inside a particle (fast
  * math), never the lists; exact_math kernels run one thread per particle and
- * ignore it.  Default: 8 lanes, 256 threads, not staged. */
+ * ignore it.  Default: 2 lanes x 128 threads for density/lambda and delta-p,
+ * 2 x 256 for XSPH and vorticity apply, 4 x 256 for vorticity (the autotuner's
+ * choice on the 1M dam), not staged. */
 enum {
   PBF_TUNE_DENSITY = 0,          /* density + lambda, and the learned solver's residual check */
   PBF_TUNE_DELTA_P = 1,          /* position delta + x* update */

@@ -2195,7 +2195,7 @@ struct pbf_ctx {
   uint64_t steps_done = 0;  // steps advanced by pbf_step (saved with the state)
   // launch shapes of the fast gather families, and the persistent grids of
   // the learned solver's skippable launches (SMs x resident blocks)
-  pbf_tuning tune{{8, 8, 8, 8, 8}, {kBlock, kBlock, kBlock, kBlock, kBlock}, {0, 0, 0, 0, 0}};
+  pbf_tuning tune{{2, 2, 2, 4, 2}, {128, 128, kBlock, kBlock, kBlock}, {0, 0, 0, 0, 0}};  // pbf.h's defaults
   int sms = 148;
   int pgrid_check = 148, pgrid_dp = 148;
   // staged gathers: tile descriptors and the 16-bit lists the list fill writes

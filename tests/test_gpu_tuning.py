@@ -24,6 +24,11 @@ REL_TOL = 1e-5
 BARS = {"mean_density_error": 0.014, "max_density_error": 0.044, "kinetic_energy": 0.02}
 
 
+# the library's default shapes (include/pbf.h)
+DEFAULT = {"density": (2, 128, 0), "delta_p": (2, 128, 0), "viscosity": (2, 256, 0), "vorticity": (4, 256, 0),
+           "apply_vorticity": (2, 256, 0)}
+
+
 def _all_families(shape):
     return {f: tuple(shape) + (0,) * (3 - len(shape)) for f in _abi.TUNE_FAMILIES}
 
@@ -100,7 +105,7 @@ def test_set_tuning_rejects_unsupported_shapes():
     for bad in ((16, 256), (8, 512), (3, 128), (8, 96)):
         with pytest.raises(RuntimeError, match="not a supported shape"):
             g.set_tuning({"viscosity": bad})
-    assert g.tuning() == _all_families((8, 256, 0))  # unchanged
+    assert g.tuning() == DEFAULT  # unchanged
     with pytest.raises(RuntimeError, match="not a supported shape"):
         g.set_tuning({"density": (8, 256, 1)})  # staged is 4 lanes x 128 threads only
 
@@ -155,7 +160,7 @@ def test_autotune_learned_solver_and_exact_math():
     ex.upload(make_scene("dam_2k").positions())
     ex.step(1)
     chosen, table = ex.autotune(1)
-    assert chosen == _all_families((8, 256, 0))
+    assert chosen == DEFAULT
     assert all(ms == 0.0 for c in table for ms in table[c].values())
 
 
