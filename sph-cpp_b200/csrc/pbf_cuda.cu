@@ -203,12 +203,18 @@ __global__ void k_predict(Dev P, int n, const float4* __restrict__ pos, const fl
   pst[a] = make_float4(s.x, s.y, s.z, 0.0f);
 }
 
+// Bins holding more particles than this walk their candidates run by run.
+constexpr uint32_t kRunBin = 512;
+
 // calculate_bins (neighbors.h:120-125) + bin histogram; the radix sort's
-// input (key, pair) goes to the particle's reference index.
-__device__ __forceinline__ void hash_out(int a, uint32_t k, const uint32_t* __restrict__ orig, uint32_t* key,
-                                         uint32_t* cell_count, uint32_t* key_ref, unsigned long long* pair_ref) {
+// input (key, pair) goes to the particle's reference index.  The word after
+// the histogram (cell_count[nbins]) is raised when a bin passes kRunBin
+// particles: only then does the list fill need the runs (k_runs).
+__device__ __forceinline__ void hash_out(const Dev& P, int a, uint32_t k, const uint32_t* __restrict__ orig,
+                                         uint32_t* key, uint32_t* cell_count, uint32_t* key_ref,
+                                         unsigned long long* pair_ref) {
   key[a] = k;
-  atomicAdd(&cell_count[k], 1u);
+  if (atomicAdd(&cell_count[k], 1u) == kRunBin) atomicOr(&cell_count[P.nbins], 1u);
   const uint32_t o = orig[a];
   key_ref[o] = k;
   pair_ref[o] = ((unsigned long long)o << 32) | (unsigned long long)(uint32_t)a;
@@ -222,7 +228,7 @@ __global__ void k_hash(Dev P, int n, const float4* __restrict__ pst, const uint3
   const float4 s = pst[a];
   uint32_t k;
   if (!pbf::bin_of(P, pbf::region_of(P, a), s.x, s.y, s.z, k)) atomicOr(err, PBF_FLAG_KEY_RANGE);
-  hash_out(a, k, orig, key, cell_count, key_ref, pair_ref);
+  hash_out(P, a, k, orig, key, cell_count, key_ref, pair_ref);
 }
 
 // Fused apply_external_forces + predict_positions + calculate_bins + histogram.
@@ -239,7 +245,7 @@ __global__ void k_ext_predict_hash(Dev P, int n, const float4* __restrict__ pos,
   pst[a] = make_float4(s.x, s.y, s.z, 0.0f);
   uint32_t k;
   if (!pbf::bin_of(P, R, s.x, s.y, s.z, k)) atomicOr(err, PBF_FLAG_KEY_RANGE);
-  hash_out(a, k, orig, key, cell_count, key_ref, pair_ref);
+  hash_out(P, a, k, orig, key, cell_count, key_ref, pair_ref);
 }
 
 // ---- exclusive scan of cell_count[0..m-1] (+ total at [m]) -> cell_start ----
@@ -444,8 +450,12 @@ __global__ void k_reorder(int n, const unsigned long long* __restrict__ pairs, c
 // run_end[i] = the first slot j > i whose x* differs from slot j - 1's, or the
 // end of i's block of kRunBlock slots, whichever comes first.  Equal x* gives
 // equal distance tests, so the list fill decides a whole run with one test.
+// crowded (may be null): the histogram's flag; zero means no bin is large
+// enough for the fill to read the runs, and the launch returns at once.
 constexpr int kRunBlock = 1024;
-__global__ void __launch_bounds__(kRunBlock) k_runs(int n, const float4* __restrict__ pst, uint32_t* run_end) {
+__global__ void __launch_bounds__(kRunBlock) k_runs(int n, const float4* __restrict__ pst, uint32_t* run_end,
+                                                    const uint32_t* __restrict__ crowded) {
+  if (crowded && *crowded == 0u) return;
   __shared__ uint32_t wfirst[kRunBlock / 32];  // first run start of every warp's 32 slots
   const int i = blockIdx.x * kRunBlock + threadIdx.x;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -479,8 +489,6 @@ __global__ void __launch_bounds__(kRunBlock) k_runs(int n, const float4* __restr
   run_end[i] = e;
 }
 
-// Bins holding more particles than this walk their candidates run by run.
-constexpr uint32_t kRunBin = 512;
 
 // One crowded bin [q0, q1) of the list fill, run by run: one distance test per
 // run of bit-identical x*; on a hit the run's slots are appended in order, the
@@ -2670,7 +2678,8 @@ void launch_sort_to_pairs(pbf_ctx* ctx) {
 void launch_fill(pbf_ctx* ctx, const float4* pst) {
   {
     Launch L(ctx, "runs");
-    k_runs<<<blocks_for(ctx->n, kRunBlock), kRunBlock, 0, ctx->stream>>>((int)ctx->n, pst, ctx->run_end);
+    k_runs<<<blocks_for(ctx->n, kRunBlock), kRunBlock, 0, ctx->stream>>>((int)ctx->n, pst, ctx->run_end,
+                                                                         ctx->cell_count + ctx->nbins);
   }
   Launch L(ctx, "fill_neighbors");
   if (any_staged(ctx))
@@ -2937,7 +2946,7 @@ void launch_step_t(pbf_ctx* ctx) {
   const Dev& P = ctx->dev;
   cudaStream_t s = ctx->stream;
   const int g = blocks_for(n);
-  cudaMemsetAsync(ctx->cell_count, 0, sizeof(uint32_t) * (size_t)ctx->nbins, s);
+  cudaMemsetAsync(ctx->cell_count, 0, sizeof(uint32_t) * ((size_t)ctx->nbins + 1), s);  // + the crowded flag
   {
     Launch L(ctx, "ext_predict_hash");
     k_ext_predict_hash<<<g, kBlock, 0, s>>>(P, n, ctx->posH, ctx->velH, ctx->pstH, ctx->origH, ctx->key,
@@ -3222,7 +3231,7 @@ static int create_ctx(const pbf_params* p, size_t capacity, const pbf_scene* sce
       (rc = dalloc(ctx, &ctx->radix_hist, radix_entries(C))) ||
       (rc = dalloc(ctx, &ctx->radix_off, radix_entries(C) + 1)) ||
       (rc = dalloc(ctx, &ctx->radix_parts, (radix_entries(C) + 1 + kScanTile - 1) / kScanTile)) ||
-      (rc = dalloc(ctx, &ctx->cell_count, (size_t)ctx->nbins)) ||
+      (rc = dalloc(ctx, &ctx->cell_count, (size_t)ctx->nbins + 1)) ||
       (rc = dalloc(ctx, &ctx->cell_start, (size_t)ctx->nbins + 1)) ||
       (rc = dalloc(ctx, &ctx->scan_part, (size_t)ctx->nscan_parts)) || (rc = dalloc(ctx, &ctx->err, 1)) ||
       (rc = dalloc(ctx, &ctx->nudge, 1)) ||
@@ -3636,7 +3645,7 @@ int pbf_find_neighbors(pbf_ctx* ctx, size_t bin_b, size_t bin_e, size_t fill_b, 
   }
   const int n = (int)ctx->n, g = blocks_for(ctx->n);
   cudaStream_t s = ctx->stream;
-  CK(cudaMemsetAsync(ctx->cell_count, 0, sizeof(uint32_t) * (size_t)ctx->nbins, s));
+  CK(cudaMemsetAsync(ctx->cell_count, 0, sizeof(uint32_t) * ((size_t)ctx->nbins + 1), s));  // + the crowded flag
   k_hash<<<g, kBlock, 0, s>>>(ctx->dev, n, ctx->pstH, ctx->origH, ctx->key, ctx->cell_count, ctx->key_ref,
                               ctx->pairs, ctx->err);
   launch_sort_to_pairs(ctx);
@@ -4755,7 +4764,7 @@ extern "C" int pbf_find_neighbors_noalloc(const pbf_params* p, const float* d_x,
     std::swap(vin, vout);
   }
   k_noalloc_gather<<<g, kBlock, 0, s>>>(nn, vin, d_x, sorted_x, sorted_id);
-  k_runs<<<blocks_for(n, kRunBlock), kRunBlock, 0, s>>>(nn, sorted_x, run_end);
+  k_runs<<<blocks_for(n, kRunBlock), kRunBlock, 0, s>>>(nn, sorted_x, run_end, nullptr);
   k_noalloc_fill<<<g, kBlock, 0, s>>>(d, nn, sorted_x, sorted_id, cell_start, run_end, d_nbr, d_cnt, err);
   if (d_flags) e = cudaMemcpyAsync(d_flags, err, 4, cudaMemcpyDeviceToDevice, s);
   if (e == cudaSuccess) e = cudaGetLastError();
