@@ -193,7 +193,10 @@ def kernel_bytes(name: str, n: int, nbar: float, K: int, nbins: int) -> float:
         "residual_check": 16 + L + 16 + 4 + 4,                  # as density_lambda
         "reorder": 8 + 4 + 3 * 16 + 3 * 16 + 4 + 4,             # pair, key, (x, x*, v) in and out, orig, key
         "runs": 16 + 4,                                         # x* in (the previous slot's is a cache hit); run end out
-        "fill_neighbors": 16 + 4 * nbar + 4 + 8.0 * nbins / n,  # own x*, list + count out, bin starts
+        "fill_neighbors": 16 + 4 * nbar + 4 + 8.0 * nbins / n + 32,  # own x*, list + count out, bin starts,
+                                                                     # the visits' starts (seg) out
+        "fill_redo": 4.0 * 5 / n,                               # the order words; its queue (capped slot-order
+                                                                # lists, walked again) is empty unless lists reach the cap
         "density_lambda": 16 + L + 16 + 4 + 4,                  # x* in; list; (x*, lambda), rho, lambda out
         "lambda_fixup": 16 + L + 16 + 4,                        # exact math after a nudge: x* in, list; (x*, lambda), lambda out
         "dp_update": 16 + L + 16 + (32.0 / K),                  # (x*, lambda) in; list; x* out; last: x in, v out

@@ -125,6 +125,8 @@ typedef struct pbf_stats_t {
   double solver_residual;     /* learned solver: mean clamped density error at its last check */
   uint32_t tiles;             /* 32-particle tiles of the last list fill that wrote staging (0: none) */
   uint32_t tiles_staged;      /* of those, the tiles the staged gathers read from shared memory */
+  uint32_t lists_slot_order;  /* fast math: 1 if the last list fill walked the bins in slot order (few lists
+                                 at the cap), 0 if in the reference's order */
 } pbf_stats_t;
 
 typedef struct pbf_ctx pbf_ctx;

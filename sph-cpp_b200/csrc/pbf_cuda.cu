@@ -209,12 +209,19 @@ constexpr uint32_t kRunBin = 512;
 // calculate_bins (neighbors.h:120-125) + bin histogram; the radix sort's
 // input (key, pair) goes to the particle's reference index.  The word after
 // the histogram (cell_count[nbins]) is raised when a bin passes kRunBin
-// particles: only then does the list fill need the runs (k_runs).
+// particles: only then does the list fill need the runs (k_runs).  The lanes
+// of a warp with the same key add to its count once (a settled dam piles
+// hundreds of thousands of particles into one bin, whose count would
+// otherwise take one atomic per particle, one after another).
 __device__ __forceinline__ void hash_out(const Dev& P, int a, uint32_t k, const uint32_t* __restrict__ orig,
                                          uint32_t* key, uint32_t* cell_count, uint32_t* key_ref,
                                          unsigned long long* pair_ref) {
   key[a] = k;
-  if (atomicAdd(&cell_count[k], 1u) == kRunBin) atomicOr(&cell_count[P.nbins], 1u);
+  const unsigned same = __match_any_sync(__activemask(), k);
+  if ((threadIdx.x & 31) == (unsigned)(__ffs(same) - 1)) {
+    const uint32_t add = (uint32_t)__popc(same), old = atomicAdd(&cell_count[k], add);
+    if (old <= kRunBin && old + add > kRunBin) atomicOr(&cell_count[P.nbins], 1u);
+  }
   const uint32_t o = orig[a];
   key_ref[o] = k;
   pair_ref[o] = ((unsigned long long)o << 32) | (unsigned long long)(uint32_t)a;
@@ -545,13 +552,144 @@ struct TileIO {
   uint16_t* nbr16;  // [slot][stride] staging index of every list entry
 };
 
-// The list of slot b (a thread's share of k_fill2; the persistent step calls
-// it too, STAGE = false).
+// The tile's staging box (STAGE): the runs of the own bins grown by one bin.
+struct FillStage {
+  bool staged;
+  int xmn, xmx, ymn, zmn, ny, nz;
+  uint16_t* row16;
+};
+
+// One visit of the list fill: bin (cx, cy, cz) of the particle's scene, its
+// candidates in ascending slot order, strict d^2 < s^2, self skipped, while
+// the list has room.  A bin at the integer offset of the particle's own bin
+// (at_offset) whose every point is provably farther than s (e2, the squared
+// distance to its faces less the margin, above s^2) is skipped; a crowded
+// bin goes run by run.  Returns the list's new length.
 template <bool STAGE>
+__device__ __forceinline__ int fill_visit(int cx, int cy, int cz, bool at_offset, float e2, float px, float py,
+                                          float pz, bool finite, const pbf::Region& R, float s2, int cap,
+                                          uint32_t self, const uint32_t* __restrict__ cell_start,
+                                          const float4* __restrict__ pst, const uint32_t* __restrict__ run_end,
+                                          int32_t* row, uint32_t* err, const FillStage& S, const int* soff,
+                                          bool& stray, int count) {
+  if (!finite || cx < 0 || cy < 0 || cz < 0 || cx >= R.dimx || cy >= R.dimy || cz >= R.dimz) {
+    atomicOr(err, PBF_FLAG_KEY_RANGE);
+    return count;
+  }
+  if (at_offset && e2 > s2) return count;
+  const uint32_t nb =
+      R.key0 + (uint32_t)(R.dimx * R.dimy) * (uint32_t)cz + ((uint32_t)cy * (uint32_t)R.dimx + (uint32_t)cx);
+  const bool staged = STAGE && S.staged;
+  int off = 0;
+  if (staged) {
+    const int ry = cy - (S.ymn - 1), rz = cz - (S.zmn - 1);
+    if (cx < S.xmn - 1 || cx > S.xmx + 1 || ry < 0 || ry >= S.ny || rz < 0 || rz >= S.nz) stray = true;
+    else off = soff[(threadIdx.x & ~31) + rz * S.ny + ry];
+  }
+  const uint32_t q0 = cell_start[nb], q1 = cell_start[nb + 1];
+  if (q1 - q0 > kRunBin) {
+    count = fill_runs(px, py, pz, s2, cap, self, q0, q1, pst, run_end, row, staged ? S.row16 : nullptr, off, count);
+  } else if (q0 <= self && self < q1) {  // the particle's own bin: skip itself
+    for (uint32_t q = q0; q < q1; ++q) {
+      const float4 xq = pst[q];
+      const float d2 = pbf::mag2<true>(pbf::xsub(px, xq.x), pbf::xsub(py, xq.y), pbf::xsub(pz, xq.z));
+      if (d2 < s2 && q != self && count < cap) {
+        if (staged) S.row16[count] = (uint16_t)((int)q + off);
+        row[pbf::list_off(count++)] = (int32_t)q;
+      }
+    }
+  } else {  // another bin (all but one of the 27, at the same offset for every lane)
+    for (uint32_t q = q0; q < q1; ++q) {
+      const float4 xq = pst[q];
+      const float d2 = pbf::mag2<true>(pbf::xsub(px, xq.x), pbf::xsub(py, xq.y), pbf::xsub(pz, xq.z));
+      if (d2 < s2 && count < cap) {
+        if (staged) S.row16[count] = (uint16_t)((int)q + off);
+        row[pbf::list_off(count++)] = (int32_t)q;
+      }
+    }
+  }
+  return count;
+}
+
+// calculate_neighbor_indices (neighbors.h:172-185): the bin of coord + i*s
+// along one axis for i = -1, 0, 1, in the reference's float operations.  The
+// 27 bins combine these per-axis values, so 9 float hashes cover all of them.
+__device__ __forceinline__ void axis_bins(float c, float s, int (&out)[3]) {
+#pragma unroll
+  for (int i = 0; i < 3; ++i) out[i] = pbf::dev_axis_bin(pbf::xadd(c, pbf::xmul((float)(i - 1), s)), s);
+}
+
+// The 27 visits of one particle, in the reference's order (x offset outer,
+// z inner) or, slot, z offset outer and x inner: the bins then come in
+// ascending keys, so a warp's lanes read neighbouring slots together in the
+// gathers.  slot records where each visit's entries start (sc[visit
+// k*9 + j*3 + i]).  Stops at the cap and returns the list's length.  The
+// order is a run-time choice in one loop: two compiled walks made the fill
+// of a settled dam (crowded bins) 10-25% slower.
+template <bool STAGE>
+__device__ __forceinline__ int fill_walk(float px, float py, float pz, const int (&bx)[3], const int (&by)[3],
+                                         const int (&bz)[3], float s, float skip_eps, const pbf::Region& R,
+                                         float s2, int cap, uint32_t self, const uint32_t* __restrict__ cell_start,
+                                         const float4* __restrict__ pst, const uint32_t* __restrict__ run_end,
+                                         int32_t* row, uint32_t* err, const FillStage& S, const int* soff,
+                                         bool& stray, bool slot, uint8_t* sc) {
+  const bool finite = isfinite(px) && isfinite(py) && isfinite(pz);
+  // per-axis distance from the particle to its own bin's faces, less the margin
+  const float lo[3] = {fmaxf(px - ((float)bx[1] * s - s) - skip_eps, 0.f),
+                       fmaxf(py - ((float)by[1] * s - s) - skip_eps, 0.f),
+                       fmaxf(pz - ((float)bz[1] * s - s) - skip_eps, 0.f)};
+  const float hi[3] = {fmaxf(((float)(bx[1] + 1) * s - s) - px - skip_eps, 0.f),
+                       fmaxf(((float)(by[1] + 1) * s - s) - py - skip_eps, 0.f),
+                       fmaxf(((float)(bz[1] + 1) * s - s) - pz - skip_eps, 0.f)};
+  int count = 0;
+  for (int u = 0; u < 3; u++) {
+    for (int j = 0; j < 3; j++) {
+      for (int w = 0; w < 3; w++) {
+        const int i = slot ? w : u, k = slot ? u : w;
+        if (slot) sc[k * 9 + j * 3 + i] = (uint8_t)count;
+        const float ex = i == 0 ? lo[0] : (i == 2 ? hi[0] : 0.f);
+        const float ey = j == 0 ? lo[1] : (j == 2 ? hi[1] : 0.f);
+        const float ez = k == 0 ? lo[2] : (k == 2 ? hi[2] : 0.f);
+        const int cx = bx[i], cy = by[j], cz = bz[k];
+        count = fill_visit<STAGE>(cx, cy, cz, cx == bx[1] + i - 1 && cy == by[1] + j - 1 && cz == bz[1] + k - 1,
+                                  ex * ex + ey * ey + ez * ez, px, py, pz, finite, R, s2, cap, self, cell_start, pst,
+                                  run_end, row, err, S, soff, stray, count);
+        if (count >= cap) return count;
+      }
+    }
+  }
+  return count;
+}
+
+// Beside each list of the fast path (seg, kSegWords words per slot): where
+// each of the 27 visits' entries start, in visit order (z offset outer), then
+// kSegReferenceOrder when the list is in the reference's order (the cap is at
+// most 64, so a byte holds an offset).
+constexpr int kSegWords = 8;
+constexpr uint8_t kSegReferenceOrder = 0xFF;
+
+// The fast path's choice of list order, in device words (FillWord): the
+// lists that reached the cap in the fill under way, the slot-order lists
+// queued for the reference's walk, the order of the next fill (1 = slot
+// order), the redo kernel's block ticket, and the order the last fill used.  The cap keeps the first entries in the
+// reference's order, so a slot-order list that reaches it is walked again in
+// that order (k_fill_redo).  Once more than 1 / kSlotCappedShare of the lists
+// reach the cap (a dam that has settled), the fill walks in the reference's
+// order, where the cap costs nothing, until the share drops again.
+enum FillWord { kFillCapped = 0, kFillQueued = 1, kFillSlotOrder = 2, kFillTicket = 3, kFillLastOrder = 4, kFillWords = 5 };
+constexpr uint32_t kSlotCappedShare = 64;
+
+// The list of slot b (a thread's share of k_fill2).  SLOT (fast math): in
+// the order fw chose, the visits' starts or the reference-order mark in seg,
+// a slot-order list that reached the cap queued for k_fill_redo; else in the
+// reference's order.
+template <bool STAGE, bool SLOT>
 __device__ __forceinline__ void fill_thread(int b, const Dev& P, int n, size_t stride, const float4* __restrict__ pst,
                                             const uint32_t* __restrict__ cell_start,
                                             const uint32_t* __restrict__ run_end, int32_t* nbr, int32_t* cnt,
-                                            uint32_t* err, const TileIO& T) {
+                                            uint32_t* err, const TileIO& T, uint32_t* seg, uint32_t* fw,
+                                            int32_t* queue) {
+  __shared__ __align__(16) uint8_t seg_smem[SLOT ? kFillBlock : 1][4 * kSegWords];
   if (!STAGE && b >= n) return;
   if (STAGE && (b & ~(kTile - 1)) >= n) return;  // a whole warp past the end: no tile (warp-uniform)
   const bool live = b < n;
@@ -561,17 +699,10 @@ __device__ __forceinline__ void fill_thread(int b, const Dev& P, int n, size_t s
   const float s = P.s;
   const pbf::Region R = pbf::region_of(P, bb);
   int32_t* row = nbr + pbf::list_base(b, stride);
-  // calculate_neighbor_indices (neighbors.h:172-185): the bin of coord + i*s
-  // per axis for i = -1, 0, 1, in the reference's float operations.  The 27
-  // bins combine these per-axis values, so 9 float hashes cover all of them.
   int bx[3], by[3], bz[3];
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    const float o = pbf::xmul((float)(i - 1), s);
-    bx[i] = pbf::dev_axis_bin(pbf::xadd(xp.x, o), s);
-    by[i] = pbf::dev_axis_bin(pbf::xadd(xp.y, o), s);
-    bz[i] = pbf::dev_axis_bin(pbf::xadd(xp.z, o), s);
-  }
+  axis_bins(xp.x, s, bx);
+  axis_bins(xp.y, s, by);
+  axis_bins(xp.z, s, bz);
   const bool finite = isfinite(xp.x) && isfinite(xp.y) && isfinite(xp.z);
   // The tile's staging runs (STAGE): warp-wide box of the own bins, one run
   // per (y, z) row of the grown box, the runs' staging bases by a prefix sum.
@@ -621,77 +752,87 @@ __device__ __forceinline__ void fill_thread(int b, const Dev& P, int n, size_t s
     __syncwarp();
     if (!live) return;
   }
-  // Per-axis distance from the particle to its own bin's faces, less the margin.
-  const float lo[3] = {fmaxf(xp.x - ((float)bx[1] * s - s) - P.skip_eps, 0.f),
-                       fmaxf(xp.y - ((float)by[1] * s - s) - P.skip_eps, 0.f),
-                       fmaxf(xp.z - ((float)bz[1] * s - s) - P.skip_eps, 0.f)};
-  const float hi[3] = {fmaxf(((float)(bx[1] + 1) * s - s) - xp.x - P.skip_eps, 0.f),
-                       fmaxf(((float)(by[1] + 1) * s - s) - xp.y - P.skip_eps, 0.f),
-                       fmaxf(((float)(bz[1] + 1) * s - s) - xp.z - P.skip_eps, 0.f)};
-  int count = 0;
-
-  for (int i = 0; i < 3; i++) {
-    const float ex = i == 0 ? lo[0] : (i == 2 ? hi[0] : 0.f);
-    for (int j = 0; j < 3; j++) {
-      const float ey = j == 0 ? lo[1] : (j == 2 ? hi[1] : 0.f);
-      for (int k = 0; k < 3; k++) {
-        const float ez = k == 0 ? lo[2] : (k == 2 ? hi[2] : 0.f);
-        const int cx = bx[i], cy = by[j], cz = bz[k];
-        if (!finite || cx < 0 || cy < 0 || cz < 0 || cx >= R.dimx || cy >= R.dimy || cz >= R.dimz) {
-          atomicOr(err, PBF_FLAG_KEY_RANGE);
-          continue;
-        }
-        // a bin at the integer offset whose every point is farther than s: skip
-        if (cx == bx[1] + i - 1 && cy == by[1] + j - 1 && cz == bz[1] + k - 1 &&
-            ex * ex + ey * ey + ez * ez > P.s2)
-          continue;
-        const uint32_t nb =
-            R.key0 + (uint32_t)(R.dimx * R.dimy) * (uint32_t)cz + ((uint32_t)cy * (uint32_t)R.dimx + (uint32_t)cx);
-        int off = 0;
-        if (STAGE && staged) {
-          const int ry = cy - (ymn - 1), rz = cz - (zmn - 1);
-          if (cx < xmn - 1 || cx > xmx + 1 || ry < 0 || ry >= ny || rz < 0 || rz >= nz) stray = true;
-          else off = soff[(threadIdx.x & ~31) + rz * ny + ry];
-        }
-        const uint32_t q0 = cell_start[nb], q1 = cell_start[nb + 1];
-        if (q1 - q0 > kRunBin) {
-          count = fill_runs(xp.x, xp.y, xp.z, P.s2, cap, (uint32_t)b, q0, q1, pst, run_end, row,
-                            STAGE && staged ? row16 : nullptr, off, count);
-        } else if (q0 <= (uint32_t)b && (uint32_t)b < q1) {  // the particle's own bin: skip itself
-          for (uint32_t q = q0; q < q1; ++q) {
-            const float4 xq = pst[q];
-            const float d2 = pbf::mag2<true>(pbf::xsub(xp.x, xq.x), pbf::xsub(xp.y, xq.y), pbf::xsub(xp.z, xq.z));
-            if (d2 < P.s2 && q != (uint32_t)b && count < cap) {
-              if (STAGE && staged) row16[count] = (uint16_t)((int)q + off);
-              row[pbf::list_off(count++)] = (int32_t)q;
-            }
-          }
-        } else {  // another bin (all but one of the 27, at the same offset for every lane)
-          for (uint32_t q = q0; q < q1; ++q) {
-            const float4 xq = pst[q];
-            const float d2 = pbf::mag2<true>(pbf::xsub(xp.x, xq.x), pbf::xsub(xp.y, xq.y), pbf::xsub(xp.z, xq.z));
-            if (d2 < P.s2 && count < cap) {
-              if (STAGE && staged) row16[count] = (uint16_t)((int)q + off);
-              row[pbf::list_off(count++)] = (int32_t)q;
-            }
-          }
-        }
-        if (count >= cap) goto done;
-      }
+  const FillStage S{staged, xmn, xmx, ymn, zmn, ny, nz, row16};
+  const bool slot = SLOT && fw[kFillSlotOrder] != 0;
+  uint8_t* sc = SLOT ? seg_smem[threadIdx.x] : nullptr;
+  const int count = fill_walk<STAGE>(xp.x, xp.y, xp.z, bx, by, bz, s, P.skip_eps, R, P.s2, cap, (uint32_t)b,
+                                     cell_start, pst, run_end, row, err, S, soff, stray, slot, sc);
+  cnt[b] = count;
+  if (SLOT) {
+    const bool capped = count >= cap;
+    // warp-aggregated counts: the lists at the cap, the slot-order ones among them queued
+    const unsigned act = __activemask(), lane_lt = (1u << (threadIdx.x & 31)) - 1u;
+    const int leader = __ffs(act) - 1;
+    const unsigned cm = __ballot_sync(act, capped), qm = __ballot_sync(act, slot && capped);
+    uint32_t qbase = 0;
+    if ((int)(threadIdx.x & 31) == leader) {
+      if (cm) atomicAdd(&fw[kFillCapped], (uint32_t)__popc(cm));
+      if (qm) qbase = atomicAdd(&fw[kFillQueued], (uint32_t)__popc(qm));
+    }
+    qbase = __shfl_sync(act, qbase, leader);
+    if (slot && capped) {
+      queue[qbase + __popc(qm & lane_lt)] = b;
+      if (STAGE) stray = true;  // the tile walks the int32 lists
+    }
+    if (slot) {  // (a fill in the reference's order leaves seg alone: the export reads its order word)
+      sc[27] = capped ? kSegReferenceOrder : 0;
+      const uint32_t* w = reinterpret_cast<const uint32_t*>(seg_smem[threadIdx.x]);
+#pragma unroll
+      for (int v = 0; v < kSegWords; ++v) seg[(size_t)b * kSegWords + v] = w[v];
     }
   }
-done:
-  cnt[b] = count;
   // a bin outside the tile's box (float re-hash at a bin face): the tile walks the int32 lists
   if (STAGE && stray) T.nruns[tile] = 0;
 }
 
-template <bool STAGE>
+template <bool STAGE, bool SLOT>
 __global__ void __launch_bounds__(kFillBlock) k_fill2(Dev P, int n, size_t stride, const float4* __restrict__ pst,
                                                       const uint32_t* __restrict__ cell_start,
                                                       const uint32_t* __restrict__ run_end, int32_t* nbr,
-                                                      int32_t* cnt, uint32_t* err, TileIO T) {
-  fill_thread<STAGE>(blockIdx.x * kFillBlock + threadIdx.x, P, n, stride, pst, cell_start, run_end, nbr, cnt, err, T);
+                                                      int32_t* cnt, uint32_t* err, TileIO T, uint32_t* seg,
+                                                      uint32_t* fw, int32_t* queue) {
+  fill_thread<STAGE, SLOT>(blockIdx.x * kFillBlock + threadIdx.x, P, n, stride, pst, cell_start, run_end, nbr, cnt,
+                           err, T, seg, fw, queue);
+}
+
+// The queued slot-order lists that reached the cap, walked again in the
+// reference's order (int32 lists; their seg already says so).  Then the last
+// block to finish picks the next fill's order from the share of lists at the
+// cap and clears the counts.  No thread returns early: every block reaches
+// the ticket.
+__global__ void __launch_bounds__(kFillBlock) k_fill_redo(Dev P, int n, size_t stride, const float4* __restrict__ pst,
+                                                          const uint32_t* __restrict__ cell_start,
+                                                          const uint32_t* __restrict__ run_end, int32_t* nbr,
+                                                          int32_t* cnt, uint32_t* err, const int32_t* __restrict__ queue,
+                                                          uint32_t* fw) {
+  const uint32_t queued = fw[kFillQueued];
+  for (uint32_t t = blockIdx.x * kFillBlock + threadIdx.x; t < queued; t += gridDim.x * kFillBlock) {
+    const int b = queue[t];
+    const float4 xp = pst[b];
+    const pbf::Region R = pbf::region_of(P, b);
+    int bx[3], by[3], bz[3];
+    axis_bins(xp.x, P.s, bx);
+    axis_bins(xp.y, P.s, by);
+    axis_bins(xp.z, P.s, bz);
+    const FillStage none{};
+    bool stray = false;
+    cnt[b] = fill_walk<false>(xp.x, xp.y, xp.z, bx, by, bz, P.s, P.skip_eps, R, P.s2, P.cap, (uint32_t)b,
+                              cell_start, pst, run_end, nbr + pbf::list_base(b, stride), err, none, nullptr,
+                              stray, false, nullptr);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&fw[kFillTicket], 1u) == gridDim.x - 1) {
+      __threadfence();
+      const uint32_t capped = atomicAdd(&fw[kFillCapped], 0u);
+      fw[kFillLastOrder] = fw[kFillSlotOrder];
+      fw[kFillSlotOrder] = (uint64_t)capped * kSlotCappedShare <= (uint64_t)n ? 1u : 0u;
+      fw[kFillCapped] = 0;
+      fw[kFillQueued] = 0;
+      fw[kFillTicket] = 0;
+    }
+  }
 }
 
 // ---- density (particles.h:292-313) ----
@@ -2131,17 +2272,35 @@ __global__ void __launch_bounds__(kBlock) k_stats(Dev P, int b0, int b1, size_t 
 }
 
 // Neighbour lists in reference index space, [N][cap], -1 past count.
+// seg (fast math, whose last fill walked in slot order when *last_order is
+// 1): each slot-order list is written back in the reference's order, visit
+// by visit (x offset outer, z inner; within a visit the entries keep their
+// ascending slots), from where the fill recorded each visit starts.
 __global__ void k_export_neighbors(int n, size_t stride, int cap, const int32_t* __restrict__ nbr,
                                    const int32_t* __restrict__ cnt, const uint32_t* __restrict__ orig,
-                                   int32_t* idx_out, int32_t* cnt_out) {
+                                   int32_t* idx_out, int32_t* cnt_out, const uint32_t* __restrict__ seg,
+                                   const uint32_t* __restrict__ last_order) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= n) return;
   const size_t o = orig[b];
   const int c = cnt[b];
   if (cnt_out) cnt_out[o] = c;
-  if (idx_out)
+  if (!idx_out) return;
+  const uint8_t* sc = seg && *last_order ? reinterpret_cast<const uint8_t*>(seg + (size_t)b * kSegWords) : nullptr;
+  if (sc == nullptr || sc[27] == kSegReferenceOrder) {
     for (int k = 0; k < cap; ++k)
       idx_out[o * cap + k] = k < c ? (int32_t)orig[nbr[pbf::list_at(b, stride, k)]] : -1;
+    return;
+  }
+  int e = 0;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j)
+      for (int k = 0; k < 3; ++k) {
+        const int v = k * 9 + j * 3 + i;  // visit v's entries: [sc[v], sc[v+1]) of the slot-order list
+        for (int t = sc[v], t1 = v < 26 ? sc[v + 1] : c; t < t1; ++t)
+          idx_out[o * cap + e++] = (int32_t)orig[nbr[pbf::list_at(b, stride, t)]];
+      }
+  for (; e < cap; ++e) idx_out[o * cap + e] = -1;
 }
 
 }  // namespace
@@ -2164,6 +2323,10 @@ struct pbf_ctx {
   cudaStream_t side = nullptr;  // captures the body of the learned solver's conditional loop
   bool capture_failed = false;  // a step's conditional loop could not be captured whole
   bool lists_valid = false;
+  bool lists_slot_order = false;  // fast math: seg says, per list, which order it is in
+  uint32_t* fill_words = nullptr;  // [kFillWords] the fast fill's order choice (FillWord)
+  int32_t* redo_queue = nullptr;   // [C] slot-order lists that reached the cap
+  uint32_t* seg = nullptr;        // [C][kSegWords] where the fast fill's visits start
 
   float4 *posH = nullptr, *pstH = nullptr, *velH = nullptr, *scrH = nullptr;
   float4 *posS = nullptr, *pstS = nullptr, *velS = nullptr, *scrS = nullptr, *xl = nullptr, *velT = nullptr;
@@ -2681,15 +2844,34 @@ void launch_fill(pbf_ctx* ctx, const float4* pst) {
     k_runs<<<blocks_for(ctx->n, kRunBlock), kRunBlock, 0, ctx->stream>>>((int)ctx->n, pst, ctx->run_end,
                                                                          ctx->cell_count + ctx->nbins);
   }
-  Launch L(ctx, "fill_neighbors");
-  if (any_staged(ctx))
-    k_fill2<true><<<blocks_for(ctx->n, kFillBlock), kFillBlock, 0, ctx->stream>>>(
-        ctx->dev, (int)ctx->n, ctx->lstride, pst, ctx->cell_start, ctx->run_end, ctx->nbr, ctx->cnt, ctx->err,
-        tile_io(ctx));
-  else
-    k_fill2<false><<<blocks_for(ctx->n, kFillBlock), kFillBlock, 0, ctx->stream>>>(
-        ctx->dev, (int)ctx->n, ctx->lstride, pst, ctx->cell_start, ctx->run_end, ctx->nbr, ctx->cnt, ctx->err,
-        tile_io(ctx));
+  // fast math: lists in slot order while few reach the cap (the gathers' sums
+  // in any order are within the fast path's tolerance), the capped ones
+  // walked again in the reference's order; exact math: the reference's order
+  const bool slot = ctx->params.exact_math == 0;
+  ctx->lists_slot_order = slot;
+  {
+    Launch L(ctx, "fill_neighbors");
+    auto fill = [&](auto stage, auto order) {
+      k_fill2<decltype(stage)::value, decltype(order)::value>
+          <<<blocks_for(ctx->n, kFillBlock), kFillBlock, 0, ctx->stream>>>(
+              ctx->dev, (int)ctx->n, ctx->lstride, pst, ctx->cell_start, ctx->run_end, ctx->nbr, ctx->cnt, ctx->err,
+              tile_io(ctx), ctx->seg, ctx->fill_words, ctx->redo_queue);
+    };
+    using T_ = std::true_type;
+    using F_ = std::false_type;
+    if (any_staged(ctx)) {
+      if (slot) fill(T_{}, T_{}); else fill(T_{}, F_{});
+    } else {
+      if (slot) fill(F_{}, T_{}); else fill(F_{}, F_{});
+    }
+  }
+  if (slot) {
+    Launch L(ctx, "fill_redo");
+    const int grid = std::max(1, std::min(blocks_for(ctx->n, kFillBlock), 4 * ctx->sms));
+    k_fill_redo<<<grid, kFillBlock, 0, ctx->stream>>>(ctx->dev, (int)ctx->n, ctx->lstride, pst, ctx->cell_start,
+                                                      ctx->run_end, ctx->nbr, ctx->cnt, ctx->err, ctx->redo_queue,
+                                                      ctx->fill_words);
+  }
 }
 
 // The list fill, then every gather pass of the step in one launch.
@@ -3137,28 +3319,29 @@ int launches_per_step(const pbf_ctx* ctx) {
   // kernels only (the memsets are not), as launched eagerly (a captured
   // learned step runs its plain iterations in a conditional graph node and
   // launches fewer once converged): ext/predict/hash + 3 scan + radix
-  // passes x (histogram, 3 scan, scatter) + reorder + runs + fill + K x
-  // (density/lambda, [exact: lambda fix-up], delta-p) + (K==0: velocity)
-  // + 2 if gamma + 4 (visc, vort, apply, visc)
+  // passes x (histogram, 3 scan, scatter) + reorder + runs + fill + [fast
+  // math: fill redo] + K x (density/lambda, [exact: lambda fix-up], delta-p)
+  // + (K==0: velocity) + 2 if gamma + 4 (visc, vort, apply, visc)
   const int sort = 5 * ctx->radix_passes;
-  if (persist_on(ctx)) return 1 + 3 + sort + 1 + 2 + 1;  // ... reorder, runs, fill, the persistent step
+  const int fill = ctx->params.exact_math ? 2 : 3;  // runs, fill, [redo]
+  if (persist_on(ctx)) return 1 + 3 + sort + 1 + fill + 1;  // ... reorder, runs, fill, redo, the persistent step
   const int K = ctx->params.solve_steps;
   const int tail = (ctx->params.gamma != 0.0f ? 2 : 0) + 4;
   if (ctx->params.solver == 1 && !ctx->params.exact_math && !(ctx->params.residual_tol > 0.0f)) {
     // learned, a fixed count: warm iteration (features, network, delta-p) + (iters-1) x (density, delta-p)
     // + velocity
     const int it = ctx->params.max_iterations > 0 ? ctx->params.max_iterations : 1;
-    return 1 + 3 + sort + 1 + 2 + 3 + 2 * (it - 1) + 1 + tail;
+    return 1 + 3 + sort + 1 + fill + 3 + 2 * (it - 1) + 1 + tail;
   }
   if (ctx->params.solver == 1 && !ctx->params.exact_math) {
     // learned: warm iteration (features, network, delta-p) + (iters-1) x (check, [sampled checks:
     // density/lambda,] delta-p) + final check + velocity
     const int it = ctx->params.max_iterations > 0 ? ctx->params.max_iterations : 1;
     const bool sampled = ctx->params.residual_sample > 1 && !ctx->tune.staged[PBF_TUNE_DENSITY];
-    return 1 + 3 + sort + 1 + 2 + 3 + (sampled ? 3 : 2) * (it - 1) + 1 + 1 + tail;
+    return 1 + 3 + sort + 1 + fill + 3 + (sampled ? 3 : 2) * (it - 1) + 1 + 1 + tail;
   }
   const int per_iter = ctx->params.exact_math ? 3 : 2;
-  return 1 + 3 + sort + 1 + 2 + per_iter * K + (K == 0 ? 1 : 0) + tail;
+  return 1 + 3 + sort + 1 + fill + per_iter * K + (K == 0 ? 1 : 0) + tail;
 }
 
 }  // namespace
@@ -3236,6 +3419,8 @@ static int create_ctx(const pbf_params* p, size_t capacity, const pbf_scene* sce
       (rc = dalloc(ctx, &ctx->scan_part, (size_t)ctx->nscan_parts)) || (rc = dalloc(ctx, &ctx->err, 1)) ||
       (rc = dalloc(ctx, &ctx->nudge, 1)) ||
       (rc = dalloc(ctx, &ctx->pairs, C)) || (rc = dalloc(ctx, &ctx->pairs_sorted, C)) || (rc = dalloc(ctx, &ctx->nbr, pbf::list_entries(C, cap))) ||
+      (rc = dalloc(ctx, &ctx->seg, C * kSegWords)) || (rc = dalloc(ctx, &ctx->fill_words, kFillWords)) ||
+      (rc = dalloc(ctx, &ctx->redo_queue, C)) ||
             (rc = dalloc(ctx, &ctx->cnt, C)) || (rc = dalloc(ctx, &ctx->stage, 6 * C)) ||
       (rc = dalloc(ctx, &ctx->stage_i, std::max(C * cap + C, pbf::list_entries(C, cap)))) ||
       (rc = dalloc(ctx, &ctx->acc, 8)) ||
@@ -3263,7 +3448,10 @@ static int create_ctx(const pbf_params* p, size_t capacity, const pbf_scene* sce
     fail(ctx, PBF_ERR_CUDA, "initialisation failed");
     return bail(PBF_ERR_CUDA);
   }
+  // the first fill walks in slot order (the byte sets word kFillSlotOrder to 1)
   if (cudaMemsetAsync(ctx->err, 0, sizeof(uint32_t), ctx->stream) != cudaSuccess ||
+      cudaMemsetAsync(ctx->fill_words, 0, kFillWords * sizeof(uint32_t), ctx->stream) != cudaSuccess ||
+      cudaMemsetAsync(ctx->fill_words + kFillSlotOrder, 1, 1, ctx->stream) != cudaSuccess ||
       cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
     fail(ctx, PBF_ERR_CUDA, "initialisation failed");
     return bail(PBF_ERR_CUDA);
@@ -3990,7 +4178,9 @@ int pbf_get_neighbors(pbf_ctx* ctx, int32_t* idx, int32_t* count) {
   int32_t* di = ctx->stage_i;
   int32_t* dc = ctx->stage_i + n * cap;
   k_export_neighbors<<<blocks_for(n), kBlock, 0, ctx->stream>>>((int)n, ctx->lstride, (int)cap, ctx->nbr, ctx->cnt,
-                                                                 ctx->origH, di, dc);
+                                                                 ctx->origH, di, dc,
+                                                                 ctx->lists_slot_order ? ctx->seg : nullptr,
+                                                                 ctx->fill_words + kFillLastOrder);
   if (int rc = check_launch(ctx, "export_neighbors")) return rc;
   if (idx) CK(cudaMemcpyAsync(idx, di, n * cap * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
   if (count) CK(cudaMemcpyAsync(count, dc, n * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
@@ -4060,6 +4250,8 @@ static int stats_range(pbf_ctx* ctx, size_t b0, size_t b1, bool clear_flags, pbf
     out->solver_iterations = (uint32_t)ctx->params.solve_steps;
     out->solver_residual = -1.0;
   }
+  if (!ctx->params.exact_math) CK(cudaMemcpy(&out->lists_slot_order, ctx->fill_words + kFillLastOrder,
+                                             sizeof(uint32_t), cudaMemcpyDeviceToHost));
   if (any_staged(ctx) && ctx->n) {  // the tiles of the last list fill
     const size_t tiles = (ctx->n + kTile - 1) / kTile;
     std::vector<int32_t> nr(tiles);

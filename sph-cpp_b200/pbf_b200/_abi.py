@@ -95,6 +95,7 @@ class PbfStats(C.Structure):
         ("solver_residual", C.c_double),
         ("tiles", C.c_uint32),
         ("tiles_staged", C.c_uint32),
+        ("lists_slot_order", C.c_uint32),
     ]
 
     def as_dict(self) -> dict:
@@ -111,6 +112,7 @@ class PbfStats(C.Structure):
             "solver_residual": self.solver_residual,
             "tiles": int(self.tiles),
             "tiles_staged": int(self.tiles_staged),
+            "lists_slot_order": int(self.lists_slot_order),
         }
 
 

@@ -19,9 +19,13 @@ from pbf_b200 import Particles, _abi, make_scene
 pytestmark = pytest.mark.gpu
 GOLDEN = Path(__file__).resolve().parent / "golden"
 REL_TOL = 1e-5
-# bars of the 100-step averaged statistics at eps 600 (twice the reference's
-# own run-to-run spread), as for the default shape against the oracle
-BARS = {"mean_density_error": 0.014, "max_density_error": 0.044, "kinetic_energy": 0.02}
+# bars of the 100-step averaged statistics at eps 600: twice the reference's
+# own run-to-run spread, as for the default shape against the oracle, except
+# the max.  The max density error is set by how many particles pile exactly
+# into a wall corner, a discrete chaotic count: averaged over steps 81-100 of
+# the 65k dam, four launch shapes of the same build gave 3.67-3.93 (7%).  It
+# has the 10% bar it has against the reference's OpenMP build.
+BARS = {"mean_density_error": 0.014, "max_density_error": 0.10, "kinetic_energy": 0.02}
 
 
 # the library's default shapes (include/pbf.h)
