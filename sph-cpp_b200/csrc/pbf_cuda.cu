@@ -2874,6 +2874,15 @@ void launch_fill(pbf_ctx* ctx, const float4* pst) {
   }
 }
 
+// An upload starts the fast fill's order choice afresh: slot order first, no
+// lists counted.  The steps from an uploaded state then do not depend on what
+// the context ran before.
+int reset_fill_order(pbf_ctx* ctx) {
+  CK(cudaMemsetAsync(ctx->fill_words, 0, kFillWords * sizeof(uint32_t), ctx->stream));
+  CK(cudaMemsetAsync(ctx->fill_words + kFillSlotOrder, 1, 1, ctx->stream));
+  return PBF_OK;
+}
+
 // The list fill, then every gather pass of the step in one launch.
 void launch_persistent(pbf_ctx* ctx) {
   cudaStream_t s = ctx->stream;
@@ -3536,6 +3545,7 @@ int pbf_upload(pbf_ctx* ctx, const float* x, const float* v, size_t n) {
   if (n != ctx->n) drop_graphs(ctx);
   ctx->n = n;
   ctx->lists_valid = false;
+  if (int rc = reset_fill_order(ctx)) return rc;
   if (n == 0) return PBF_OK;
   float* dx = ctx->stage;
   float* dv = ctx->stage + 3 * ctx->capacity;
@@ -4633,7 +4643,8 @@ int pbf_autotune(pbf_ctx* ctx, int steps, pbf_tuning* chosen, double* ms) {
   if ((rc = snap.take(ctx, ctx->posH, n * sizeof(float4))) || (rc = snap.take(ctx, ctx->pstH, n * sizeof(float4))) ||
       (rc = snap.take(ctx, ctx->velH, n * sizeof(float4))) || (rc = snap.take(ctx, ctx->scrH, n * sizeof(float4))) ||
       (rc = snap.take(ctx, ctx->lamH, n * sizeof(float))) || (rc = snap.take(ctx, ctx->origH, n * sizeof(uint32_t))) ||
-      (rc = snap.take(ctx, ctx->lamsumH, n * sizeof(float))))
+      (rc = snap.take(ctx, ctx->lamsumH, n * sizeof(float))) ||
+      (rc = snap.take(ctx, ctx->fill_words, kFillWords * sizeof(uint32_t))))
     return rc;
   const bool timing = ctx->timing;
   const pbf_tuning before = ctx->tune;
