@@ -183,7 +183,9 @@ const char* pbf_create_error(void);
 int pbf_set_params(pbf_ctx* ctx, const pbf_params* p);
 int pbf_get_params(const pbf_ctx* ctx, pbf_params* p);
 
-/* Host AoS float3 state in; x* = x (particles.h:184-199).  v may be NULL (zero). */
+/* Host AoS float3 state in; x* = x (particles.h:184-199).  v may be NULL (zero).
+ * Fast math: also starts the list-order choice afresh (slot order first), so
+ * steps from an uploaded state do not depend on what the context ran before. */
 int pbf_upload(pbf_ctx* ctx, const float* x_aos, const float* v_aos, size_t n);
 /* Download in the reference's particle order; any pointer may be NULL. */
 int pbf_download(pbf_ctx* ctx, float* x_aos, float* v_aos, float* rho, float* lambda);
@@ -226,7 +228,8 @@ int pbf_step(pbf_ctx* ctx, int nsteps);
  *  sorted_ids [N]   particle ids in sorted-bin order (neighbors.h:130-132)
  *  sorted_keys [N]  bin id of each sorted entry
  *  bin_begin/bin_end [B]  lower/upper bound of every bin (neighbors.h:137-148)
- * Any pointer may be NULL. */
+ * Any pointer may be NULL.  idx is in the reference's order (x offset outer)
+ * whatever order the fast fill walked in (pbf_stats_t.lists_slot_order). */
 int pbf_get_neighbors(pbf_ctx* ctx, int32_t* idx, int32_t* count);
 int pbf_get_bins(pbf_ctx* ctx, uint32_t* sorted_keys, uint32_t* sorted_ids,
                  uint32_t* bin_begin, uint32_t* bin_end);
