@@ -671,12 +671,21 @@ constexpr uint8_t kSegReferenceOrder = 0xFF;
 // The fast path's choice of list order, in device words (FillWord): the
 // lists that reached the cap in the fill under way, the slot-order lists
 // queued for the reference's walk, the order of the next fill (1 = slot
-// order), the redo kernel's block ticket, and the order the last fill used.  The cap keeps the first entries in the
-// reference's order, so a slot-order list that reaches it is walked again in
-// that order (k_fill_redo).  Once more than 1 / kSlotCappedShare of the lists
-// reach the cap (a dam that has settled), the fill walks in the reference's
-// order, where the cap costs nothing, until the share drops again.
-enum FillWord { kFillCapped = 0, kFillQueued = 1, kFillSlotOrder = 2, kFillTicket = 3, kFillLastOrder = 4, kFillWords = 5 };
+// order), the redo kernel's block ticket, and the order the last fill used.
+// The cap keeps the first entries in the reference's order, so a slot-order
+// list that reaches it is walked again in that order (k_fill_redo).  Once
+// more than 1 / kSlotCappedShare of the lists reach the cap (a dam that has
+// settled), the fill walks in the reference's order, where the cap costs
+// nothing, until the share drops again.  At 1 in 16 or 1 in 8 the re-walks
+// cost more than the slot order saves in the gathers.
+enum FillWord {
+  kFillCapped = 0,
+  kFillQueued = 1,
+  kFillSlotOrder = 2,
+  kFillTicket = 3,
+  kFillLastOrder = 4,
+  kFillWords = 5
+};
 constexpr uint32_t kSlotCappedShare = 64;
 
 // The list of slot b (a thread's share of k_fill2).  SLOT (fast math): in
