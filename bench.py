@@ -200,14 +200,14 @@ def kernel_bytes(name: str, n: int, nbar: float, K: int, nbins: int) -> float:
         "density_lambda": 16 + L + 16 + 4 + 4,                  # x* in; list; (x*, lambda), rho, lambda out
         "lambda_fixup": 16 + L + 16 + 4,                        # exact math after a nudge: x* in, list; (x*, lambda), lambda out
         "dp_update": 16 + L + 16 + (32.0 / K),                  # (x*, lambda) in; list; x* out; last: x in, v out
-        "viscosity": 16 + 16 + L + 16 + 4 * nbar,                # ...; v out and the weight of every entry
+        "viscosity": 16 + 16 + L + 16 + 2 * nbar,                # ...; v out and the weight of every entry (half)
         "vorticity": 16 + 16 + L + 16 + 16,
         "apply_vorticity": 16 + 16 + 16 + L + 16,
-        "viscosity_final": 16 + 16 + L + 4 * nbar + 16 + 16 + 16 + 4 + 4,  # ...; the entries' weights in
+        "viscosity_final": 16 + 16 + L + 2 * nbar + 16 + 16 + 16 + 4 + 4,  # ...; the entries' weights in (half)
         "update_velocities": 16 + 16 + 16,
         # every gather pass of the step in one launch (pbf_set_persistent)
-        "persistent_step": K * ((40 + L) + (32 + L)) + 32 + (48 + L + 4 * nbar) + (64 + L) + (64 + L)
-                           + (96 + L + 4 * nbar),
+        "persistent_step": K * ((40 + L) + (32 + L)) + 32 + (48 + L + 2 * nbar) + (64 + L) + (64 + L)
+                           + (96 + L + 2 * nbar),
         "color_field": 16 + 16 + L + 16,
         "surface_tension": 16 + 16 + 16 + L + 16,
     }

@@ -1857,7 +1857,7 @@ __device__ __forceinline__ void viscosity_tile(int tile, const Fast& F, int n, s
                                                const int32_t* __restrict__ nbr, const int32_t* __restrict__ cnt,
                                                const float4* __restrict__ pst, const float4* __restrict__ vin,
                                                float4* vout, float4* posH, float4* pstH,
-                                               const uint32_t* __restrict__ origS, uint32_t* origH, float* wvis,
+                                               const uint32_t* __restrict__ origS, uint32_t* origH, __half* wvis,
                                                Src src = Src{nullptr, nullptr, nullptr, 0}) {
   const pbf::Group G = pbf::group_at<GL>(n, tile);
   const int b = G.b;
@@ -1876,7 +1876,7 @@ __device__ __forceinline__ void viscosity_tile(int tile, const Fast& F, int n, s
   };
   const int32_t* row = nbr + pbf::list_base(b, stride);
   if (!STAGED && wvis != nullptr) {
-    float* wrow = wvis + pbf::list_base(b, stride);
+    __half* wrow = wvis + pbf::list_base(b, stride);
     if (FINAL)
       pbf::gwalkw<GL, false, COH>(row, wrow, c, n, G.lane, vin, [&](int, float wr, float4 vq) { add(wr, vq); });
     else
@@ -1909,7 +1909,7 @@ __global__ void __launch_bounds__(kBlock) kf_viscosity(Dev P, Fast F, int n, siz
                                                        const float4* __restrict__ pst, const float4* __restrict__ vin,
                                                        float4* vout, float4* posH, float4* pstH,
                                                        const uint32_t* __restrict__ origS, uint32_t* origH,
-                                                       float* wvis) {
+                                                       __half* wvis) {
   viscosity_tile<FINAL, GL>(blockIdx.x, F, n, stride, nbr, cnt, pst, vin, vout, posH, pstH, origS, origH, wvis);
 }
 
@@ -2100,7 +2100,8 @@ struct PersistPlan {
 };
 struct PersistArrays {
   float4 *pst, *xl, *vel, *velT, *pos, *scr, *velH, *posH, *pstH;
-  float *lam, *wvis;
+  float* lam;
+  __half* wvis;
   uint32_t *nudge, *err, *origH;
   const uint32_t *cell_start, *run_end, *origS;
   int32_t *nbr, *cnt;
@@ -2352,7 +2353,7 @@ struct pbf_ctx {
   uint32_t *cell_count = nullptr, *cell_start = nullptr, *scan_part = nullptr, *err = nullptr, *nudge = nullptr;
   unsigned long long *pairs = nullptr, *pairs_sorted = nullptr;
   int32_t *nbr = nullptr, *cnt = nullptr;
-  float* wvis = nullptr;  // XSPH weights per list entry (the list's layout), in stage_i's memory
+  __half* wvis = nullptr;  // XSPH weights per list entry (the list's layout, half precision), in stage_i's memory
   float* stage = nullptr;  // 6*C floats: two AoS float3 staging areas
   // neighbor export staging (C*cap + C); within a step, the XSPH weights
   // (wvis: written by the first viscosity pass, read by the final one)
@@ -3456,7 +3457,7 @@ static int create_ctx(const pbf_params* p, size_t capacity, const pbf_scene* sce
       (rc = dalloc(ctx, &ctx->mlp_loss, 1)) || (rc = dalloc(ctx, &ctx->w1b, pbf::kMlpH * pbf::kMlpInPad)) ||
       (rc = dalloc(ctx, &ctx->w2b, pbf::kMlpH * pbf::kMlpH)) || (rc = dalloc(ctx, &ctx->w2tb, pbf::kMlpH * pbf::kMlpH)))
     return bail(rc);
-  ctx->wvis = reinterpret_cast<float*>(ctx->stage_i);
+  ctx->wvis = reinterpret_cast<__half*>(ctx->stage_i);
   if (!ctx->scenes.empty() &&
       ((rc = dalloc(ctx, &ctx->d_regions, ctx->regions.size())) ||
        (rc = dalloc(ctx, &ctx->d_scene_first, ctx->scene_first.size())) || (rc = upload_scenes(ctx))))

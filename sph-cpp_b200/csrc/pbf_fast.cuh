@@ -16,6 +16,7 @@
 // nudge condition |r| < 1e-8, particles.h:303-305) falls back to the
 // reference-ordered path for that particle.
 #pragma once
+#include <cuda_fp16.h>
 #include "pbf_kernels.cuh"
 
 namespace pbf {
@@ -253,20 +254,23 @@ __device__ __forceinline__ void gwalk2(const int32_t* __restrict__ row, int c, i
 // change between them), so the first stores it beside its list entry (the
 // same warp-tiled layout, `wrow` = the weight row of the particle's list row)
 // and the final pass reads it as a coalesced stream instead of gathering the
-// neighbour's x* (one scattered record per entry instead of two).
+// neighbour's x* (one scattered record per entry instead of two).  Stored
+// in half precision (2 bytes per entry, the final pass's weight within 2^-11
+// of the first pass's): half the weight stream's bytes, within the fast
+// path's tolerances.
 // gwalk2 that also stores body's return value per entry:
 template <int GL = kGL, bool COH = false, class Body>
-__device__ __forceinline__ void gwalk2w(const int32_t* __restrict__ row, float* wrow, int c, int dummy, int lane,
+__device__ __forceinline__ void gwalk2w(const int32_t* __restrict__ row, __half* wrow, int c, int dummy, int lane,
                                         const float4* __restrict__ a, const float4* __restrict__ bsrc, Body&& body) {
   const int2* r2 = reinterpret_cast<const int2*>(row);
-  float2* w2 = reinterpret_cast<float2*>(wrow);
+  __half2* w2 = reinterpret_cast<__half2*>(wrow);
   auto at = [&](int t) { return GL % 4 == 0 ? t * kBatchVecs * GL + vec2_at(lane) : vec2_at(t * GL + lane); };
   auto two = [&](int t, int2 q) {
     const float4 a0 = ldw<COH>(a + q.x), b0 = ldw<COH>(bsrc + q.x);
     const float4 a1 = ldw<COH>(a + q.y), b1 = ldw<COH>(bsrc + q.y);
     const float w0 = body(q.x, a0, b0);
     const float w1 = body(q.y, a1, b1);
-    w2[at(t)] = make_float2(w0, w1);
+    w2[at(t)] = __floats2half2_rn(w0, w1);
   };
   const int full = c / (2 * GL);
   int t = 0;
@@ -277,10 +281,10 @@ __device__ __forceinline__ void gwalk2w(const int32_t* __restrict__ row, float* 
 // The final pass's walk: entry q with its stored weight w and one record
 // (entries past the count: the dummy record, weight 0); PF as gwalk1.
 template <int GL = kGL, bool PF = false, bool COH = false, class Body>
-__device__ __forceinline__ void gwalkw(const int32_t* __restrict__ row, const float* __restrict__ wrow, int c,
+__device__ __forceinline__ void gwalkw(const int32_t* __restrict__ row, const __half* __restrict__ wrow, int c,
                                        int dummy, int lane, const float4* __restrict__ bsrc, Body&& body) {
   const int2* r2 = reinterpret_cast<const int2*>(row);
-  const float2* w2 = reinterpret_cast<const float2*>(wrow);
+  const __half2* w2 = reinterpret_cast<const __half2*>(wrow);
   auto at = [&](int t) { return GL % 4 == 0 ? t * kBatchVecs * GL + vec2_at(lane) : vec2_at(t * GL + lane); };
   auto two = [&](int2 q, float2 w) {
     const float4 b0 = ldw<COH>(bsrc + q.x), b1 = ldw<COH>(bsrc + q.y);
@@ -296,10 +300,10 @@ __device__ __forceinline__ void gwalkw(const int32_t* __restrict__ row, const fl
     const int batches = (c + 2 * GL - 1) / (2 * GL);
     if (batches == 0) return;
     int2 next = ldw<COH>(r2 + at(0));
-    float2 wnext = ldw<COH>(w2 + at(0));
+    __half2 wnext = ldw<COH>(w2 + at(0));
     for (int t = 0; t < batches; ++t) {
       int2 q = next;
-      float2 w = wnext;
+      float2 w = __half22float2(wnext);
       if (t + 1 < batches) {
         next = ldw<COH>(r2 + at(t + 1));
         wnext = ldw<COH>(w2 + at(t + 1));
@@ -310,10 +314,10 @@ __device__ __forceinline__ void gwalkw(const int32_t* __restrict__ row, const fl
   } else {
     const int full = c / (2 * GL);
     int t = 0;
-    for (; t < full; ++t) two(ldw<COH>(r2 + at(t)), ldw<COH>(w2 + at(t)));
+    for (; t < full; ++t) two(ldw<COH>(r2 + at(t)), __half22float2(ldw<COH>(w2 + at(t))));
     if (t * 2 * GL < c) {
       int2 q = ldw<COH>(r2 + at(t));
-      float2 w = ldw<COH>(w2 + at(t));
+      float2 w = __half22float2(ldw<COH>(w2 + at(t)));
       tail(t, q, w);
       two(q, w);
     }
